@@ -1,0 +1,434 @@
+"""Benchmark of the Wilson hopping matrix on B200 (one JSON line on rank 0).
+
+Workload: FP64 Wilson hopping matrix H on a 32^3x64 lattice (random SU(3)
+links, Gaussian spinor), the reference's single-device benchmark size. One
+step = one full-lattice application H = (H_eo, H_oe), which the reference's
+driver times as an eo+oe pair of calls (tests/test_hopping.c:291-301).
+GFLOP/s use 1320 flop per output site.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value     : device-resident full-lattice kernel, inputs in HBM, CUDA events.
+e2e       : the reference-facing C-ABI (plqcd_hopping_matrix_eo/oe on host
+            arrays from amalloc'd pinned memory), host<->device copies of each
+            call's input and output parity inside the timed region.
+roofline  : the dominant kernel's algorithmic bytes / launch time against the
+            measured HBM copy bandwidth.
+cpu_baseline / --impl reference: the reference's own plain-C OpenMP hopping
+            pair compiled from its sources (oracle/_ref), on the host cores.
+
+Multi-GPU (torchrun): independent replicas, one lattice per GPU, no
+collective on the data path; barrier + max over ranks for the timing.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L_BENCH = (32, 32, 32, 64)
+FLOP_PER_SITE = 1320
+# algorithmic (compulsory) bytes per output site
+BYTES_PARITY = {0: 192 + 8 * 144 + 192, 1: 96 + 8 * 72 + 96}        # F64 / F32, 18-real, one parity
+BYTES_FULL = {0: 192 + 4 * 144 + 192, 1: 96 + 4 * 72 + 96}          # full lattice: each link read once
+BYTES_F32_12 = 96 + 8 * 48 + 96
+BYTES_HALF_12 = 52 + 8 * 24 + 52
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend="nccl"):
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, n in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        if not sm:
+            return None
+        busy = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle/_ref): the reference's own plain-C OpenMP pair
+# ---------------------------------------------------------------------------
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_reference_time(L, qin, u, steps: int, warmup: int, budget_s: float | None):
+    """Seconds per full H (eo+oe) of the compiled reference, from its own
+    return values (lib/dirac.c:405-407). Returns (sec_per_step, steps_run,
+    threads, kind)."""
+    from oracle import oracle as O
+    nthr = host_threads()
+    try:
+        ref = O.CompiledReference("patched")
+        kind = "reference"
+    except FileNotFoundError:
+        ref = None
+        kind = "port"
+    out = np.zeros_like(qin)
+    if ref is not None:
+        for _ in range(warmup):
+            ref.hop("full", L, qin, u, out, nthreads=nthr)
+        tot, n = 0.0, 0
+        t_start = time.time()
+        while n < steps and (budget_s is None or time.time() - t_start < budget_s or n == 0):
+            _, t = ref.hop("full", L, qin, u, out, nthreads=nthr)
+            tot += t
+            n += 1
+        return tot / n, n, nthr, kind
+    R = O.Restatement()
+    for _ in range(warmup):
+        R.hop("full", L, qin, u, nthreads=nthr)
+    tot, n = 0.0, 0
+    t_start = time.time()
+    while n < steps and (budget_s is None or time.time() - t_start < budget_s or n == 0):
+        t0 = time.perf_counter()
+        R.hop("full", L, qin, u, nthreads=nthr)
+        tot += time.perf_counter() - t0
+        n += 1
+    return tot / n, n, nthr, kind
+
+
+def host_fields(L, seed):
+    """API-layout host fields (qin, u) generated on the host with numpy."""
+    from oracle import oracle as O
+    V = O.volume(L)
+    rng = np.random.default_rng(seed)
+    return O.gaussian_spinor(V, rng), O.random_su3(4 * V, rng)
+
+
+def run_reference(args, d: Dist):
+    """--impl reference: the reference's CPU implementation of the path."""
+    if d.rank != 0:
+        return 0
+    L = L_BENCH
+    V = int(np.prod(L))
+    qin, u = host_fields(L, 1234)
+    sec, n, nthr, kind = cpu_reference_time(L, qin, u, args.steps, args.warmup, None)
+    gflops = V * FLOP_PER_SITE / sec / 1e9
+    line = {
+        "impl": "reference", "metric": "Dslash GFLOP/s", "value": round(gflops, 3), "unit": "GFLOP/s",
+        "n_gpus": args.gpus, "steps": n, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (random SU(3) links, Gaussian spinor)",
+        "config": {"workload": "FP64 Wilson hopping matrix, full lattice (eo+oe), 32^3x64",
+                   "lattice": list(L), "flop_per_site": FLOP_PER_SITE},
+        "cpu_baseline": {"value": round(gflops, 3), "unit": "GFLOP/s", "cores": nthr, "kind": kind,
+                         "sample": f"{n} full-lattice applications (eo+oe) at 32^3x64, times from the "
+                                   "reference's own return values"},
+        "e2e": {"value": round(gflops, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def time_kernel(torch, fn, steps: int, warmup: int, d: Dist | None = None):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    if d:
+        d.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    if d:
+        d.barrier()
+    return e0.elapsed_time(e1)
+
+
+def run_ours(args, d: Dist):
+    import torch
+
+    import plqcd_b200 as P
+    torch.cuda.set_device(d.local)
+    hbm, peak_kind = measured_peaks()
+    L = L_BENCH
+    lat = P.Lattice(L, d.local, torch.cuda.current_stream().cuda_stream)
+    V, Vh = lat.V, lat.Vh
+
+    def buf(prec):
+        return torch.empty(lat.spinor_bytes(prec), dtype=torch.uint8, device="cuda")
+
+    g64 = P.Gauge(lat, P.F64, 18)
+    g64.random(1234 + d.rank)
+    fe, fo, oe_, oo_ = buf(P.F64), buf(P.F64), buf(P.F64), buf(P.F64)
+    lat.spinor_gaussian(fe, P.F64, 0, 77 + d.rank)
+    lat.spinor_gaussian(fo, P.F64, 1, 77 + d.rank)
+
+    # ---- headline: full lattice H, FP64, device resident ------------------
+    K, W = args.steps, args.warmup
+    full = lambda: lat.dslash_full(g64, oe_, oo_, fe, fo, P.F64)
+    clk = ClockSampler(d.local)
+    clk.start()
+    ms = time_kernel(torch, full, K, W, d)
+    clocks = clk.stop()
+    ms_max = d.max(ms)
+    t_step = ms_max / 1e3 / K
+    value = d.world * V * FLOP_PER_SITE / t_step / 1e9
+    achieved = V * BYTES_FULL[0] / t_step / 1e9
+
+    # ---- per-parity kernels (the drop-in and solver building block) ---------
+    Kp = max(10, K // 2)
+    eo = lambda: lat.dslash(g64, oe_, fo, P.EVEN, P.F64)
+    oe = lambda: lat.dslash(g64, oo_, fe, P.ODD, P.F64)
+    ms_eo = time_kernel(torch, eo, Kp, W)
+    ms_oe = time_kernel(torch, oe, Kp, W)
+    t_eo, t_oe = ms_eo / 1e3 / Kp, ms_oe / 1e3 / Kp
+    parity = {
+        "eo_gflops": round(Vh * FLOP_PER_SITE / t_eo / 1e9, 1),
+        "oe_gflops": round(Vh * FLOP_PER_SITE / t_oe / 1e9, 1),
+        "eo_gbs": round(Vh * BYTES_PARITY[0] / t_eo / 1e9, 1),
+        "oe_gbs": round(Vh * BYTES_PARITY[0] / t_oe / 1e9, 1),
+        "pair_gflops": round(V * FLOP_PER_SITE / (t_eo + t_oe) / 1e9, 1),
+    }
+
+    # ---- FP32 (config: FP64 and FP32 at 32^3x64) ------------------------------
+    g32 = P.Gauge(lat, P.F32, 18)
+    g32.copy_from(g64)
+    f32e, f32o, o32e, o32o = buf(P.F32), buf(P.F32), buf(P.F32), buf(P.F32)
+    lat.spinor_convert(f32e, P.F32, fe, P.F64)
+    lat.spinor_convert(f32o, P.F32, fo, P.F64)
+    ms32 = time_kernel(torch, lambda: lat.dslash_full(g32, o32e, o32o, f32e, f32o, P.F32), Kp, W)
+    ms32e = time_kernel(torch, lambda: lat.dslash(g32, o32e, f32o, P.EVEN, P.F32), Kp, W)
+    t32, t32e = ms32 / 1e3 / Kp, ms32e / 1e3 / Kp
+    fp32 = {"full_gflops": round(V * FLOP_PER_SITE / t32 / 1e9, 1),
+            "full_gbs": round(V * BYTES_FULL[1] / t32 / 1e9, 1),
+            "eo_gflops": round(Vh * FLOP_PER_SITE / t32e / 1e9, 1),
+            "eo_gbs": round(Vh * BYTES_PARITY[1] / t32e / 1e9, 1)}
+    del g32, f32e, f32o, o32e, o32o
+
+    # ---- e2e through the reference-facing C-ABI (host arrays) ---------------
+    e2e = run_e2e(torch, P, lat, g64, fe, fo, d, args)
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
+    cpu = None
+    if d.world == 1 and not args.no_cpu:
+        qin = e2e.pop("_qin")
+        u = e2e.pop("_u")
+        sec, n, nthr, kind = cpu_reference_time(L, qin, u, 1000, 1, args.cpu_budget)
+        cpu = {"value": round(V * FLOP_PER_SITE / sec / 1e9, 3), "unit": "GFLOP/s", "cores": nthr, "kind": kind,
+               "sample": f"{n} full-lattice applications (eo+oe) at 32^3x64 after 1 warm-up, "
+                         "times from the reference's own return values"}
+    e2e.pop("_qin", None)
+    e2e.pop("_u", None)
+
+    line = {
+        "metric": "Dslash GFLOP/s", "value": round(value, 1), "unit": "GFLOP/s", "n_gpus": d.world,
+        "steps": K, "warmup": W, "ms_per_step": round(t_step * 1e3, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (random SU(3) links from a counter-based generator, Gaussian spinor)",
+        "config": {"workload": "FP64 Wilson hopping matrix, full lattice (eo+oe in one launch), 32^3x64",
+                   "lattice": list(L), "flop_per_site": FLOP_PER_SITE, "links": "18-real",
+                   "l2": "inputs larger than L2 (1.5 GB per step vs 126 MB)",
+                   "parallelism": f"replicas x{d.world}"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
+                     "bytes_per_site": BYTES_FULL[0], "kernel": "k_dslash<F64,18,full>",
+                     "traffic": None},
+        "per_parity_f64": parity,
+        "f32": fp32,
+        "e2e": e2e,
+        "gpu_launches": K,
+        "clocks": clocks,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_e2e(torch, P, lat, g64, fe, fo, d: Dist, args):
+    """eo+oe through plqcd_hopping_matrix_*_sse3_assymbly on pinned host
+    arrays, copies included, wall clock (the calls are synchronous)."""
+    from oracle import oracle as O
+    L = lat.dims
+    V = lat.V
+    os.environ["PLQCD_DEVICE"] = str(d.local)
+    path = O.write_input_file(L, nthreads=1)
+    P.finalize_plqcd()
+    if P.init_plqcd(path) != 0:
+        raise RuntimeError(P.last_error())
+    os.unlink(path)
+    lib = P.lib()
+    nq, nu = V * 192, 4 * V * 144
+    pq, pout, pu = lib.amalloc(nq, 6), lib.amalloc(nq, 6), lib.amalloc(nu, 6)
+    mk = lambda p, n: np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_double)), (n // 8,)).view(
+        np.complex128)
+    qin, qout, u = mk(pq, nq).reshape(V, 12), mk(pout, nq).reshape(V, 12), mk(pu, nu).reshape(4 * V, 9)
+    P.check(lib.plqcd_gauge_store_host(g64.handle, pu))
+    aos = torch.zeros((V, 12), dtype=torch.complex128, device="cuda")
+    lat.spinor_export(fe, P.F64, 0, aos)
+    lat.spinor_export(fo, P.F64, 1, aos)
+    lat.synchronize()
+    qin[:] = aos.cpu().numpy()
+    del aos
+    qout[:] = 0
+    Ke = max(3, min(args.steps, args.e2e_steps))
+    for _ in range(max(1, min(args.warmup, 3))):
+        P.hopping_matrix("eo", qin, qout, u)
+        P.hopping_matrix("oe", qin, qout, u)
+    d.barrier()
+    t0 = time.perf_counter()
+    for _ in range(Ke):
+        P.hopping_matrix("eo", qin, qout, u)
+        P.hopping_matrix("oe", qin, qout, u)
+    dt = time.perf_counter() - t0
+    d.barrier()
+    dt = d.max(dt)
+    kms, h2d, d2h = P.dropin_last_stats()
+    res = {"value": round(d.world * V * FLOP_PER_SITE * Ke / dt / 1e9, 2), "unit": "GFLOP/s",
+           "h2d_bytes_per_step": int(2 * h2d), "d2h_bytes_per_step": int(2 * d2h), "steps": Ke,
+           "ms_per_step": round(dt / Ke * 1e3, 3),
+           "api": "plqcd_hopping_matrix_eo/oe_sse3_assymbly on amalloc'd (pinned) host arrays; "
+                  "gauge field cached on the device after the first call"}
+    # keep copies for the CPU baseline before the pinned blocks go away
+    res["_qin"] = np.array(qin)
+    res["_u"] = np.array(u)
+    P.finalize_plqcd()
+    lib.afree(pq)
+    lib.afree(pout)
+    lib.afree(pu)
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-baseline sampling")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    d = Dist()
+    if args.impl == "reference":
+        return run_reference(args, d)
+    d.init("nccl")
+    try:
+        return run_ours(args, d)
+    finally:
+        d.close()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

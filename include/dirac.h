@@ -1,0 +1,58 @@
+/*
+ * dirac.h -- Wilson hopping matrix entry points (plqcd-b200).
+ *
+ * The reference's include/dirac.h:19-33 entry points on host arrays in the
+ * API layout of su3.h, all computed by the sm_100a CUDA kernels:
+ *
+ *   eo: qout[0, V/2)   = H_eo qin[V/2, V)   (odd input -> even output)
+ *   oe: qout[V/2, V)   = H_oe qin[0, V/2)   (even input -> odd output)
+ *
+ *   (H psi)(x) = sum_mu U_mu(x) (1 - g_mu) psi(x+mu)
+ *              + U_mu(x-mu)^dag (1 + g_mu) psi(x-mu)
+ *
+ * with periodic boundaries, no kappa, the reference's gamma basis and even/odd
+ * site order, links u[4*i+mu] = U_mu(x_i) (lib/dirac.c:35-791). Only the
+ * output half of qout is written. The return value is the call's wall-clock
+ * time in seconds (lib/dirac.c:405-407), host<->device copies included, or a
+ * negative value on failure (message in plqcd_last_error()).
+ *
+ * Results follow the correct operator. The reference as shipped differs in
+ * spin components s2/s3 (include/su3.h:135-138 used at lib/dirac.c:373-374,
+ * 756-757) and in the oe forward links (lib/dirac.c:643); setting the
+ * environment variable PLQCD_REF_COMPAT=1 before init_plqcd reproduces that
+ * behaviour exactly.
+ *
+ * The SSE3-intrinsic names (lib/dirac.c:801, 1272, 1748, 2124) take the same
+ * arguments and map to the same correct kernel. The gauge field is cached on
+ * the device by host pointer plus a sampled fingerprint; call
+ * plqcd_gauge_update() (plqcd_b200.h) after changing links in place, or set
+ * PLQCD_GAUGE_CACHE=0 to upload on every call.
+ */
+#ifndef _DIRAC_H
+#define _DIRAC_H
+
+#include "plqcd_global_params.h"
+#include "start.h"
+#include "utils.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct plqcd_timer {
+    double total;
+    double computation;
+};
+
+double plqcd_hopping_matrix_eo_sse3_assymbly(spinor *qin, spinor *qout, su3 *u);
+double plqcd_hopping_matrix_oe_sse3_assymbly(spinor *qin, spinor *qout, su3 *u);
+
+double plqcd_hopping_matrix_eo_sse3_intrin(spinor *qin, spinor *qout, su3 *u);
+double plqcd_hopping_matrix_oe_sse3_intrin(spinor *qin, spinor *qout, su3 *u);
+double plqcd_hopping_matrix_eo_sse3_intrin_blocking(spinor *qin, spinor *qout, su3 *u);
+double plqcd_hopping_matrix_oe_sse3_intrin_blocking(spinor *qin, spinor *qout, su3 *u);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

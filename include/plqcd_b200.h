@@ -1,0 +1,156 @@
+/*
+ * plqcd_b200.h -- device-resident API of plqcd-b200 (sm_100a).
+ *
+ * The drop-in entry points of dirac.h take host arrays in the API layout
+ * and pay host<->device copies on every call. This header exposes the same
+ * operator on fields that stay in HBM, in the layouts the kernels read,
+ * plus reduced-precision storage, the even/odd preconditioned Wilson
+ * solver, multi-RHS and multi-lattice batches. The reference has no
+ * counterpart for anything here except the hopping matrix itself
+ * (lib/dirac.c:35-791); its operator and solver parameters are
+ * placeholders (include/plqcd_global_params.h:197-201).
+ *
+ * Conventions
+ *  - Every function returns PLQCD_OK (0) or a negative status; the message
+ *    is in plqcd_last_error() (thread-local). Nothing aborts the caller.
+ *  - Device pointers are plain CUDA device addresses on the lattice's
+ *    device; the caller owns them. Work is queued on the lattice's stream.
+ *  - Site order is the reference's even/odd order (lib/start.c:406-433):
+ *    within one parity, half-site index h = x/2 + L0/2*(y + L1*(z + L2*t)).
+ *
+ * Device field layouts (one parity, Vh = V/2 half-sites; "plane" = Vh
+ * consecutive elements):
+ *   spinor PLQCD_F64  : double2 [12][Vh]   plane k = complex 3*spin+colour
+ *   spinor PLQCD_F32  : float4  [6][Vh]    plane k = complexes 2k, 2k+1
+ *   spinor PLQCD_F16,
+ *          PLQCD_BF16 : 16-bit  [3][Vh][8] (uint4 planes, complexes 4k..4k+3)
+ *                       followed by float norm[Vh]; value = stored * norm,
+ *                       norm = max |real or imaginary part| of the site
+ *   gauge (both parities, 4 directions): [parity][mu][element][Vh]
+ *          F64 recon 18 : double2, 9 elements (row-major c00..c22)
+ *          F64 recon 12 : double2, 6 elements (rows 0,1)
+ *          F32 recon 18 : float2,  9 elements
+ *          F32 recon 12 : float4,  3 elements (complex pairs of rows 0,1)
+ *          F16/BF16 12  : 16-bit x4 (uint2), 3 elements
+ *   With 12-real storage row 2 is rebuilt as conj(row0 x row1), exact for
+ *   SU(3) links only.
+ * A multi-RHS spinor block is n fields back to back: [rhs][...one field...].
+ */
+#ifndef PLQCD_B200_H
+#define PLQCD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "su3.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ----------------------------------------------------------- */
+#define PLQCD_OK 0
+#define PLQCD_ERR_ARG -1      /* invalid argument */
+#define PLQCD_ERR_CUDA -2     /* CUDA runtime error */
+#define PLQCD_ERR_NOMEM -3    /* allocation failed */
+#define PLQCD_ERR_STATE -4    /* not initialised / wrong object state */
+#define PLQCD_ERR_TIMEOUT -5  /* a bounded device wait ran out */
+#define PLQCD_ERR_NOCONV -6   /* solver did not converge */
+#define PLQCD_ERR_NODEV -7    /* no CUDA device */
+
+const char *plqcd_last_error(void);
+int plqcd_last_status(void);
+void plqcd_clear_error(void);
+/* Library version string. */
+const char *plqcd_version(void);
+
+/* ---- precisions and flags --------------------------------------------- */
+#define PLQCD_F64 0
+#define PLQCD_F32 1
+#define PLQCD_F16 2
+#define PLQCD_BF16 3
+
+#define PLQCD_EVEN 0
+#define PLQCD_ODD 1
+
+/* dslash flags */
+#define PLQCD_DSLASH_COMPAT 1u  /* reproduce the reference as shipped (F64/18 only) */
+#define PLQCD_DSLASH_G5_IN 2u   /* apply gamma5 to the input spinor */
+#define PLQCD_DSLASH_G5_OUT 4u  /* apply gamma5 to H psi before the epilogue */
+
+/* ---- lattice context ---------------------------------------------------- */
+typedef struct plqcd_lattice plqcd_lattice;
+
+/* dims: L0..L3, each even and >= 2 (>= 4 for init_plqcd compatibility is
+ * not required here). device: CUDA ordinal. stream: cudaStream_t or NULL
+ * for a new non-blocking stream owned by the lattice. */
+int plqcd_lattice_create(const int dims[4], int device, void *stream, plqcd_lattice **out);
+int plqcd_lattice_destroy(plqcd_lattice *lat);
+int plqcd_lattice_set_stream(plqcd_lattice *lat, void *stream);
+void *plqcd_lattice_stream(const plqcd_lattice *lat);
+int plqcd_lattice_synchronize(plqcd_lattice *lat);
+long plqcd_lattice_half_volume(const plqcd_lattice *lat);
+/* Device time of the last kernel launched through the *_timed calls, ms. */
+double plqcd_lattice_last_kernel_ms(const plqcd_lattice *lat);
+
+size_t plqcd_spinor_bytes(const plqcd_lattice *lat, int prec);
+size_t plqcd_gauge_bytes(const plqcd_lattice *lat, int prec, int recon);
+
+/* ---- gauge fields (owned by the library) -------------------------------- */
+typedef struct plqcd_gauge plqcd_gauge;
+
+int plqcd_gauge_create(plqcd_lattice *lat, int prec, int recon, plqcd_gauge **out);
+int plqcd_gauge_destroy(plqcd_gauge *g);
+/* Device address of the gauge storage (layout above). */
+void *plqcd_gauge_data(plqcd_gauge *g);
+/* Load from links in the API layout (4V su3, u[4*i+mu]) on the host or on
+ * the device. */
+int plqcd_gauge_load_host(plqcd_gauge *g, const su3 *u_host);
+int plqcd_gauge_load_device(plqcd_gauge *g, const su3 *u_dev);
+/* Store to the API layout (row 2 rebuilt for 12-real storage). */
+int plqcd_gauge_store_host(const plqcd_gauge *g, su3 *u_host);
+/* Random SU(3) links from a counter-based generator keyed by (seed, site,
+ * mu): Gaussian complex 3x3, Gram-Schmidt rows 0,1, row 2 = conj(row0 x
+ * row1). */
+int plqcd_gauge_random(plqcd_gauge *g, uint64_t seed);
+/* Unit links (free field). */
+int plqcd_gauge_unit(plqcd_gauge *g);
+/* Convert between precisions / storage (dst and src on the same lattice). */
+int plqcd_gauge_copy(plqcd_gauge *dst, const plqcd_gauge *src);
+
+/* ---- spinor fields (caller-owned device buffers) ------------------------ */
+/* Import / export one parity between the API layout (full-lattice array of
+ * V spinors on the device, even/odd order) and a device field. */
+int plqcd_spinor_import(plqcd_lattice *lat, const spinor *aos_dev, int parity, void *dst, int prec);
+int plqcd_spinor_export(plqcd_lattice *lat, const void *src, int prec, int parity, spinor *aos_dev);
+/* Convert one parity between precisions. */
+int plqcd_spinor_convert(plqcd_lattice *lat, void *dst, int dst_prec, const void *src, int src_prec);
+/* Gaussian N(0,1) complex components, keyed by (seed, parity, site). */
+int plqcd_spinor_gaussian(plqcd_lattice *lat, void *dst, int prec, int parity, uint64_t seed);
+
+/* ---- hopping matrix on device fields ------------------------------------ */
+/* out (parity out_parity) = a * H in (in on the other parity) [+ b * x]
+ * where a applies to spins 0,1 and a_low to spins 2,3 (gamma5 folding),
+ * x may be NULL (then b is ignored). Spinor and gauge precisions must
+ * match. */
+int plqcd_dslash(plqcd_lattice *lat, const plqcd_gauge *g, void *out, const void *in, int out_parity,
+                 int prec, unsigned flags);
+int plqcd_dslash_xpay(plqcd_lattice *lat, const plqcd_gauge *g, void *out, const void *in,
+                      int out_parity, int prec, unsigned flags, double a, const void *x, double b);
+/* Full-lattice H in one launch: out_e = H_eo in_o and out_o = H_oe in_e.
+ * Each link is used by two sites of the same launch and read from HBM
+ * once. */
+int plqcd_dslash_full(plqcd_lattice *lat, const plqcd_gauge *g, void *out_even, void *out_odd,
+                      const void *in_even, const void *in_odd, int prec);
+
+/* ---- drop-in path controls ---------------------------------------------- */
+/* Mark the host gauge field `u` as changed (or a new field) so the next
+ * drop-in call uploads it. */
+int plqcd_gauge_update(const su3 *u);
+/* Device time (ms) of the kernels of the last drop-in hopping call and its
+ * host<->device byte counts. */
+int plqcd_dropin_last_stats(double *kernel_ms, double *h2d_bytes, double *d2h_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,301 @@
+"""plqcd_b200 -- Python binding of the B200 Wilson hopping-matrix library.
+
+The product is the C-ABI shared library ``libplqcd_b200.so`` built from
+``plqcd_b200/csrc`` (``python -m plqcd_b200.build``); this module only binds
+it with ctypes. There is no Python or CPU fallback: importing fails loudly
+when the library is missing.
+
+Two layers mirror the C headers in ``include/``:
+
+* the reference's drop-in entry points (``include/dirac.h``,
+  ``include/start.h``): ``init_plqcd``, ``hopping_matrix_eo/oe`` on host
+  numpy arrays in the API layout (reference lib/dirac.c:35-791);
+* the device-resident API (``include/plqcd_b200.h``): ``Lattice``,
+  ``Gauge`` and functions taking device pointers (e.g. ``tensor.data_ptr()``
+  of a torch CUDA tensor).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libplqcd_b200.so")
+
+F64, F32, F16, BF16 = 0, 1, 2, 3
+EVEN, ODD = 0, 1
+DSLASH_COMPAT, DSLASH_G5_IN, DSLASH_G5_OUT = 1, 2, 4
+PREC_NAMES = {F64: "f64", F32: "f32", F16: "f16", BF16: "bf16"}
+SPINOR_BYTES_PER_SITE = {F64: 192, F32: 96, F16: 52, BF16: 52}
+
+OK = 0
+
+
+class PlqcdError(RuntimeError):
+    pass
+
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+_u64 = ctypes.c_uint64
+_sz = ctypes.c_size_t
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+# name: (restype, argtypes)
+_SIGS = {
+    # include/start.h
+    "init_plqcd": (_i, [_i, ctypes.POINTER(ctypes.c_char_p)]),
+    "finalize_plqcd": (None, []),
+    "ipr": (_i, [_ip]),
+    "comp_cpr": (None, [_i, _ip]),
+    "set_npr": (None, []),
+    "lex2cart": (None, [_i, _ip]),
+    "cart2lex": (_i, [_ip]),
+    "set_geometry": (None, []),
+    "find_site": (None, [_ip, _ip, _ip]),
+    "print_params": (None, [_vp]),
+    # include/utils.h
+    "alloc": (_vp, [_sz, _sz]),
+    "amalloc": (_vp, [_sz, _i]),
+    "afree": (None, [_vp]),
+    "mpi_permanent_tag": (_i, []),
+    "mpi_tag": (_i, []),
+    "stop_watch": (_d, [_d]),
+    # include/dirac.h
+    "plqcd_hopping_matrix_eo_sse3_assymbly": (_d, [_vp, _vp, _vp]),
+    "plqcd_hopping_matrix_oe_sse3_assymbly": (_d, [_vp, _vp, _vp]),
+    "plqcd_hopping_matrix_eo_sse3_intrin": (_d, [_vp, _vp, _vp]),
+    "plqcd_hopping_matrix_oe_sse3_intrin": (_d, [_vp, _vp, _vp]),
+    "plqcd_hopping_matrix_eo_sse3_intrin_blocking": (_d, [_vp, _vp, _vp]),
+    "plqcd_hopping_matrix_oe_sse3_intrin_blocking": (_d, [_vp, _vp, _vp]),
+    # include/plqcd_b200.h
+    "plqcd_last_error": (ctypes.c_char_p, []),
+    "plqcd_last_status": (_i, []),
+    "plqcd_clear_error": (None, []),
+    "plqcd_version": (ctypes.c_char_p, []),
+    "plqcd_lattice_create": (_i, [_ip, _i, _vp, ctypes.POINTER(_vp)]),
+    "plqcd_lattice_destroy": (_i, [_vp]),
+    "plqcd_lattice_set_stream": (_i, [_vp, _vp]),
+    "plqcd_lattice_stream": (_vp, [_vp]),
+    "plqcd_lattice_synchronize": (_i, [_vp]),
+    "plqcd_lattice_half_volume": (ctypes.c_long, [_vp]),
+    "plqcd_lattice_last_kernel_ms": (_d, [_vp]),
+    "plqcd_spinor_bytes": (_sz, [_vp, _i]),
+    "plqcd_gauge_bytes": (_sz, [_vp, _i, _i]),
+    "plqcd_gauge_create": (_i, [_vp, _i, _i, ctypes.POINTER(_vp)]),
+    "plqcd_gauge_destroy": (_i, [_vp]),
+    "plqcd_gauge_data": (_vp, [_vp]),
+    "plqcd_gauge_load_host": (_i, [_vp, _vp]),
+    "plqcd_gauge_load_device": (_i, [_vp, _vp]),
+    "plqcd_gauge_store_host": (_i, [_vp, _vp]),
+    "plqcd_gauge_random": (_i, [_vp, _u64]),
+    "plqcd_gauge_unit": (_i, [_vp]),
+    "plqcd_gauge_copy": (_i, [_vp, _vp]),
+    "plqcd_spinor_import": (_i, [_vp, _vp, _i, _vp, _i]),
+    "plqcd_spinor_export": (_i, [_vp, _vp, _i, _i, _vp]),
+    "plqcd_spinor_convert": (_i, [_vp, _vp, _i, _vp, _i]),
+    "plqcd_spinor_gaussian": (_i, [_vp, _vp, _i, _i, _u64]),
+    "plqcd_dslash": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint]),
+    "plqcd_dslash_xpay": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint, _d, _vp, _d]),
+    "plqcd_dslash_full": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i]),
+    "plqcd_gauge_update": (_i, [_vp]),
+    "plqcd_dropin_last_stats": (_i, [_dp, _dp, _dp]),
+}
+
+_lib = None
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PlqcdError(f"{LIB_PATH} not found: build it with `python -m plqcd_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return (lib().plqcd_last_error() or b"").decode()
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise PlqcdError(f"plqcd error {rc}: {last_error()}")
+
+
+def _dims(L):
+    return (ctypes.c_int * 4)(*[int(x) for x in L])
+
+
+def _ptr(x) -> int | None:
+    """Device or host address of a torch tensor, numpy array or int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    raise TypeError(f"cannot take the address of {type(x)}")
+
+
+# ---------------------------------------------------------------------------
+# drop-in layer (include/start.h, include/dirac.h)
+# ---------------------------------------------------------------------------
+
+def init_plqcd(input_file: str) -> int:
+    argv = (ctypes.c_char_p * 3)(b"plqcd", input_file.encode(), None)
+    return lib().init_plqcd(2, argv)
+
+
+def finalize_plqcd() -> None:
+    lib().finalize_plqcd()
+
+
+def hopping_matrix(which: str, qin: np.ndarray, qout: np.ndarray, u: np.ndarray, variant: str = "sse3_assymbly") -> float:
+    """Call plqcd_hopping_matrix_{eo,oe}_<variant> on host arrays in the API
+    layout (complex128 (V, 12) spinors, (4V, 9) links). Returns the
+    library's elapsed seconds; raises on a negative return."""
+    for a in (qin, qout, u):
+        assert a.dtype == np.complex128 and a.flags.c_contiguous
+    f = getattr(lib(), f"plqcd_hopping_matrix_{which}_{variant}")
+    t = f(qin.ctypes.data, qout.ctypes.data, u.ctypes.data)
+    if t < 0:
+        raise PlqcdError(f"hopping matrix failed: {last_error()}")
+    return t
+
+
+def dropin_last_stats():
+    k, h, d = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    check(lib().plqcd_dropin_last_stats(ctypes.byref(k), ctypes.byref(h), ctypes.byref(d)))
+    return k.value, h.value, d.value
+
+
+# ---------------------------------------------------------------------------
+# device-resident layer (include/plqcd_b200.h)
+# ---------------------------------------------------------------------------
+
+class Lattice:
+    """A plqcd_lattice: geometry, CUDA stream and scratch of one lattice."""
+
+    def __init__(self, dims, device: int = 0, stream: int | None = None):
+        self.dims = tuple(int(x) for x in dims)
+        h = _vp()
+        check(lib().plqcd_lattice_create(_dims(self.dims), device, stream, ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+        self.Vh = int(lib().plqcd_lattice_half_volume(h))
+        self.V = 2 * self.Vh
+
+    def close(self):
+        if self.handle:
+            lib().plqcd_lattice_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self):
+        check(lib().plqcd_lattice_synchronize(self.handle))
+
+    @property
+    def stream(self) -> int:
+        return lib().plqcd_lattice_stream(self.handle) or 0
+
+    def spinor_bytes(self, prec: int) -> int:
+        return int(lib().plqcd_spinor_bytes(self.handle, prec))
+
+    def gauge_bytes(self, prec: int, recon: int) -> int:
+        return int(lib().plqcd_gauge_bytes(self.handle, prec, recon))
+
+    # spinor helpers -------------------------------------------------------
+    def spinor_import(self, aos_dev, parity: int, dst, prec: int):
+        check(lib().plqcd_spinor_import(self.handle, _ptr(aos_dev), parity, _ptr(dst), prec))
+
+    def spinor_export(self, src, prec: int, parity: int, aos_dev):
+        check(lib().plqcd_spinor_export(self.handle, _ptr(src), prec, parity, _ptr(aos_dev)))
+
+    def spinor_convert(self, dst, dprec: int, src, sprec: int):
+        check(lib().plqcd_spinor_convert(self.handle, _ptr(dst), dprec, _ptr(src), sprec))
+
+    def spinor_gaussian(self, dst, prec: int, parity: int, seed: int):
+        check(lib().plqcd_spinor_gaussian(self.handle, _ptr(dst), prec, parity, seed))
+
+    # hopping ----------------------------------------------------------------
+    def dslash(self, gauge: "Gauge", out, inp, out_parity: int, prec: int, flags: int = 0):
+        check(lib().plqcd_dslash(self.handle, gauge.handle, _ptr(out), _ptr(inp), out_parity, prec, flags))
+
+    def dslash_xpay(self, gauge: "Gauge", out, inp, out_parity: int, prec: int, a: float, x, b: float,
+                    flags: int = 0):
+        check(lib().plqcd_dslash_xpay(self.handle, gauge.handle, _ptr(out), _ptr(inp), out_parity, prec, flags,
+                                      a, _ptr(x), b))
+
+    def dslash_full(self, gauge: "Gauge", out_even, out_odd, in_even, in_odd, prec: int):
+        check(lib().plqcd_dslash_full(self.handle, gauge.handle, _ptr(out_even), _ptr(out_odd), _ptr(in_even),
+                                      _ptr(in_odd), prec))
+
+
+class Gauge:
+    """A plqcd_gauge: device gauge field owned by the library."""
+
+    def __init__(self, lat: Lattice, prec: int = F64, recon: int = 18):
+        h = _vp()
+        check(lib().plqcd_gauge_create(lat.handle, prec, recon, ctypes.byref(h)))
+        self.handle = h
+        self.lat = lat
+        self.prec = prec
+        self.recon = recon
+
+    def close(self):
+        if self.handle:
+            lib().plqcd_gauge_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def data(self) -> int:
+        return lib().plqcd_gauge_data(self.handle)
+
+    def load_host(self, u: np.ndarray):
+        assert u.dtype == np.complex128 and u.flags.c_contiguous and u.shape == (4 * self.lat.V, 9)
+        check(lib().plqcd_gauge_load_host(self.handle, u.ctypes.data))
+
+    def load_device(self, u_dev):
+        check(lib().plqcd_gauge_load_device(self.handle, _ptr(u_dev)))
+
+    def store_host(self) -> np.ndarray:
+        u = np.empty((4 * self.lat.V, 9), np.complex128)
+        check(lib().plqcd_gauge_store_host(self.handle, u.ctypes.data))
+        return u
+
+    def random(self, seed: int):
+        check(lib().plqcd_gauge_random(self.handle, seed))
+
+    def unit(self):
+        check(lib().plqcd_gauge_unit(self.handle))
+
+    def copy_from(self, src: "Gauge"):
+        check(lib().plqcd_gauge_copy(self.handle, src.handle))

@@ -1,0 +1,338 @@
+// device_fields.cuh -- complex arithmetic and storage accessors for the
+// device field layouts documented in include/plqcd_b200.h.
+//
+// Every accessor converts between a storage format in HBM and compute-type
+// complex numbers in registers. Loads go through the read-only path; stores
+// use streaming (evict-first) hints because outputs are not re-read by the
+// launch that writes them.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plqcd_b200.h"
+
+namespace plqcd {
+namespace dev {
+
+template <typename R>
+struct cx {
+    R re, im;
+};
+
+template <typename R>
+__device__ __forceinline__ cx<R> cadd(cx<R> a, cx<R> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename R>
+__device__ __forceinline__ cx<R> csub(cx<R> a, cx<R> b) { return {a.re - b.re, a.im - b.im}; }
+template <typename R>
+__device__ __forceinline__ cx<R> cmul(cx<R> a, cx<R> b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename R>
+__device__ __forceinline__ cx<R> conjmul(cx<R> a, cx<R> b) {  // conj(a) * b
+    return {a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re};
+}
+template <typename R>
+__device__ __forceinline__ cx<R> cconj(cx<R> a) { return {a.re, -a.im}; }
+
+// ---- streaming / read-only memory helpers ----------------------------------
+__device__ __forceinline__ double2 ld_ro(const double2 *p) { return __ldg(p); }
+__device__ __forceinline__ float4 ld_ro(const float4 *p) { return __ldg(p); }
+__device__ __forceinline__ float2 ld_ro(const float2 *p) { return __ldg(p); }
+__device__ __forceinline__ uint4 ld_ro(const uint4 *p) { return __ldg(p); }
+__device__ __forceinline__ uint2 ld_ro(const uint2 *p) { return __ldg(p); }
+__device__ __forceinline__ float ld_ro(const float *p) { return __ldg(p); }
+
+__device__ __forceinline__ void st_cs(double2 *p, double2 v) { __stcs(p, v); }
+__device__ __forceinline__ void st_cs(float4 *p, float4 v) { __stcs(p, v); }
+__device__ __forceinline__ void st_cs(float2 *p, float2 v) { __stcs(p, v); }
+__device__ __forceinline__ void st_cs(uint4 *p, uint4 v) { __stcs(p, v); }
+__device__ __forceinline__ void st_cs(uint2 *p, uint2 v) { __stcs(p, v); }
+__device__ __forceinline__ void st_cs(float *p, float v) { __stcs(p, v); }
+
+// ---- 16-bit pair packing ----------------------------------------------------
+template <int PREC>
+struct Half2;
+template <>
+struct Half2<PLQCD_F16> {
+    __device__ static __forceinline__ uint32_t pack(float a, float b) {
+        __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<uint32_t *>(&h);
+    }
+    __device__ static __forceinline__ float2 unpack(uint32_t w) {
+        __half2 h = *reinterpret_cast<__half2 *>(&w);
+        return __half22float2(h);
+    }
+};
+template <>
+struct Half2<PLQCD_BF16> {
+    __device__ static __forceinline__ uint32_t pack(float a, float b) {
+        __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<uint32_t *>(&h);
+    }
+    __device__ static __forceinline__ float2 unpack(uint32_t w) {
+        __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162 *>(&w);
+        return __bfloat1622float2(h);
+    }
+};
+
+// =============================================================================
+// spinor storage (one parity)
+// =============================================================================
+template <int PREC>
+struct SpinorIO;
+
+template <>
+struct SpinorIO<PLQCD_F64> {
+    using real = double;
+    static constexpr int bytes_per_site = 192;
+    __device__ static __forceinline__ void load(const void *base, long Vh, long h, cx<double> s[12]) {
+        const double2 *p = static_cast<const double2 *>(base) + h;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            double2 v = ld_ro(p + c * Vh);
+            s[c] = {v.x, v.y};
+        }
+    }
+    __device__ static __forceinline__ void store(void *base, long Vh, long h, const cx<double> s[12]) {
+        double2 *p = static_cast<double2 *>(base) + h;
+#pragma unroll
+        for (int c = 0; c < 12; c++) st_cs(p + c * Vh, make_double2(s[c].re, s[c].im));
+    }
+};
+
+template <>
+struct SpinorIO<PLQCD_F32> {
+    using real = float;
+    static constexpr int bytes_per_site = 96;
+    __device__ static __forceinline__ void load(const void *base, long Vh, long h, cx<float> s[12]) {
+        const float4 *p = static_cast<const float4 *>(base) + h;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            float4 v = ld_ro(p + k * Vh);
+            s[2 * k] = {v.x, v.y};
+            s[2 * k + 1] = {v.z, v.w};
+        }
+    }
+    __device__ static __forceinline__ void store(void *base, long Vh, long h, const cx<float> s[12]) {
+        float4 *p = static_cast<float4 *>(base) + h;
+#pragma unroll
+        for (int k = 0; k < 6; k++)
+            st_cs(p + k * Vh, make_float4(s[2 * k].re, s[2 * k].im, s[2 * k + 1].re, s[2 * k + 1].im));
+    }
+};
+
+// 16-bit storage with a per-site norm: value = stored * norm,
+// norm = max |component| over the 24 reals of the site.
+template <int PREC>
+struct SpinorIO16 {
+    using real = float;
+    static constexpr int bytes_per_site = 52;
+    __device__ static __forceinline__ const float *norms(const void *base, long Vh) {
+        return reinterpret_cast<const float *>(static_cast<const uint4 *>(base) + 3 * Vh);
+    }
+    __device__ static __forceinline__ void load(const void *base, long Vh, long h, cx<float> s[12]) {
+        const uint4 *p = static_cast<const uint4 *>(base) + h;
+        float n = ld_ro(norms(base, Vh) + h);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            uint4 v = ld_ro(p + k * Vh);
+            float2 a = Half2<PREC>::unpack(v.x), b = Half2<PREC>::unpack(v.y);
+            float2 c = Half2<PREC>::unpack(v.z), d = Half2<PREC>::unpack(v.w);
+            s[4 * k + 0] = {a.x * n, a.y * n};
+            s[4 * k + 1] = {b.x * n, b.y * n};
+            s[4 * k + 2] = {c.x * n, c.y * n};
+            s[4 * k + 3] = {d.x * n, d.y * n};
+        }
+    }
+    __device__ static __forceinline__ void store(void *base, long Vh, long h, const cx<float> s[12]) {
+        float m = 0.f;
+#pragma unroll
+        for (int c = 0; c < 12; c++) m = fmaxf(m, fmaxf(fabsf(s[c].re), fabsf(s[c].im)));
+        float inv = m > 0.f ? 1.f / m : 0.f;
+        uint4 *p = static_cast<uint4 *>(base) + h;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            uint4 v;
+            v.x = Half2<PREC>::pack(s[4 * k + 0].re * inv, s[4 * k + 0].im * inv);
+            v.y = Half2<PREC>::pack(s[4 * k + 1].re * inv, s[4 * k + 1].im * inv);
+            v.z = Half2<PREC>::pack(s[4 * k + 2].re * inv, s[4 * k + 2].im * inv);
+            v.w = Half2<PREC>::pack(s[4 * k + 3].re * inv, s[4 * k + 3].im * inv);
+            st_cs(p + k * Vh, v);
+        }
+        st_cs(const_cast<float *>(norms(base, Vh)) + h, m);
+    }
+};
+template <>
+struct SpinorIO<PLQCD_F16> : SpinorIO16<PLQCD_F16> {};
+template <>
+struct SpinorIO<PLQCD_BF16> : SpinorIO16<PLQCD_BF16> {};
+
+// =============================================================================
+// gauge storage: [parity][mu][element][Vh]
+// =============================================================================
+
+// row 2 of an SU(3) matrix from rows 0 and 1: conj(row0 x row1)
+template <typename R>
+__device__ __forceinline__ void reconstruct_row2(cx<R> U[9]) {
+    U[6] = cconj(csub(cmul(U[1], U[5]), cmul(U[2], U[4])));
+    U[7] = cconj(csub(cmul(U[2], U[3]), cmul(U[0], U[5])));
+    U[8] = cconj(csub(cmul(U[0], U[4]), cmul(U[1], U[3])));
+}
+
+template <int PREC, int RECON>
+struct LinkIO;
+
+template <>
+struct LinkIO<PLQCD_F64, 18> {
+    using real = double;
+    using elem = double2;
+    static constexpr int NE = 9;
+    __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
+                                                cx<double> U[9]) {
+        const double2 *p = static_cast<const double2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            double2 v = ld_ro(p + e * Vh);
+            U[e] = {v.x, v.y};
+        }
+    }
+    __device__ static __forceinline__ void store(void *base, long Vh, int par, int mu, long h,
+                                                 const cx<double> U[9]) {
+        double2 *p = static_cast<double2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 9; e++) p[e * Vh] = make_double2(U[e].re, U[e].im);
+    }
+};
+
+template <>
+struct LinkIO<PLQCD_F64, 12> {
+    using real = double;
+    using elem = double2;
+    static constexpr int NE = 6;
+    __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
+                                                cx<double> U[9]) {
+        const double2 *p = static_cast<const double2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            double2 v = ld_ro(p + e * Vh);
+            U[e] = {v.x, v.y};
+        }
+        reconstruct_row2(U);
+    }
+    __device__ static __forceinline__ void store(void *base, long Vh, int par, int mu, long h,
+                                                 const cx<double> U[9]) {
+        double2 *p = static_cast<double2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 6; e++) p[e * Vh] = make_double2(U[e].re, U[e].im);
+    }
+};
+
+template <>
+struct LinkIO<PLQCD_F32, 18> {
+    using real = float;
+    using elem = float2;
+    static constexpr int NE = 9;
+    __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
+                                                cx<float> U[9]) {
+        const float2 *p = static_cast<const float2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            float2 v = ld_ro(p + e * Vh);
+            U[e] = {v.x, v.y};
+        }
+    }
+    __device__ static __forceinline__ void store(void *base, long Vh, int par, int mu, long h,
+                                                 const cx<double> U[9]) {
+        float2 *p = static_cast<float2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 9; e++) p[e * Vh] = make_float2((float)U[e].re, (float)U[e].im);
+    }
+};
+
+template <>
+struct LinkIO<PLQCD_F32, 12> {
+    using real = float;
+    using elem = float4;
+    static constexpr int NE = 3;
+    __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
+                                                cx<float> U[9]) {
+        const float4 *p = static_cast<const float4 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            float4 v = ld_ro(p + e * Vh);
+            U[2 * e] = {v.x, v.y};
+            U[2 * e + 1] = {v.z, v.w};
+        }
+        reconstruct_row2(U);
+    }
+    __device__ static __forceinline__ void store(void *base, long Vh, int par, int mu, long h,
+                                                 const cx<double> U[9]) {
+        float4 *p = static_cast<float4 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 3; e++)
+            p[e * Vh] = make_float4((float)U[2 * e].re, (float)U[2 * e].im, (float)U[2 * e + 1].re,
+                                    (float)U[2 * e + 1].im);
+    }
+};
+
+// 16-bit links, rows 0,1 only. SU(3) entries satisfy |U_ij| <= 1, so no
+// scale factor is stored.
+template <int PREC>
+struct LinkIO16 {
+    using real = float;
+    using elem = uint2;
+    static constexpr int NE = 3;
+    __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
+                                                cx<float> U[9]) {
+        const uint2 *p = static_cast<const uint2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            uint2 v = ld_ro(p + e * Vh);
+            float2 a = Half2<PREC>::unpack(v.x), b = Half2<PREC>::unpack(v.y);
+            U[2 * e] = {a.x, a.y};
+            U[2 * e + 1] = {b.x, b.y};
+        }
+        reconstruct_row2(U);
+    }
+    __device__ static __forceinline__ void store(void *base, long Vh, int par, int mu, long h,
+                                                 const cx<double> U[9]) {
+        uint2 *p = static_cast<uint2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            uint2 v;
+            v.x = Half2<PREC>::pack((float)U[2 * e].re, (float)U[2 * e].im);
+            v.y = Half2<PREC>::pack((float)U[2 * e + 1].re, (float)U[2 * e + 1].im);
+            p[e * Vh] = v;
+        }
+    }
+};
+template <>
+struct LinkIO<PLQCD_F16, 12> : LinkIO16<PLQCD_F16> {};
+template <>
+struct LinkIO<PLQCD_BF16, 12> : LinkIO16<PLQCD_BF16> {};
+
+// ---- site coordinates of a half-site index ------------------------------------
+struct Coords {
+    int x, y, z, t;
+    long row;  // y + L1*(z + L2*t)
+};
+
+__device__ __forceinline__ Coords site_coords(long h, int par, int L0h, int L1, int L2) {
+    Coords c;
+    int xh = (int)(h % L0h);
+    c.row = h / L0h;
+    long r = c.row;
+    c.y = (int)(r % L1);
+    r /= L1;
+    c.z = (int)(r % L2);
+    c.t = (int)(r / L2);
+    c.x = 2 * xh + ((c.y + c.z + c.t + par) & 1);
+    return c;
+}
+
+}  // namespace dev
+}  // namespace plqcd

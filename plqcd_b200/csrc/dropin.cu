@@ -1,0 +1,214 @@
+// dropin.cu -- the reference's hopping entry points on host arrays
+// (include/dirac.h; reference lib/dirac.c:35-791).
+//
+// Each call copies the input parity of `qin` (API layout, host) to the
+// device, converts it to the kernel layout, runs the sm_100a hopping kernel
+// and copies the output parity back into `qout`; the other half of `qout` is
+// not touched, as in the reference. The gauge field is uploaded on first use
+// and kept on the device keyed by its host address plus a fingerprint of
+// 1024 sampled doubles; plqcd_gauge_update() or PLQCD_GAUGE_CACHE=0 force a
+// fresh upload. The return value is the call's wall-clock seconds
+// (lib/dirac.c:405-407), or -1 on failure with the reason in
+// plqcd_last_error(). Calls are serialised (the reference is not
+// re-entrant either: lib/dirac.c:12-13 and the global phip/phim buffers).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+#include "dirac.h"
+#include "internal.h"
+
+using namespace plqcd;
+
+namespace {
+
+struct DropIn {
+    int dims[4] = {0, 0, 0, 0};
+    plqcd_lattice *lat = nullptr;
+    plqcd_gauge *gauge = nullptr;
+    void *aos_in = nullptr, *aos_out = nullptr;  // API layout staging, one parity
+    void *f_in = nullptr, *f_out = nullptr;      // kernel layout (F64), one parity
+    const su3 *cached_u = nullptr;
+    uint64_t fingerprint = 0;
+    bool dirty = true;
+    cudaEvent_t k0 = nullptr, k1 = nullptr;
+    double kernel_ms = 0, h2d = 0, d2h = 0;
+};
+
+std::mutex g_mu;
+DropIn g_d;
+
+void release_locked() {
+    if (g_d.lat) cudaSetDevice(g_d.lat->device);
+    if (g_d.gauge) plqcd_gauge_destroy(g_d.gauge);
+    void *bufs[4] = {g_d.aos_in, g_d.aos_out, g_d.f_in, g_d.f_out};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (g_d.k0) cudaEventDestroy(g_d.k0);
+    if (g_d.k1) cudaEventDestroy(g_d.k1);
+    if (g_d.lat) plqcd_lattice_destroy(g_d.lat);
+    g_d = DropIn();
+}
+
+bool env_flag(const char *name, bool dflt) {
+    const char *v = getenv(name);
+    if (!v || !*v) return dflt;
+    return !(v[0] == '0' || v[0] == 'n' || v[0] == 'N' || v[0] == 'f' || v[0] == 'F');
+}
+
+uint64_t fingerprint(const su3 *u, long nlinks) {
+    const uint64_t *w = reinterpret_cast<const uint64_t *>(u);
+    long nwords = nlinks * 18;
+    uint64_t h = 1469598103934665603ULL;
+    const int samples = 1024;
+    for (int k = 0; k < samples; k++) {
+        long idx = (long)((double)k / samples * nwords);
+        h = (h ^ w[idx]) * 1099511628211ULL;
+    }
+    h = (h ^ w[nwords - 1]) * 1099511628211ULL;
+    return h;
+}
+
+int ensure_locked() {
+    if (!plqcd_g.init) return set_error(PLQCD_ERR_STATE, "hopping matrix called before init_plqcd");
+    const int *L = plqcd_g.latdims;
+    if (g_d.lat && memcmp(g_d.dims, L, sizeof g_d.dims) == 0) return PLQCD_OK;
+    release_locked();
+    int dev = 0;
+    if (const char *e = getenv("PLQCD_DEVICE")) dev = atoi(e);
+    PLQCD_TRY(plqcd_lattice_create(L, dev, nullptr, &g_d.lat));
+    memcpy(g_d.dims, L, sizeof g_d.dims);
+    int rc = plqcd_gauge_create(g_d.lat, PLQCD_F64, 18, &g_d.gauge);
+    if (rc != PLQCD_OK) {
+        release_locked();
+        return rc;
+    }
+    size_t bytes = spinor_parity_bytes(g_d.lat->geom.Vh, PLQCD_F64);
+    void **bufs[4] = {&g_d.aos_in, &g_d.aos_out, &g_d.f_in, &g_d.f_out};
+    for (void **b : bufs)
+        if (cudaMalloc(b, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            release_locked();
+            return set_error(PLQCD_ERR_NOMEM, "drop-in: device allocation of %zu bytes failed", bytes);
+        }
+    if (cudaEventCreate(&g_d.k0) != cudaSuccess || cudaEventCreate(&g_d.k1) != cudaSuccess) {
+        release_locked();
+        return set_error(PLQCD_ERR_CUDA, "drop-in: event creation failed");
+    }
+    g_d.dirty = true;
+    return PLQCD_OK;
+}
+
+// out_parity 0: eo (qout even half from qin odd half); 1: oe.
+double hop_call(spinor *qin, spinor *qout, su3 *u, int out_parity) {
+    double t0 = stop_watch(0.0);
+    clear_error();
+    if (!qin || !qout || !u) {
+        set_error(PLQCD_ERR_ARG, "hopping matrix: null argument");
+        return -1.0;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (ensure_locked() != PLQCD_OK) return -1.0;
+    plqcd_lattice *lat = g_d.lat;
+    const long Vh = lat->geom.Vh;
+    cudaStream_t s = lat->stream;
+    if (cudaSetDevice(lat->device) != cudaSuccess) {
+        set_error(PLQCD_ERR_CUDA, "hopping matrix: cudaSetDevice failed");
+        return -1.0;
+    }
+    g_d.h2d = g_d.d2h = 0;
+
+    // gauge field: upload when new, changed or caching is disabled
+    uint64_t fp = fingerprint(u, 8 * Vh);
+    if (!env_flag("PLQCD_GAUGE_CACHE", true) || g_d.dirty || g_d.cached_u != u || g_d.fingerprint != fp) {
+        if (plqcd_gauge_load_host(g_d.gauge, u) != PLQCD_OK) return -1.0;
+        g_d.cached_u = u;
+        g_d.fingerprint = fp;
+        g_d.dirty = false;
+        g_d.h2d += 8.0 * Vh * sizeof(su3);
+    }
+
+    const size_t bytes = (size_t)Vh * sizeof(spinor);
+    const int in_parity = out_parity ^ 1;
+    unsigned flags = env_flag("PLQCD_REF_COMPAT", false) ? PLQCD_DSLASH_COMPAT : 0u;
+    cudaError_t e = cudaMemcpyAsync(g_d.aos_in, qin + in_parity * Vh, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        set_error(PLQCD_ERR_CUDA, "hopping matrix: H2D copy: %s", cudaGetErrorString(e));
+        return -1.0;
+    }
+    g_d.h2d += (double)bytes;
+    // staging holds one parity, so it is addressed as parity 0
+    if (launch_spinor_import(lat->geom, s, g_d.aos_in, 0, g_d.f_in, PLQCD_F64) != PLQCD_OK) return -1.0;
+    cudaEventRecord(g_d.k0, s);
+    DslashCall c;
+    c.gauge = g_d.gauge->data;
+    c.prec = PLQCD_F64;
+    c.recon = 18;
+    c.out = g_d.f_out;
+    c.in = g_d.f_in;
+    c.out_parity = out_parity;
+    c.flags = flags;
+    if (launch_dslash(lat->geom, s, c) != PLQCD_OK) return -1.0;
+    cudaEventRecord(g_d.k1, s);
+    if (launch_spinor_export(lat->geom, s, g_d.f_out, PLQCD_F64, 0, g_d.aos_out) != PLQCD_OK) return -1.0;
+    e = cudaMemcpyAsync(qout + out_parity * Vh, g_d.aos_out, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error(PLQCD_ERR_CUDA, "hopping matrix: %s", cudaGetErrorString(e));
+        return -1.0;
+    }
+    g_d.d2h += (double)bytes;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, g_d.k0, g_d.k1);
+    g_d.kernel_ms = ms;
+    lat->last_kernel_ms = ms;
+    return stop_watch(t0);
+}
+
+}  // namespace
+
+namespace plqcd {
+void dropin_release() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    release_locked();
+}
+}  // namespace plqcd
+
+extern "C" int plqcd_gauge_update(const su3 *u) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    (void)u;
+    g_d.dirty = true;
+    return PLQCD_OK;
+}
+
+extern "C" int plqcd_dropin_last_stats(double *kernel_ms, double *h2d, double *d2h) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (kernel_ms) *kernel_ms = g_d.kernel_ms;
+    if (h2d) *h2d = g_d.h2d;
+    if (d2h) *d2h = g_d.d2h;
+    return PLQCD_OK;
+}
+
+// lib/dirac.c:35 and :414, plus the same-signature SSE3 names of
+// lib/dirac.c:801, 1272, 1748, 2124.
+extern "C" double plqcd_hopping_matrix_eo_sse3_assymbly(spinor *qin, spinor *qout, su3 *u) {
+    return hop_call(qin, qout, u, 0);
+}
+extern "C" double plqcd_hopping_matrix_oe_sse3_assymbly(spinor *qin, spinor *qout, su3 *u) {
+    return hop_call(qin, qout, u, 1);
+}
+extern "C" double plqcd_hopping_matrix_eo_sse3_intrin(spinor *qin, spinor *qout, su3 *u) {
+    return hop_call(qin, qout, u, 0);
+}
+extern "C" double plqcd_hopping_matrix_oe_sse3_intrin(spinor *qin, spinor *qout, su3 *u) {
+    return hop_call(qin, qout, u, 1);
+}
+extern "C" double plqcd_hopping_matrix_eo_sse3_intrin_blocking(spinor *qin, spinor *qout, su3 *u) {
+    return hop_call(qin, qout, u, 0);
+}
+extern "C" double plqcd_hopping_matrix_oe_sse3_intrin_blocking(spinor *qin, spinor *qout, su3 *u) {
+    return hop_call(qin, qout, u, 1);
+}

@@ -1,0 +1,112 @@
+// internal.h -- shared declarations of the plqcd-b200 library (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "plqcd_b200.h"
+
+namespace plqcd {
+
+// ---- error state (thread-local; read through plqcd_last_error) ----------
+int set_error(int code, const char *fmt, ...);
+void clear_error();
+
+#define PLQCD_CUDA_TRY(expr)                                                              \
+    do {                                                                                  \
+        cudaError_t _e = (expr);                                                          \
+        if (_e != cudaSuccess)                                                            \
+            return ::plqcd::set_error(PLQCD_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, \
+                                      #expr, cudaGetErrorString(_e));                     \
+    } while (0)
+
+#define PLQCD_TRY(expr)               \
+    do {                              \
+        int _s = (expr);              \
+        if (_s != PLQCD_OK) return _s; \
+    } while (0)
+
+// ---- geometry --------------------------------------------------------------
+struct Geom {
+    int L[4];
+    int L0h;     // L0 / 2
+    long Vh;     // V / 2
+};
+
+inline bool dims_ok(const int d[4]) {
+    for (int k = 0; k < 4; k++)
+        if (d[k] < 2 || (d[k] & 1)) return false;
+    return true;
+}
+
+// ---- element sizes / counts ------------------------------------------------
+// bytes of one parity of a spinor field
+size_t spinor_parity_bytes(long Vh, int prec);
+// number of stored "elements" (planes) per link and bytes per element
+int gauge_elems(int prec, int recon);
+size_t gauge_elem_bytes(int prec, int recon);
+size_t gauge_total_bytes(long Vh, int prec, int recon);
+bool gauge_format_ok(int prec, int recon);
+
+}  // namespace plqcd
+
+// ---- opaque objects ----------------------------------------------------------
+struct plqcd_lattice {
+    plqcd::Geom geom;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_kernel_ms = 0.0;
+    // reduction scratch (partials of dot products / norms)
+    double *red = nullptr;
+    size_t red_count = 0;
+    double *red_host = nullptr;  // pinned mirror of the final reduction results
+};
+
+struct plqcd_gauge {
+    plqcd_lattice *lat = nullptr;
+    int prec = PLQCD_F64;
+    int recon = 18;
+    void *data = nullptr;
+    size_t bytes = 0;
+};
+
+namespace plqcd {
+
+// ---- kernels (fields.cu) ------------------------------------------------------
+int launch_spinor_import(const Geom &g, cudaStream_t s, const void *aos, int parity, void *dst, int prec);
+int launch_spinor_export(const Geom &g, cudaStream_t s, const void *src, int prec, int parity, void *aos);
+int launch_spinor_convert(const Geom &g, cudaStream_t s, void *dst, int dprec, const void *src, int sprec);
+int launch_spinor_gaussian(const Geom &g, cudaStream_t s, void *dst, int prec, int parity, uint64_t seed);
+int launch_gauge_import(const Geom &g, cudaStream_t s, const void *aos, long first_link, long nlinks,
+                        void *dst, int prec, int recon);
+int launch_gauge_export(const Geom &g, cudaStream_t s, const void *src, int prec, int recon, void *aos);
+int launch_gauge_random(const Geom &g, cudaStream_t s, void *dst, int prec, int recon, uint64_t seed);
+int launch_gauge_unit(const Geom &g, cudaStream_t s, void *dst, int prec, int recon);
+int launch_gauge_copy(const Geom &g, cudaStream_t s, void *dst, int dprec, int drecon, const void *src,
+                      int sprec, int srecon);
+
+// ---- hopping kernels (dslash.cu) ---------------------------------------------
+struct DslashCall {
+    const void *gauge = nullptr;
+    int prec = PLQCD_F64;
+    int recon = 18;
+    void *out = nullptr;
+    const void *in = nullptr;
+    int out_parity = 0;
+    unsigned flags = 0;
+    // epilogue: out = a_up/a_low * H in + b * x   (x may be null)
+    double a_up = 1.0, a_low = 1.0, b = 0.0;
+    const void *x = nullptr;
+    // full-lattice mode
+    bool full = false;
+    void *out2 = nullptr;      // odd output in full mode (out = even output)
+    const void *in2 = nullptr; // odd input in full mode (in = even input)
+    int block = 0;             // 0 = library default
+};
+int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c);
+
+}  // namespace plqcd

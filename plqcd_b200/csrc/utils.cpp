@@ -1,0 +1,110 @@
+// utils.cpp -- aligned host allocation, timer and tags (include/utils.h).
+//
+// Same entry points as the reference's lib/utils.c:23-125. amalloc hands out
+// page-locked host memory when a CUDA device is usable, so fields that a
+// caller allocates with it (as tests/test_hopping.c:96-115 does) cross PCIe
+// at full speed in the drop-in hopping calls; otherwise it falls back to
+// ordinary aligned heap memory. A registry maps each aligned address back to
+// its allocation so afree can release it (and ignores unknown addresses, as
+// lib/utils.c:68-90 does).
+#include <cuda_runtime.h>
+#include <sys/time.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <unordered_map>
+
+#include "internal.h"
+#include "utils.h"
+
+namespace {
+
+struct Block {
+    void *base;
+    bool pinned;
+};
+
+std::mutex g_mu;
+std::unordered_map<uintptr_t, Block> &registry() {
+    static std::unordered_map<uintptr_t, Block> r;
+    return r;
+}
+
+bool pinned_allowed() {
+    static int allowed = -1;
+    if (allowed < 0) {
+        const char *env = getenv("PLQCD_PINNED_AMALLOC");
+        int n = 0;
+        allowed = (env && env[0] == '0') ? 0 : (cudaGetDeviceCount(&n) == cudaSuccess && n > 0);
+        if (!allowed) cudaGetLastError();
+    }
+    return allowed == 1;
+}
+
+}  // namespace
+
+extern "C" void *alloc(size_t size, size_t alignment) {
+    void *p = nullptr;
+    if (posix_memalign(&p, alignment, size) != 0 || !p) {
+        plqcd::set_error(PLQCD_ERR_NOMEM, "alloc() returned NULL. Out of memory?");
+        return nullptr;
+    }
+    return p;
+}
+
+extern "C" void *amalloc(size_t size, int p) {
+    if (size == 0 || p < 0 || p > 30) return nullptr;
+    size_t shift = (size_t)1 << p;
+    void *base = nullptr;
+    bool pinned = false;
+    if (pinned_allowed() && cudaHostAlloc(&base, size + shift, cudaHostAllocPortable) == cudaSuccess) {
+        pinned = true;
+    } else {
+        cudaGetLastError();
+        base = malloc(size + shift);
+        if (!base) return nullptr;
+    }
+    uintptr_t a = ((uintptr_t)base + shift) & ~(uintptr_t)(shift - 1);
+    std::lock_guard<std::mutex> lk(g_mu);
+    registry()[a] = Block{base, pinned};
+    return (void *)a;
+}
+
+extern "C" void afree(void *addr) {
+    Block b;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = registry().find((uintptr_t)addr);
+        if (it == registry().end()) return;
+        b = it->second;
+        registry().erase(it);
+    }
+    if (b.pinned)
+        cudaFreeHost(b.base);
+    else
+        free(b.base);
+}
+
+// Tag counters (lib/utils.c:6-9, 94-114).
+static const int kMaxTag = 32767;
+static const int kMaxPermanentTag = kMaxTag / 2;
+static int g_pcmn = -1, g_cmn = kMaxTag;
+
+extern "C" int mpi_permanent_tag(void) {
+    if (g_pcmn < kMaxPermanentTag) return ++g_pcmn;
+    plqcd::set_error(PLQCD_ERR_STATE, "mpi_permanent_tag: requested more than 16384 tags");
+    return -1;
+}
+
+extern "C" int mpi_tag(void) {
+    if (g_cmn == kMaxTag) g_cmn = kMaxPermanentTag;
+    return ++g_cmn;
+}
+
+extern "C" double stop_watch(double t) {
+    struct timeval tv;
+    gettimeofday(&tv, nullptr);
+    return (tv.tv_sec + tv.tv_usec * 1e-6) - t;
+}

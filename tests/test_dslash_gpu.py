@@ -1,0 +1,298 @@
+"""Parity of the sm_100a hopping kernels with the oracle, through the C-ABI.
+
+FP64 results must match the reference's operator to 1e-14 relative
+(max |diff| / max |value|); reduced precisions are bounded in relative L2
+against the FP64 kernel."""
+import os
+
+import numpy as np
+import pytest
+
+import plqcd_b200 as P
+from oracle import oracle as O
+from tests.gpu_util import dev_bytes, field_from_host, field_to_host, new_lattice, rel_l2, relmax, to_dev
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL64 = 1e-14
+
+
+@pytest.fixture
+def dropin(cuda):
+    paths = []
+
+    def init(L):
+        P.finalize_plqcd()
+        p = O.write_input_file(L)
+        paths.append(p)
+        assert P.init_plqcd(p) == 0, P.last_error()
+
+    yield init
+    P.finalize_plqcd()
+    os.environ.pop("PLQCD_REF_COMPAT", None)
+    for p in paths:
+        os.unlink(p)
+
+
+def test_dropin_golden_4x4x4x4(dropin):
+    g = np.load(os.path.join(GOLD, "hop_4x4x4x4.npz"))
+    L = tuple(g["L"])
+    dropin(L)
+    qout = np.zeros_like(g["qin"])
+    t1 = P.hopping_matrix("eo", g["qin"], qout, g["u"])
+    t2 = P.hopping_matrix("oe", g["qin"], qout, g["u"])
+    assert t1 > 0 and t2 > 0
+    assert relmax(qout, g["qout_patched"]) < TOL64
+
+
+def test_dropin_compat_reproduces_shipped_reference(dropin):
+    g = np.load(os.path.join(GOLD, "hop_4x4x4x4.npz"))
+    dropin(tuple(g["L"]))
+    os.environ["PLQCD_REF_COMPAT"] = "1"
+    qout = np.zeros_like(g["qin"])
+    P.hopping_matrix("eo", g["qin"], qout, g["u"])
+    P.hopping_matrix("oe", g["qin"], qout, g["u"])
+    assert relmax(qout, g["qout_shipped"]) < TOL64
+
+
+@pytest.mark.parametrize("L", [(8, 8, 8, 16), (4, 6, 8, 10), (6, 4, 4, 4), (16, 8, 4, 4)])
+@pytest.mark.parametrize("fill", ["su3", "uniform"])
+def test_dropin_matches_oracle(dropin, restatement, L, fill):
+    dropin(L)
+    V = O.volume(L)
+    rng = np.random.default_rng(11)
+    if fill == "su3":
+        q, u = O.gaussian_spinor(V, rng), O.random_su3(4 * V, rng)
+    else:  # the reference driver's fill: rand()/RAND_MAX, links not SU(3)
+        q, u = O.uniform_spinor(V, rng), O.uniform_spinor(4 * V, rng)[:, :9].copy()
+    want = restatement.hop("full", L, q, u)
+    got = np.full_like(q, np.nan)
+    P.hopping_matrix("eo", q, got, u, variant="sse3_intrin")
+    # only the even half is written by eo
+    assert np.isnan(got[V // 2:]).all() and not np.isnan(got[: V // 2]).any()
+    P.hopping_matrix("oe", q, got, u, variant="sse3_intrin_blocking")
+    assert relmax(got, want) < TOL64
+
+
+def test_dropin_gauge_cache_sees_in_place_update(dropin, restatement):
+    L = (4, 4, 4, 8)
+    dropin(L)
+    V = O.volume(L)
+    rng = np.random.default_rng(5)
+    q, u = O.gaussian_spinor(V, rng), O.random_su3(4 * V, rng)
+    out = np.zeros_like(q)
+    P.hopping_matrix("eo", q, out, u)
+    u[:] = O.random_su3(4 * V, rng)            # same address, new links
+    P.lib().plqcd_gauge_update(u.ctypes.data)
+    P.hopping_matrix("eo", q, out, u)
+    want = restatement.hop("eo", L, q, u)
+    assert relmax(out[: V // 2], want[: V // 2]) < TOL64
+
+
+def _device_setup(L, seed=1):
+    lat = new_lattice(L)
+    g64 = P.Gauge(lat, P.F64, 18)
+    g64.random(seed)
+    u = g64.store_host()
+    return lat, g64, u
+
+
+@pytest.mark.parametrize("L", [(4, 4, 4, 4), (8, 4, 6, 10), (16, 16, 16, 32)])
+@pytest.mark.parametrize("recon", [18, 12])
+def test_device_dslash_f64_matches_oracle(cuda, restatement, L, recon):
+    lat, g64, u = _device_setup(L)
+    g = g64 if recon == 18 else P.Gauge(lat, P.F64, 12)
+    if recon == 12:
+        g.copy_from(g64)
+    V = lat.V
+    q = O.gaussian_spinor(V, np.random.default_rng(2))
+    want = restatement.hop("full", L, q, u)
+    fe, fo = field_from_host(lat, q, 0, P.F64), field_from_host(lat, q, 1, P.F64)
+    oe_, oo_ = dev_bytes(lat.spinor_bytes(P.F64)), dev_bytes(lat.spinor_bytes(P.F64))
+    lat.dslash(g, oe_, fo, P.EVEN, P.F64)
+    lat.dslash(g, oo_, fe, P.ODD, P.F64)
+    got = field_to_host(lat, oe_, P.F64, 0)
+    got[V // 2:] = field_to_host(lat, oo_, P.F64, 1)[V // 2:]
+    # 12-real storage rebuilds row 2 in FP64: agreement at rounding level
+    assert relmax(got, want) < (TOL64 if recon == 18 else 1e-13)
+
+
+@pytest.mark.parametrize("L", [(4, 4, 4, 4), (8, 6, 4, 10)])
+def test_full_lattice_kernel_equals_two_halves(cuda, L):
+    lat, g64, u = _device_setup(L, 3)
+    bs = lat.spinor_bytes(P.F64)
+    fe, fo = dev_bytes(bs), dev_bytes(bs)
+    lat.spinor_gaussian(fe, P.F64, 0, 9)
+    lat.spinor_gaussian(fo, P.F64, 1, 9)
+    a_e, a_o, b_e, b_o = (dev_bytes(bs) for _ in range(4))
+    lat.dslash(g64, a_e, fo, 0, P.F64)
+    lat.dslash(g64, a_o, fe, 1, P.F64)
+    lat.dslash_full(g64, b_e, b_o, fe, fo, P.F64)
+    lat.synchronize()
+    assert bool((a_e == b_e).all()) and bool((a_o == b_o).all())
+
+
+@pytest.mark.parametrize("prec,recon,tol", [(P.F32, 18, 2e-6), (P.F32, 12, 3e-6), (P.F16, 12, 2e-3),
+                                            (P.BF16, 12, 1.5e-2)])
+def test_reduced_precision_error(cuda, prec, recon, tol):
+    L = (8, 8, 8, 16)
+    lat, g64, u = _device_setup(L, 4)
+    g = P.Gauge(lat, prec, recon)
+    g.copy_from(g64)
+    V = lat.V
+    q = O.gaussian_spinor(V, np.random.default_rng(8))
+    f64 = field_from_host(lat, q, 1, P.F64)
+    ref = dev_bytes(lat.spinor_bytes(P.F64))
+    lat.dslash(g64, ref, f64, 0, P.F64)
+    flo = dev_bytes(lat.spinor_bytes(prec))
+    lat.spinor_convert(flo, prec, f64, P.F64)
+    out = dev_bytes(lat.spinor_bytes(prec))
+    lat.dslash(g, out, flo, 0, prec)
+    want = field_to_host(lat, ref, P.F64, 0)[: V // 2]
+    got = field_to_host(lat, out, prec, 0)[: V // 2]
+    err = rel_l2(got, want)
+    assert err < tol, err
+
+
+def test_xpay_and_gamma5_flags(cuda, restatement):
+    L = (4, 4, 6, 8)
+    lat, g64, u = _device_setup(L, 6)
+    V = lat.V
+    rng = np.random.default_rng(12)
+    q, x = O.gaussian_spinor(V, rng), O.gaussian_spinor(V, rng)
+    g5 = np.array([1.0] * 6 + [-1.0] * 6)
+    fin = field_from_host(lat, q, 1, P.F64)
+    fx = field_from_host(lat, x, 0, P.F64)
+    out = dev_bytes(lat.spinor_bytes(P.F64))
+    a, b = -0.0144, 1.0
+    lat.dslash_xpay(g64, out, fin, 0, P.F64, a, fx, b, flags=P.DSLASH_G5_IN | P.DSLASH_G5_OUT)
+    got = field_to_host(lat, out, P.F64, 0)[: V // 2]
+    h = restatement.hop("eo", L, g5 * q, u)[: V // 2]
+    want = b * x[: V // 2] + a * (g5 * h)
+    assert relmax(got, want) < TOL64
+
+
+def test_point_source_kat_gpu(cuda, restatement):
+    L = (4, 4, 4, 6)
+    lat = new_lattice(L)
+    g = P.Gauge(lat, P.F64, 18)
+    g.unit()
+    V = lat.V
+    _, _, iup, idn = restatement.geometry(L)
+    src, s, c = V // 2 + 7, 3, 2  # an odd site
+    q = np.zeros((V, 12), complex)
+    q[src, 3 * s + c] = 1.0
+    fo = field_from_host(lat, q, 1, P.F64)
+    out = dev_bytes(lat.spinor_bytes(P.F64))
+    lat.dslash(g, out, fo, 0, P.F64)
+    got = field_to_host(lat, out, P.F64, 0)[: V // 2]
+    nz = set(np.nonzero(np.abs(got).sum(axis=1))[0])
+    assert nz == set(iup[src]) | set(idn[src])
+    gs = O.gamma_matrices()
+    for mu in range(4):
+        np.testing.assert_allclose(got[idn[src, mu]].reshape(4, 3)[:, c], (np.eye(4) - gs[mu])[:, s], atol=0)
+        np.testing.assert_allclose(got[iup[src, mu]].reshape(4, 3)[:, c], (np.eye(4) + gs[mu])[:, s], atol=0)
+
+
+def test_random_gauge_is_su3(cuda):
+    lat, g64, u = _device_setup((4, 4, 4, 8), 21)
+    U = u.reshape(-1, 3, 3)
+    eye = np.eye(3)
+    assert np.abs(np.einsum("nab,ncb->nac", U, U.conj()) - eye).max() < 1e-14
+    assert np.abs(np.linalg.det(U) - 1).max() < 1e-14
+    # a different seed gives different links; the same seed the same links
+    g2 = P.Gauge(lat, P.F64, 18)
+    g2.random(21)
+    assert np.array_equal(g2.store_host(), u)
+    g2.random(22)
+    assert not np.allclose(g2.store_host(), u)
+
+
+def test_gauge_and_spinor_roundtrips(cuda):
+    L = (4, 6, 4, 8)
+    lat = new_lattice(L)
+    V = lat.V
+    rng = np.random.default_rng(4)
+    u = O.random_su3(4 * V, rng)
+    g = P.Gauge(lat, P.F64, 18)
+    g.load_host(u)
+    assert np.array_equal(g.store_host(), u)
+    g12 = P.Gauge(lat, P.F64, 12)
+    g12.load_host(u)
+    np.testing.assert_allclose(g12.store_host(), u, atol=1e-15)
+    gd = P.Gauge(lat, P.F64, 18)
+    gd.load_device(to_dev(u))
+    assert np.array_equal(gd.store_host(), u)
+    q = O.gaussian_spinor(V, rng)
+    for par in (0, 1):
+        f = field_from_host(lat, q, par, P.F64)
+        back = field_to_host(lat, f, P.F64, par)
+        sl = slice(0, V // 2) if par == 0 else slice(V // 2, V)
+        assert np.array_equal(back[sl], q[sl])
+    f = field_from_host(lat, q, 0, P.F64)
+    for prec, tol in ((P.F32, 1e-7), (P.F16, 1e-3), (P.BF16, 8e-3)):
+        lo = dev_bytes(lat.spinor_bytes(prec))
+        lat.spinor_convert(lo, prec, f, P.F64)
+        back = field_to_host(lat, lo, prec, 0)[: V // 2]
+        assert rel_l2(back, q[: V // 2]) < tol
+
+
+def test_gamma5_hermiticity_and_gauge_covariance_large(cuda):
+    """Size-independent properties at 16^3x32 on device-generated fields:
+    <phi_e, H_eo psi_o> = <g5 H_oe g5 phi_e, psi_o>; and H transforms
+    covariantly under a random local SU(3) rotation."""
+    L = (16, 16, 16, 32)
+    lat, g64, u = _device_setup(L, 31)
+    V = lat.V
+    bs = lat.spinor_bytes(P.F64)
+    phi, psi = dev_bytes(bs), dev_bytes(bs)
+    lat.spinor_gaussian(phi, P.F64, 0, 1)
+    lat.spinor_gaussian(psi, P.F64, 1, 2)
+    a, b = dev_bytes(bs), dev_bytes(bs)
+    lat.dslash(g64, a, psi, 0, P.F64)                                     # H_eo psi
+    lat.dslash(g64, b, phi, 1, P.F64, flags=P.DSLASH_G5_IN | P.DSLASH_G5_OUT)  # g5 H_oe g5 phi
+    ph = field_to_host(lat, phi, P.F64, 0)[: V // 2]
+    ps = field_to_host(lat, psi, P.F64, 1)[V // 2:]
+    A = field_to_host(lat, a, P.F64, 0)[: V // 2]
+    B = field_to_host(lat, b, P.F64, 1)[V // 2:]
+    lhs, rhs = np.vdot(ph, A), np.vdot(B, ps)
+    assert abs(lhs - rhs) < 1e-12 * abs(lhs)
+
+    # gauge covariance: U'_mu(x) = G(x) U_mu(x) G(x+mu)^dag, psi' = G psi
+    from oracle.oracle import random_su3
+    rng = np.random.default_rng(5)
+    G = random_su3(V, rng).reshape(V, 3, 3)
+    R = O.Restatement()
+    _, _, iup, _ = R.geometry(L)
+    U = u.reshape(V, 4, 3, 3)
+    Up = np.einsum("nab,nmbc,nmdc->nmad", G, U, G[iup].conj()).reshape(4 * V, 9)
+    q = np.concatenate([ph, ps])
+    qp = np.einsum("nab,nsb->nsa", G, q.reshape(V, 4, 3)).reshape(V, 12)
+    gp = P.Gauge(lat, P.F64, 18)
+    gp.load_host(np.ascontiguousarray(Up))
+    fo = field_from_host(lat, qp, 1, P.F64)
+    out = dev_bytes(bs)
+    lat.dslash(gp, out, fo, 0, P.F64)
+    got = field_to_host(lat, out, P.F64, 0)[: V // 2]
+    want = np.einsum("nab,nsb->nsa", G[: V // 2], A.reshape(-1, 4, 3)).reshape(-1, 12)
+    assert relmax(got, want) < 1e-13
+
+
+def test_dropin_32x32x32x64_matches_oracle(dropin, restatement):
+    """The benchmark size, element-wise against the oracle (FP64, 1e-14)."""
+    L = (32, 32, 32, 64)
+    lat, g64, u = _device_setup(L, 1234)
+    V = lat.V
+    bs = lat.spinor_bytes(P.F64)
+    fe, fo = dev_bytes(bs), dev_bytes(bs)
+    lat.spinor_gaussian(fe, P.F64, 0, 77)
+    lat.spinor_gaussian(fo, P.F64, 1, 77)
+    q = field_to_host(lat, fe, P.F64, 0)
+    q[V // 2:] = field_to_host(lat, fo, P.F64, 1)[V // 2:]
+    del lat, g64, fe, fo
+    dropin(L)
+    got = np.zeros_like(q)
+    P.hopping_matrix("eo", q, got, u)
+    P.hopping_matrix("oe", q, got, u)
+    want = restatement.hop("full", L, q, u)
+    assert relmax(got, want) < TOL64
