@@ -80,9 +80,9 @@ const char *plqcd_version(void);
 /* ---- lattice context ---------------------------------------------------- */
 typedef struct plqcd_lattice plqcd_lattice;
 
-/* dims: L0..L3, each even and >= 2 (>= 4 for init_plqcd compatibility is
- * not required here). device: CUDA ordinal. stream: cudaStream_t or NULL
- * for a new non-blocking stream owned by the lattice. */
+/* dims: L0..L3, each even and >= 2. device: CUDA ordinal. stream: the
+ * cudaStream_t all work of this lattice is queued on (NULL = the device's
+ * default stream); the caller keeps ownership of the stream. */
 int plqcd_lattice_create(const int dims[4], int device, void *stream, plqcd_lattice **out);
 int plqcd_lattice_destroy(plqcd_lattice *lat);
 int plqcd_lattice_set_stream(plqcd_lattice *lat, void *stream);

@@ -46,14 +46,9 @@ extern "C" int plqcd_lattice_create(const int dims[4], int device, void *stream,
     lat->geom.L0h = dims[0] / 2;
     lat->geom.Vh = V / 2;
     lat->device = device;
-    cudaError_t e = cudaSuccess;
-    if (stream) {
-        lat->stream = (cudaStream_t)stream;
-    } else {
-        e = cudaStreamCreateWithFlags(&lat->stream, cudaStreamNonBlocking);
-        lat->own_stream = true;
-    }
-    if (e == cudaSuccess) e = cudaEventCreate(&lat->ev0);
+    // NULL selects the device's default stream, as everywhere in CUDA
+    lat->stream = (cudaStream_t)stream;
+    cudaError_t e = cudaEventCreate(&lat->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&lat->ev1);
     if (e != cudaSuccess) {
         plqcd_lattice_destroy(lat);
@@ -71,18 +66,13 @@ extern "C" int plqcd_lattice_destroy(plqcd_lattice *lat) {
     if (lat->red_host) cudaFreeHost(lat->red_host);
     if (lat->ev0) cudaEventDestroy(lat->ev0);
     if (lat->ev1) cudaEventDestroy(lat->ev1);
-    if (lat->own_stream && lat->stream) cudaStreamDestroy(lat->stream);
     delete lat;
     return PLQCD_OK;
 }
 
 extern "C" int plqcd_lattice_set_stream(plqcd_lattice *lat, void *stream) {
     PLQCD_TRY(check_lat(lat));
-    if (lat->own_stream && lat->stream) {
-        cudaStreamSynchronize(lat->stream);
-        cudaStreamDestroy(lat->stream);
-    }
-    lat->own_stream = false;
+    PLQCD_CUDA_TRY(cudaStreamSynchronize(lat->stream));
     lat->stream = (cudaStream_t)stream;
     return PLQCD_OK;
 }

@@ -35,6 +35,7 @@ struct DropIn {
     uint64_t fingerprint = 0;
     bool dirty = true;
     cudaEvent_t k0 = nullptr, k1 = nullptr;
+    cudaStream_t stream = nullptr;  // owned by the drop-in path
     double kernel_ms = 0, h2d = 0, d2h = 0;
 };
 
@@ -50,6 +51,7 @@ void release_locked() {
     if (g_d.k0) cudaEventDestroy(g_d.k0);
     if (g_d.k1) cudaEventDestroy(g_d.k1);
     if (g_d.lat) plqcd_lattice_destroy(g_d.lat);
+    if (g_d.stream) cudaStreamDestroy(g_d.stream);
     g_d = DropIn();
 }
 
@@ -79,7 +81,16 @@ int ensure_locked() {
     release_locked();
     int dev = 0;
     if (const char *e = getenv("PLQCD_DEVICE")) dev = atoi(e);
-    PLQCD_TRY(plqcd_lattice_create(L, dev, nullptr, &g_d.lat));
+    cudaStream_t stream = nullptr;
+    if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(PLQCD_ERR_CUDA, "drop-in: cannot create a stream on device %d", dev);
+    }
+    if (plqcd_lattice_create(L, dev, stream, &g_d.lat) != PLQCD_OK) {
+        cudaStreamDestroy(stream);
+        return plqcd_last_status();
+    }
+    g_d.stream = stream;
     memcpy(g_d.dims, L, sizeof g_d.dims);
     int rc = plqcd_gauge_create(g_d.lat, PLQCD_F64, 18, &g_d.gauge);
     if (rc != PLQCD_OK) {

@@ -20,6 +20,8 @@
 // is read from HBM once: 192 + 4*144 + 192 = 960 B per site.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "device_fields.cuh"
 #include "internal.h"
 
@@ -249,6 +251,15 @@ static int launch_pr(const Geom &g, cudaStream_t s, const DslashArgs &a, int blo
 
 }  // namespace dev
 
+static int default_block() {
+    static int b = -1;
+    if (b < 0) {
+        const char *e = getenv("PLQCD_DSLASH_BLOCK");
+        b = e ? atoi(e) : 128;
+    }
+    return b;
+}
+
 int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
     dev::DslashArgs a{};
     a.gauge = c.gauge;
@@ -277,7 +288,7 @@ int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
     const bool xpay = c.x != nullptr;
     if (c.full && (compat || xpay || (c.flags & (PLQCD_DSLASH_G5_IN | PLQCD_DSLASH_G5_OUT))))
         return set_error(PLQCD_ERR_ARG, "dslash_full: flags and xpay are not supported in full-lattice mode");
-    int block = c.block > 0 ? c.block : 128;
+    int block = c.block > 0 ? c.block : default_block();
     if (block % 32 || block > 256) return set_error(PLQCD_ERR_ARG, "dslash: block size %d invalid", block);
     switch (c.prec * 100 + c.recon) {
         case PLQCD_F64 * 100 + 18: return dev::launch_pr<PLQCD_F64, 18>(g, s, a, block, compat, xpay, c.full);

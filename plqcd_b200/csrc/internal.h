@@ -57,7 +57,6 @@ struct plqcd_lattice {
     plqcd::Geom geom;
     int device = 0;
     cudaStream_t stream = nullptr;
-    bool own_stream = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_kernel_ms = 0.0;
     // reduction scratch (partials of dot products / norms)
