@@ -142,6 +142,51 @@ int plqcd_dslash_xpay(plqcd_lattice *lat, const plqcd_gauge *g, void *out, const
 int plqcd_dslash_full(plqcd_lattice *lat, const plqcd_gauge *g, void *out_even, void *out_odd,
                       const void *in_even, const void *in_odd, int prec);
 
+/* ---- even/odd preconditioned Wilson solver ------------------------------ */
+/* D = 1 - kappa H. CG on Mhat^dag Mhat with Mhat = 1 - kappa^2 H_eo H_oe on
+ * even sites, x_o = b_o + kappa H_oe x_e. With a sloppy precision other
+ * than F64 the recursion runs in that precision and reliable updates (FP64
+ * defect correction of the solution and true residual) keep the result
+ * exact to `tol`. */
+typedef struct {
+    double kappa;     /* hopping parameter */
+    double tol;       /* target |b' - Mhat x_e| / |b'| (FP64 true residual) */
+    int max_iter;
+    int sloppy_prec;  /* PLQCD_F64, F32, F16 or BF16: precision of the inner operator */
+    double delta;     /* reliable update when |r| drops below delta * max|r| (mixed only) */
+    int verbose;
+} plqcd_cg_param;
+
+typedef struct {
+    int iterations;
+    int reliable_updates;
+    int converged;
+    double schur_residual;  /* |b' - Mhat x_e| / |b'| in FP64 */
+    double true_residual;   /* |b - D x| / |b| on the full lattice, FP64 */
+    double seconds;         /* device time of the whole solve */
+    double sloppy_hops;     /* half-lattice hopping applications in the sloppy precision */
+    double f64_hops;        /* ... and in FP64 */
+} plqcd_cg_info;
+
+void plqcd_cg_param_default(plqcd_cg_param *p);
+/* x and b are F64 device fields of each parity (x is overwritten). g_sloppy
+ * must have precision param->sloppy_prec (NULL: use g64). */
+int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const plqcd_gauge *g_sloppy, void *x_even,
+                    void *x_odd, const void *b_even, const void *b_odd, const plqcd_cg_param *param,
+                    plqcd_cg_info *info);
+
+/* ---- autotuner ---------------------------------------------------------- */
+/* Kernel launch configurations (load strategy, block size) are chosen by
+ * timing the candidates on first use per (kernel, format, lattice, GPU) and
+ * persisted as JSON lines in PLQCD_TUNE_FILE (default
+ * $HOME/.cache/plqcd_b200/tunecache.json). */
+int plqcd_tune_enable(int on);
+int plqcd_tune_clear(void);
+int plqcd_tune_save(const char *path);   /* NULL = default file */
+int plqcd_tune_load(const char *path);   /* NULL = default file */
+int plqcd_tune_count(void);
+int plqcd_tune_get(const char *key, int *variant, int *block, double *ms);
+
 /* ---- drop-in path controls ---------------------------------------------- */
 /* Mark the host gauge field `u` as changed (or a new field) so the next
  * drop-in call uploads it. */

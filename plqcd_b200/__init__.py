@@ -102,6 +102,12 @@ _SIGS = {
     "plqcd_dslash": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint]),
     "plqcd_dslash_xpay": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint, _d, _vp, _d]),
     "plqcd_dslash_full": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i]),
+    "plqcd_tune_enable": (_i, [_i]),
+    "plqcd_tune_clear": (_i, []),
+    "plqcd_tune_save": (_i, [ctypes.c_char_p]),
+    "plqcd_tune_load": (_i, [ctypes.c_char_p]),
+    "plqcd_tune_count": (_i, []),
+    "plqcd_tune_get": (_i, [ctypes.c_char_p, _ip, _ip, _dp]),
     "plqcd_gauge_update": (_i, [_vp]),
     "plqcd_dropin_last_stats": (_i, [_dp, _dp, _dp]),
 }
@@ -299,3 +305,45 @@ class Gauge:
 
     def copy_from(self, src: "Gauge"):
         check(lib().plqcd_gauge_copy(self.handle, src.handle))
+
+
+# ---------------------------------------------------------------------------
+# solver (include/plqcd_b200.h: plqcd_invert_cg)
+# ---------------------------------------------------------------------------
+
+class CgParam(ctypes.Structure):
+    _fields_ = [("kappa", ctypes.c_double), ("tol", ctypes.c_double), ("max_iter", ctypes.c_int),
+                ("sloppy_prec", ctypes.c_int), ("delta", ctypes.c_double), ("verbose", ctypes.c_int)]
+
+
+class CgInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("reliable_updates", ctypes.c_int), ("converged", ctypes.c_int),
+                ("schur_residual", ctypes.c_double), ("true_residual", ctypes.c_double),
+                ("seconds", ctypes.c_double), ("sloppy_hops", ctypes.c_double), ("f64_hops", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_SIGS.update({
+    "plqcd_cg_param_default": (None, [ctypes.POINTER(CgParam)]),
+    "plqcd_invert_cg": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(CgParam), ctypes.POINTER(CgInfo)]),
+})
+
+
+def cg_param(**kw) -> CgParam:
+    p = CgParam()
+    lib().plqcd_cg_param_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def invert_cg(lat: Lattice, g64: Gauge, g_sloppy: Gauge | None, x_even, x_odd, b_even, b_odd,
+              param: CgParam, raise_on_error: bool = True) -> CgInfo:
+    info = CgInfo()
+    rc = lib().plqcd_invert_cg(lat.handle, g64.handle, g_sloppy.handle if g_sloppy else None, _ptr(x_even),
+                               _ptr(x_odd), _ptr(b_even), _ptr(b_odd), ctypes.byref(param), ctypes.byref(info))
+    if rc != OK and raise_on_error:
+        raise PlqcdError(f"plqcd error {rc}: {last_error()}")
+    return info

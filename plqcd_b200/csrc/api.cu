@@ -62,8 +62,7 @@ extern "C" int plqcd_lattice_destroy(plqcd_lattice *lat) {
     if (!lat) return PLQCD_OK;
     cudaSetDevice(lat->device);
     if (lat->stream) cudaStreamSynchronize(lat->stream);
-    if (lat->red) cudaFree(lat->red);
-    if (lat->red_host) cudaFreeHost(lat->red_host);
+    if (lat->ws) cudaFree(lat->ws);
     if (lat->ev0) cudaEventDestroy(lat->ev0);
     if (lat->ev1) cudaEventDestroy(lat->ev1);
     delete lat;

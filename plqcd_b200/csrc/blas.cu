@@ -1,0 +1,272 @@
+// blas.cu -- vector kernels and deterministic FP64 reductions.
+//
+// Reductions accumulate in FP64 whatever the storage precision. Each block
+// writes its partial sum; the last block to arrive (atomic ticket) adds the
+// partials in a fixed order, so results do not depend on block scheduling,
+// and applies the solver-scalar update selected by RedOp.
+#include <cuda_runtime.h>
+
+#include "blas.cuh"
+#include "device_fields.cuh"
+
+namespace plqcd {
+
+size_t red_scratch_bytes() { return sizeof(double) * kMaxRedBlocks * 2 + 256 + sizeof(CgState); }
+
+RedScratch red_scratch_from(void *mem) {
+    RedScratch r;
+    char *p = static_cast<char *>(mem);
+    r.partials = reinterpret_cast<double *>(p);
+    r.counter = reinterpret_cast<unsigned *>(p + sizeof(double) * kMaxRedBlocks * 2);
+    r.state = reinterpret_cast<CgState *>(p + sizeof(double) * kMaxRedBlocks * 2 + 256);
+    return r;
+}
+
+namespace dev {
+
+inline int blas_grid(long n) {
+    long b = (n + kBlasBlock - 1) / kBlasBlock;
+    return (int)(b < kMaxRedBlocks ? b : kMaxRedBlocks);
+}
+
+__device__ __forceinline__ void apply_op(RedOp op, double sum, CgState *st) {
+    switch (op) {
+        case RED_AUX: st->aux = sum; break;
+        case RED_ALPHA:
+            st->pAp = sum;
+            st->alpha = sum > 0 ? st->rr / sum : 0.0;
+            break;
+        case RED_RR:
+            st->rr_old = st->rr;
+            st->rr = sum;
+            st->beta = st->rr_old > 0 ? sum / st->rr_old : 0.0;
+            break;
+        case RED_SR2: st->sr2 = sum; break;
+        case RED_RR_TRUE:
+            st->rr = sum;
+            st->beta = st->rr_old > 0 ? sum / st->rr_old : 0.0;
+            break;
+        case RED_RR_INIT:
+            st->rr = sum;
+            st->rr_old = sum;
+            break;
+    }
+}
+
+// Block-reduce v, publish the partial, and let the last block finish.
+__device__ void reduce_finish(double v, RedScratch r, RedOp op) {
+    __shared__ double warp_sums[kBlasBlock / 32];
+    __shared__ bool last;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) warp_sums[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) b += warp_sums[k];
+        r.partials[blockIdx.x] = b;
+        __threadfence();
+        unsigned ticket = atomicAdd(r.counter, 1u);
+        last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // fixed-order sum of the partials
+    double t = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) t += ((volatile double *)r.partials)[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    __syncthreads();
+    if (lane == 0) warp_sums[w] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) tot += warp_sums[k];
+        apply_op(op, tot, r.state);
+        *r.counter = 0;  // ready for the next reduction on this scratch
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ double norm2_site(const cx<R> v[12]) {
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < 12; k++) s += (double)v[k].re * v[k].re + (double)v[k].im * v[k].im;
+    return s;
+}
+
+template <int P>
+__global__ void __launch_bounds__(kBlasBlock) k_norm2(const void *x, long Vh, RedScratch r, RedOp op) {
+    using R = typename SpinorIO<P>::real;
+    double acc = 0;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<R> v[12];
+        SpinorIO<P>::load(x, Vh, h, v);
+        acc += norm2_site(v);
+    }
+    reduce_finish(acc, r, op);
+}
+
+// x_s (XP) += alpha p ; r_s (P) -= alpha Ap ; |r_s|^2
+template <int P, int XP>
+__global__ void __launch_bounds__(kBlasBlock) k_cg_update(void *xs, void *rs, const void *p, const void *Ap, long Vh,
+                                                          RedScratch r) {
+    using R = typename SpinorIO<P>::real;
+    using RX = typename SpinorIO<XP>::real;
+    const double alpha = r.state->alpha;
+    double acc = 0;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<R> pv[12], av[12], rv[12];
+        cx<RX> xv[12];
+        SpinorIO<P>::load(p, Vh, h, pv);
+        SpinorIO<P>::load(Ap, Vh, h, av);
+        SpinorIO<P>::load(rs, Vh, h, rv);
+        SpinorIO<XP>::load(xs, Vh, h, xv);
+        const R a = (R)alpha;
+        const RX ax = (RX)alpha;
+#pragma unroll
+        for (int k = 0; k < 12; k++) {
+            xv[k] = {fma(ax, (RX)pv[k].re, xv[k].re), fma(ax, (RX)pv[k].im, xv[k].im)};
+            rv[k] = {fma(-a, av[k].re, rv[k].re), fma(-a, av[k].im, rv[k].im)};
+        }
+        SpinorIO<XP>::store(xs, Vh, h, xv);
+        SpinorIO<P>::store(rs, Vh, h, rv);
+        acc += norm2_site(rv);
+    }
+    reduce_finish(acc, r, RED_RR);
+}
+
+// p = r + beta p
+template <int P>
+__global__ void __launch_bounds__(kBlasBlock) k_cg_p(void *p, const void *rs, long Vh, const CgState *st) {
+    using R = typename SpinorIO<P>::real;
+    const R beta = (R)st->beta;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<R> pv[12], rv[12];
+        SpinorIO<P>::load(p, Vh, h, pv);
+        SpinorIO<P>::load(rs, Vh, h, rv);
+#pragma unroll
+        for (int k = 0; k < 12; k++) pv[k] = {fma(beta, pv[k].re, rv[k].re), fma(beta, pv[k].im, rv[k].im)};
+        SpinorIO<P>::store(p, Vh, h, pv);
+    }
+}
+
+template <int XP>
+__global__ void __launch_bounds__(kBlasBlock) k_accum_zero(void *x64, void *xs, long Vh) {
+    using RX = typename SpinorIO<XP>::real;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<double> xv[12];
+        cx<RX> sv[12], z[12];
+        SpinorIO<PLQCD_F64>::load(x64, Vh, h, xv);
+        SpinorIO<XP>::load(xs, Vh, h, sv);
+#pragma unroll
+        for (int k = 0; k < 12; k++) {
+            xv[k] = {xv[k].re + (double)sv[k].re, xv[k].im + (double)sv[k].im};
+            z[k] = {RX(0), RX(0)};
+        }
+        SpinorIO<PLQCD_F64>::store(x64, Vh, h, xv);
+        SpinorIO<XP>::store(xs, Vh, h, z);
+    }
+}
+
+__global__ void __launch_bounds__(kBlasBlock) k_sub_norm2(void *out, const void *a, const void *b, long Vh,
+                                                          RedScratch r, RedOp op) {
+    double acc = 0;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<double> av[12], bv[12];
+        SpinorIO<PLQCD_F64>::load(a, Vh, h, av);
+        SpinorIO<PLQCD_F64>::load(b, Vh, h, bv);
+#pragma unroll
+        for (int k = 0; k < 12; k++) av[k] = csub(av[k], bv[k]);
+        SpinorIO<PLQCD_F64>::store(out, Vh, h, av);
+        acc += norm2_site(av);
+    }
+    reduce_finish(acc, r, op);
+}
+
+__global__ void __launch_bounds__(kBlasBlock) k_axpby64(double a, const void *x, double b, void *y, long Vh) {
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<double> xv[12], yv[12];
+        SpinorIO<PLQCD_F64>::load(x, Vh, h, xv);
+        SpinorIO<PLQCD_F64>::load(y, Vh, h, yv);
+#pragma unroll
+        for (int k = 0; k < 12; k++) yv[k] = {fma(a, xv[k].re, b * yv[k].re), fma(a, xv[k].im, b * yv[k].im)};
+        SpinorIO<PLQCD_F64>::store(y, Vh, h, yv);
+    }
+}
+
+}  // namespace dev
+
+#define BLAS_PREC_SWITCH(prec, F)                                                   \
+    switch (prec) {                                                                 \
+        case PLQCD_F64: F(PLQCD_F64); break;                                        \
+        case PLQCD_F32: F(PLQCD_F32); break;                                        \
+        case PLQCD_F16: F(PLQCD_F16); break;                                        \
+        case PLQCD_BF16: F(PLQCD_BF16); break;                                      \
+        default: return set_error(PLQCD_ERR_ARG, "blas: unknown precision %d", prec); \
+    }
+
+int blas_norm2(const Geom &g, cudaStream_t s, const void *x, int prec, const RedScratch &r, RedOp op) {
+    const int nb = dev::blas_grid(g.Vh);
+#define F(P) dev::k_norm2<P><<<nb, kBlasBlock, 0, s>>>(x, g.Vh, r, op)
+    BLAS_PREC_SWITCH(prec, F)
+#undef F
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int blas_cg_update(const Geom &g, cudaStream_t s, void *xs, int xprec, void *rs, const void *p, const void *Ap,
+                   int prec, const RedScratch &r) {
+    const int nb = dev::blas_grid(g.Vh);
+    if (xprec == PLQCD_F64) {
+#define F(P) dev::k_cg_update<P, PLQCD_F64><<<nb, kBlasBlock, 0, s>>>(xs, rs, p, Ap, g.Vh, r)
+        BLAS_PREC_SWITCH(prec, F)
+#undef F
+    } else if (xprec == PLQCD_F32) {
+#define F(P) dev::k_cg_update<P, PLQCD_F32><<<nb, kBlasBlock, 0, s>>>(xs, rs, p, Ap, g.Vh, r)
+        BLAS_PREC_SWITCH(prec, F)
+#undef F
+    } else {
+        return set_error(PLQCD_ERR_ARG, "blas_cg_update: solution accumulator must be F64 or F32");
+    }
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int blas_cg_p(const Geom &g, cudaStream_t s, void *p, const void *rs, int prec, const RedScratch &r) {
+    const int nb = dev::blas_grid(g.Vh);
+#define F(P) dev::k_cg_p<P><<<nb, kBlasBlock, 0, s>>>(p, rs, g.Vh, r.state)
+    BLAS_PREC_SWITCH(prec, F)
+#undef F
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int blas_accum_zero(const Geom &g, cudaStream_t s, void *x64, void *xs, int xprec) {
+    const int nb = dev::blas_grid(g.Vh);
+    if (xprec == PLQCD_F64)
+        dev::k_accum_zero<PLQCD_F64><<<nb, kBlasBlock, 0, s>>>(x64, xs, g.Vh);
+    else if (xprec == PLQCD_F32)
+        dev::k_accum_zero<PLQCD_F32><<<nb, kBlasBlock, 0, s>>>(x64, xs, g.Vh);
+    else
+        return set_error(PLQCD_ERR_ARG, "blas_accum_zero: accumulator must be F64 or F32");
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int blas_sub_norm2(const Geom &g, cudaStream_t s, void *out, const void *a, const void *b, const RedScratch &r,
+                   RedOp op) {
+    dev::k_sub_norm2<<<dev::blas_grid(g.Vh), kBlasBlock, 0, s>>>(out, a, b, g.Vh, r, op);
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int blas_axpby64(const Geom &g, cudaStream_t s, double a, const void *x, double b, void *y) {
+    dev::k_axpby64<<<dev::blas_grid(g.Vh), kBlasBlock, 0, s>>>(a, x, b, y, g.Vh);
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+}  // namespace plqcd

@@ -1,0 +1,61 @@
+// blas.cuh -- vector kernels and FP64 reductions for the solvers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace plqcd {
+
+// Solver scalars kept in device memory. Reductions finalise them on the
+// device (last block of the reducing kernel), so kernels read alpha / beta
+// from here and the host only needs them to steer the iteration.
+struct CgState {
+    double rr;       // |r_sloppy|^2 (iterated), or |r|^2 after a reliable update
+    double rr_old;   // previous rr
+    double pAp;      // <p, A p> = |Mhat p|^2
+    double alpha;    // rr / pAp
+    double beta;     // rr / rr_old
+    double sr2;      // |b' - Mhat x|^2 at the last reliable update (Schur residual)
+    double aux;      // last plain reduction result
+    double pad;
+};
+
+// Reduction scratch: per-block partials, the arrival counter of the
+// last-block pattern, and the CgState block.
+struct RedScratch {
+    double *partials = nullptr;  // kMaxRedBlocks * 2 doubles
+    unsigned *counter = nullptr;
+    CgState *state = nullptr;
+};
+constexpr int kMaxRedBlocks = 1184;  // 8 x 148 SMs
+constexpr int kBlasBlock = 256;
+size_t red_scratch_bytes();
+// carve a RedScratch out of `mem` (red_scratch_bytes(), zero-initialised)
+RedScratch red_scratch_from(void *mem);
+
+enum RedOp : int {
+    RED_AUX = 0,     // state.aux = sum
+    RED_ALPHA = 1,   // state.pAp = sum; state.alpha = state.rr / sum
+    RED_RR = 2,      // state.rr_old = state.rr; state.rr = sum; state.beta = sum / state.rr_old
+    RED_SR2 = 3,     // state.sr2 = sum
+    RED_RR_TRUE = 4, // state.rr = sum; state.beta = sum / state.rr_old (after a reliable update)
+    RED_RR_INIT = 5, // state.rr = state.rr_old = sum
+};
+
+// sum |x|^2 (FP64 accumulation); finalised by `op`
+int blas_norm2(const Geom &g, cudaStream_t s, const void *x, int prec, const RedScratch &r, RedOp op);
+// x_s += alpha p; r_s -= alpha Ap; sum |r_s|^2 -> RED_RR
+int blas_cg_update(const Geom &g, cudaStream_t s, void *xs, int xprec, void *rs, const void *p, const void *Ap,
+                   int prec, const RedScratch &r);
+// p = r + beta p
+int blas_cg_p(const Geom &g, cudaStream_t s, void *p, const void *rs, int prec, const RedScratch &r);
+// x64 += xs; xs = 0
+int blas_accum_zero(const Geom &g, cudaStream_t s, void *x64, void *xs, int xprec);
+// out64 = a64 - b64; sum |out|^2 -> op
+int blas_sub_norm2(const Geom &g, cudaStream_t s, void *out, const void *a, const void *b, const RedScratch &r,
+                   RedOp op);
+// y = a x + b y (F64 fields)
+int blas_axpby64(const Geom &g, cudaStream_t s, double a, const void *x, double b, void *y);
+
+}  // namespace plqcd

@@ -53,6 +53,30 @@ __device__ __forceinline__ void st_cs(uint4 *p, uint4 v) { __stcs(p, v); }
 __device__ __forceinline__ void st_cs(uint2 *p, uint2 v) { __stcs(p, v); }
 __device__ __forceinline__ void st_cs(float *p, float v) { __stcs(p, v); }
 
+// ---- asynchronous global->shared copies (cp.async, sm_80+) -------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+// 16 bytes, cached in L2 only
+__device__ __forceinline__ void cp_async16_cg(uint32_t s, const void *g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g) : "memory");
+}
+// 16 / 8 / 4 bytes, cached in L1 and L2
+__device__ __forceinline__ void cp_async16_ca(uint32_t s, const void *g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t s, const void *g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t s, const void *g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // ---- 16-bit pair packing ----------------------------------------------------
 template <int PREC>
 struct Half2;
@@ -102,6 +126,21 @@ struct SpinorIO<PLQCD_F64> {
 #pragma unroll
         for (int c = 0; c < 12; c++) st_cs(p + c * Vh, make_double2(s[c].re, s[c].im));
     }
+    // staged form: NSLOT 16-byte shared-memory slots per site, slot j of
+    // this thread at s0 + j*stride bytes
+    static constexpr int NSLOT = 12;
+    __device__ static __forceinline__ void issue(const void *base, long Vh, long h, uint32_t s0, int stride) {
+        const double2 *p = static_cast<const double2 *>(base) + h;
+#pragma unroll
+        for (int c = 0; c < 12; c++) cp_async16_ca(s0 + c * stride, p + c * Vh);
+    }
+    __device__ static __forceinline__ void load_staged(const uint4 *s0, int B, cx<double> s[12]) {
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            double2 v = *reinterpret_cast<const double2 *>(s0 + c * B);
+            s[c] = {v.x, v.y};
+        }
+    }
 };
 
 template <>
@@ -122,6 +161,20 @@ struct SpinorIO<PLQCD_F32> {
 #pragma unroll
         for (int k = 0; k < 6; k++)
             st_cs(p + k * Vh, make_float4(s[2 * k].re, s[2 * k].im, s[2 * k + 1].re, s[2 * k + 1].im));
+    }
+    static constexpr int NSLOT = 6;
+    __device__ static __forceinline__ void issue(const void *base, long Vh, long h, uint32_t s0, int stride) {
+        const float4 *p = static_cast<const float4 *>(base) + h;
+#pragma unroll
+        for (int k = 0; k < 6; k++) cp_async16_ca(s0 + k * stride, p + k * Vh);
+    }
+    __device__ static __forceinline__ void load_staged(const uint4 *s0, int B, cx<float> s[12]) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            float4 v = *reinterpret_cast<const float4 *>(s0 + k * B);
+            s[2 * k] = {v.x, v.y};
+            s[2 * k + 1] = {v.z, v.w};
+        }
     }
 };
 
@@ -165,6 +218,26 @@ struct SpinorIO16 {
         }
         st_cs(const_cast<float *>(norms(base, Vh)) + h, m);
     }
+    static constexpr int NSLOT = 4;  // 3 x 16 bytes of values, the norm in slot 3
+    __device__ static __forceinline__ void issue(const void *base, long Vh, long h, uint32_t s0, int stride) {
+        const uint4 *p = static_cast<const uint4 *>(base) + h;
+#pragma unroll
+        for (int k = 0; k < 3; k++) cp_async16_ca(s0 + k * stride, p + k * Vh);
+        cp_async4(s0 + 3 * stride, norms(base, Vh) + h);
+    }
+    __device__ static __forceinline__ void load_staged(const uint4 *s0, int B, cx<float> s[12]) {
+        const float n = *reinterpret_cast<const float *>(s0 + 3 * B);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            uint4 v = s0[k * B];
+            float2 a = Half2<PREC>::unpack(v.x), b = Half2<PREC>::unpack(v.y);
+            float2 c = Half2<PREC>::unpack(v.z), d = Half2<PREC>::unpack(v.w);
+            s[4 * k + 0] = {a.x * n, a.y * n};
+            s[4 * k + 1] = {b.x * n, b.y * n};
+            s[4 * k + 2] = {c.x * n, c.y * n};
+            s[4 * k + 3] = {d.x * n, d.y * n};
+        }
+    }
 };
 template <>
 struct SpinorIO<PLQCD_F16> : SpinorIO16<PLQCD_F16> {};
@@ -191,6 +264,20 @@ struct LinkIO<PLQCD_F64, 18> {
     using real = double;
     using elem = double2;
     static constexpr int NE = 9;
+    static constexpr int NSLOT = 9;
+    __device__ static __forceinline__ void issue(const void *base, long Vh, int par, int mu, long h, uint32_t s0,
+                                                 int stride) {
+        const double2 *p = static_cast<const double2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 9; e++) cp_async16_cg(s0 + e * stride, p + e * Vh);
+    }
+    __device__ static __forceinline__ void load_staged(const uint4 *s0, int B, cx<double> U[9]) {
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            double2 v = *reinterpret_cast<const double2 *>(s0 + e * B);
+            U[e] = {v.x, v.y};
+        }
+    }
     __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
                                                 cx<double> U[9]) {
         const double2 *p = static_cast<const double2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
@@ -213,6 +300,21 @@ struct LinkIO<PLQCD_F64, 12> {
     using real = double;
     using elem = double2;
     static constexpr int NE = 6;
+    static constexpr int NSLOT = 6;
+    __device__ static __forceinline__ void issue(const void *base, long Vh, int par, int mu, long h, uint32_t s0,
+                                                 int stride) {
+        const double2 *p = static_cast<const double2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 6; e++) cp_async16_cg(s0 + e * stride, p + e * Vh);
+    }
+    __device__ static __forceinline__ void load_staged(const uint4 *s0, int B, cx<double> U[9]) {
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            double2 v = *reinterpret_cast<const double2 *>(s0 + e * B);
+            U[e] = {v.x, v.y};
+        }
+        reconstruct_row2(U);
+    }
     __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
                                                 cx<double> U[9]) {
         const double2 *p = static_cast<const double2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
@@ -236,6 +338,20 @@ struct LinkIO<PLQCD_F32, 18> {
     using real = float;
     using elem = float2;
     static constexpr int NE = 9;
+    static constexpr int NSLOT = 9;
+    __device__ static __forceinline__ void issue(const void *base, long Vh, int par, int mu, long h, uint32_t s0,
+                                                 int stride) {
+        const float2 *p = static_cast<const float2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 9; e++) cp_async8(s0 + e * stride, p + e * Vh);
+    }
+    __device__ static __forceinline__ void load_staged(const uint4 *s0, int B, cx<float> U[9]) {
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            float2 v = *reinterpret_cast<const float2 *>(s0 + e * B);
+            U[e] = {v.x, v.y};
+        }
+    }
     __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
                                                 cx<float> U[9]) {
         const float2 *p = static_cast<const float2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
@@ -258,6 +374,22 @@ struct LinkIO<PLQCD_F32, 12> {
     using real = float;
     using elem = float4;
     static constexpr int NE = 3;
+    static constexpr int NSLOT = 3;
+    __device__ static __forceinline__ void issue(const void *base, long Vh, int par, int mu, long h, uint32_t s0,
+                                                 int stride) {
+        const float4 *p = static_cast<const float4 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 3; e++) cp_async16_cg(s0 + e * stride, p + e * Vh);
+    }
+    __device__ static __forceinline__ void load_staged(const uint4 *s0, int B, cx<float> U[9]) {
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            float4 v = *reinterpret_cast<const float4 *>(s0 + e * B);
+            U[2 * e] = {v.x, v.y};
+            U[2 * e + 1] = {v.z, v.w};
+        }
+        reconstruct_row2(U);
+    }
     __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
                                                 cx<float> U[9]) {
         const float4 *p = static_cast<const float4 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
@@ -286,6 +418,23 @@ struct LinkIO16 {
     using real = float;
     using elem = uint2;
     static constexpr int NE = 3;
+    static constexpr int NSLOT = 3;
+    __device__ static __forceinline__ void issue(const void *base, long Vh, int par, int mu, long h, uint32_t s0,
+                                                 int stride) {
+        const uint2 *p = static_cast<const uint2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;
+#pragma unroll
+        for (int e = 0; e < 3; e++) cp_async8(s0 + e * stride, p + e * Vh);
+    }
+    __device__ static __forceinline__ void load_staged(const uint4 *s0, int B, cx<float> U[9]) {
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            uint2 v = *reinterpret_cast<const uint2 *>(s0 + e * B);
+            float2 a = Half2<PREC>::unpack(v.x), b = Half2<PREC>::unpack(v.y);
+            U[2 * e] = {a.x, a.y};
+            U[2 * e + 1] = {b.x, b.y};
+        }
+        reconstruct_row2(U);
+    }
     __device__ static __forceinline__ void load(const void *base, long Vh, int par, int mu, long h,
                                                 cx<float> U[9]) {
         const uint2 *p = static_cast<const uint2 *>(base) + ((long)(par * 4 + mu) * NE) * Vh + h;

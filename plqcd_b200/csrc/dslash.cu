@@ -24,6 +24,7 @@
 
 #include "device_fields.cuh"
 #include "internal.h"
+#include "tune.h"
 
 namespace plqcd {
 namespace dev {
@@ -226,8 +227,163 @@ __global__ void __launch_bounds__(256) k_dslash(const DslashArgs a) {
     SIO::store(out, Vh, h, acc);
 }
 
+// Projection, SU(3) product and rebuild of one direction on data already in
+// registers.
+template <int MU, bool FWD, bool COMPAT, typename R>
+__device__ __forceinline__ void compute_dir(cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg_in) {
+    cx<R> h0[3], h1[3];
+    project<MU, R>(s, FWD ? sg_in : -sg_in, h0, h1);
+    cx<R> c0[3], c1[3];
+    if (FWD) {
+        su3_mul(U, h0, c0);
+        su3_mul(U, h1, c1);
+    } else {
+        su3_dag_mul(U, h0, c0);
+        su3_dag_mul(U, h1, c1);
+    }
+    accumulate<MU, FWD ? 1 : -1, !(COMPAT && FWD), R>(acc, c0, c1);
+}
+
+template <bool COMPAT, typename R>
+__device__ __forceinline__ void compute_dir_n(int d, cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg) {
+    // d is a compile-time constant after unrolling, so this switch folds
+    switch (d) {
+        case 0: compute_dir<0, true, COMPAT>(acc, s, U, sg); break;
+        case 1: compute_dir<1, true, COMPAT>(acc, s, U, sg); break;
+        case 2: compute_dir<2, true, COMPAT>(acc, s, U, sg); break;
+        case 3: compute_dir<3, true, COMPAT>(acc, s, U, sg); break;
+        case 4: compute_dir<0, false, COMPAT>(acc, s, U, sg); break;
+        case 5: compute_dir<1, false, COMPAT>(acc, s, U, sg); break;
+        case 6: compute_dir<2, false, COMPAT>(acc, s, U, sg); break;
+        default: compute_dir<3, false, COMPAT>(acc, s, U, sg); break;
+    }
+}
+
+// Pipelined variant: the neighbour spinor and link of each of the 8
+// directions are copied global->shared with cp.async, ST directions ahead of
+// the one being computed, into slots private to the thread (no block-level
+// synchronisation). The register file then only holds the direction being
+// computed, while ST directions' loads are in flight per thread.
+// Shared memory per block: ST * (spinor + link slots) * 16 bytes * blockDim.
+template <class SIO, class LIO, int ST, bool COMPAT, bool XPAY, bool FULL>
+__global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
+    using R = typename SIO::real;
+    extern __shared__ uint4 smem[];
+    constexpr int NS = SIO::NSLOT + LIO::NSLOT;
+    const int B = blockDim.x;
+    int par;
+    long h;
+    if (FULL) {
+        par = blockIdx.x & 1;
+        h = (long)(blockIdx.x >> 1) * B + threadIdx.x;
+    } else {
+        par = a.out_parity;
+        h = (long)blockIdx.x * B + threadIdx.x;
+    }
+    if (h >= a.Vh) return;  // no block-level barrier below
+    const void *in = (FULL && par == 0) ? a.in[1] : a.in[0];
+    void *out = (FULL && par == 1) ? a.out[1] : a.out[0];
+    const long Vh = a.Vh;
+    const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
+    const Coords c = site_coords(h, par, L0h, L1, L2);
+    const int xh = (int)(h - c.row * L0h);
+    const long L01 = L1, L012 = (long)L1 * L2;
+    const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
+    const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
+    long nb[8];
+    nb[0] = (xp >> 1) + L0h * c.row;
+    nb[1] = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
+    nb[2] = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
+    nb[3] = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
+    nb[4] = (xm >> 1) + L0h * c.row;
+    nb[5] = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
+    nb[6] = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
+    nb[7] = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
+    const int opp = par ^ 1;
+    const int fpar = (COMPAT && par == 1) ? 0 : par;
+
+    const int stride = B * 16;  // bytes between consecutive slots of one thread
+    const uint32_t s_thread = smem_addr(smem) + threadIdx.x * 16;
+    auto issue = [&](int d) {
+        const uint32_t s0 = s_thread + (uint32_t)((d % ST) * NS) * stride;
+        SIO::issue(in, Vh, nb[d], s0, stride);
+        if (d < 4)
+            LIO::issue(a.gauge, Vh, fpar, d, h, s0 + SIO::NSLOT * stride, stride);
+        else
+            LIO::issue(a.gauge, Vh, opp, d - 4, nb[d], s0 + SIO::NSLOT * stride, stride);
+    };
+#pragma unroll
+    for (int d = 0; d < ST; d++) {
+        issue(d);
+        cp_async_commit();
+    }
+    cx<R> acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = {R(0), R(0)};
+    const R sg = (R)a.g5_in;
+#pragma unroll
+    for (int d = 0; d < 8; d++) {
+        cp_async_wait<ST - 1>();
+        const uint4 *s0 = smem + threadIdx.x + (d % ST) * NS * B;
+        cx<R> s[12], U[9];
+        SIO::load_staged(s0, B, s);
+        LIO::load_staged(s0 + SIO::NSLOT * B, B, U);
+        compute_dir_n<COMPAT, R>(d, acc, s, U, sg);
+        // the slot just consumed is refilled only after its values were used
+        if (d + ST < 8) issue(d + ST);
+        cp_async_commit();
+    }
+
+    const R aup = (R)a.a_up, alow = (R)a.a_low;
+    if (XPAY) {
+        cx<R> xv[12];
+        SIO::load(a.x, Vh, h, xv);
+        const R b = (R)a.b;
+#pragma unroll
+        for (int k = 0; k < 12; k++) {
+            const R ak = k < 6 ? aup : alow;
+            acc[k] = {fma(ak, acc[k].re, b * xv[k].re), fma(ak, acc[k].im, b * xv[k].im)};
+        }
+    } else {
+#pragma unroll
+        for (int k = 6; k < 12; k++) acc[k] = {alow * acc[k].re, alow * acc[k].im};
+#pragma unroll
+        for (int k = 0; k < 6; k++) acc[k] = {aup * acc[k].re, aup * acc[k].im};
+    }
+    SIO::store(out, Vh, h, acc);
+}
+
+template <class SIO, class LIO, int ST, bool COMPAT, bool XPAY, bool FULL>
+static int launch_pipe(const Geom &g, cudaStream_t s, const DslashArgs &a, int block) {
+    long nblk = (g.Vh + block - 1) / block;
+    if (FULL) nblk *= 2;
+    constexpr int NS = SIO::NSLOT + LIO::NSLOT;
+    const size_t smem = (size_t)ST * NS * 16 * block;
+    auto k = k_dslash_pipe<SIO, LIO, ST, COMPAT, XPAY, FULL>;
+    static bool attr_set = false;  // per instantiation
+    if (!attr_set) {
+        PLQCD_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        attr_set = true;
+    }
+    if (smem > 227 * 1024) return set_error(PLQCD_ERR_ARG, "dslash: %zu bytes of shared memory requested", smem);
+    k<<<(unsigned)nblk, block, smem, s>>>(a);
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
 template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
-static int launch_t(const Geom &g, cudaStream_t s, const DslashArgs &a, int block) {
+static int launch_direct(const Geom &g, cudaStream_t s, const DslashArgs &a, int block);
+
+// variant 0: direct loads; 2, 3: cp.async pipeline of that depth
+template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
+static int launch_t(const Geom &g, cudaStream_t s, const DslashArgs &a, int variant, int block) {
+    if (variant == 2) return launch_pipe<SIO, LIO, 2, COMPAT, XPAY, FULL>(g, s, a, block);
+    if (variant == 3) return launch_pipe<SIO, LIO, 3, COMPAT, XPAY, FULL>(g, s, a, block);
+    return launch_direct<SIO, LIO, COMPAT, XPAY, FULL>(g, s, a, block);
+}
+
+template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
+static int launch_direct(const Geom &g, cudaStream_t s, const DslashArgs &a, int block) {
     long nblk = (g.Vh + block - 1) / block;
     if (FULL) nblk *= 2;
     k_dslash<SIO, LIO, COMPAT, XPAY, FULL><<<(unsigned)nblk, block, 0, s>>>(a);
@@ -236,29 +392,28 @@ static int launch_t(const Geom &g, cudaStream_t s, const DslashArgs &a, int bloc
 }
 
 template <int PREC, int RECON>
-static int launch_pr(const Geom &g, cudaStream_t s, const DslashArgs &a, int block, bool compat, bool xpay,
-                     bool full) {
+static int launch_pr(const Geom &g, cudaStream_t s, const DslashArgs &a, int variant, int block, bool compat,
+                     bool xpay, bool full) {
     using S = SpinorIO<PREC>;
     using L = LinkIO<PREC, RECON>;
-    if (full) return launch_t<S, L, false, false, true>(g, s, a, block);
+    if (full) return launch_t<S, L, false, false, true>(g, s, a, variant, block);
     if (compat) {
-        if (PREC == PLQCD_F64 && RECON == 18) return launch_t<S, L, true, false, false>(g, s, a, block);
+        if (PREC == PLQCD_F64 && RECON == 18) return launch_t<S, L, true, false, false>(g, s, a, variant, block);
         return set_error(PLQCD_ERR_ARG, "dslash: the bug-compatible mode exists for F64 18-real links only");
     }
-    if (xpay) return launch_t<S, L, false, true, false>(g, s, a, block);
-    return launch_t<S, L, false, false, false>(g, s, a, block);
+    if (xpay) return launch_t<S, L, false, true, false>(g, s, a, variant, block);
+    return launch_t<S, L, false, false, false>(g, s, a, variant, block);
 }
 
 }  // namespace dev
 
-static int default_block() {
-    static int b = -1;
-    if (b < 0) {
-        const char *e = getenv("PLQCD_DSLASH_BLOCK");
-        b = e ? atoi(e) : 128;
-    }
-    return b;
+static int env_int(const char *name, int dflt) {
+    const char *e = getenv(name);
+    return e ? atoi(e) : dflt;
 }
+
+static int dispatch(const Geom &g, cudaStream_t s, const DslashCall &c, const dev::DslashArgs &a, int variant,
+                    int block);
 
 int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
     dev::DslashArgs a{};
@@ -285,18 +440,64 @@ int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
     a.b = c.b;
     a.g5_in = (c.flags & PLQCD_DSLASH_G5_IN) ? -1.0 : 1.0;
     const bool compat = (c.flags & PLQCD_DSLASH_COMPAT) != 0;
-    const bool xpay = c.x != nullptr;
-    if (c.full && (compat || xpay || (c.flags & (PLQCD_DSLASH_G5_IN | PLQCD_DSLASH_G5_OUT))))
+    if (c.full && (compat || c.x || (c.flags & (PLQCD_DSLASH_G5_IN | PLQCD_DSLASH_G5_OUT))))
         return set_error(PLQCD_ERR_ARG, "dslash_full: flags and xpay are not supported in full-lattice mode");
-    int block = c.block > 0 ? c.block : default_block();
-    if (block % 32 || block > 256) return set_error(PLQCD_ERR_ARG, "dslash: block size %d invalid", block);
+
+    // explicit configuration (block from the call, or the environment for
+    // experiments) bypasses the tuner
+    const int env_block = env_int("PLQCD_DSLASH_BLOCK", 0), env_var = env_int("PLQCD_DSLASH_STAGES", -1);
+    if (c.block > 0 || env_block > 0 || env_var >= 0) {
+        int block = c.block > 0 ? c.block : (env_block > 0 ? env_block : 128);
+        return dispatch(g, s, c, a, env_var >= 0 ? env_var : 2, block);
+    }
+    char key[256];
+    snprintf(key, sizeof key, "%sdslash|p%d|r%d|%s%s%s|%dx%dx%dx%d", device_tag().c_str(), c.prec, c.recon,
+             c.full ? "full" : "half", c.x ? "+xpay" : "", compat ? "+compat" : "", g.L[0], g.L[1], g.L[2], g.L[3]);
+    std::vector<TuneResult> cands;
+    for (int v : {2, 0, 3})
+        for (int b : {64, 128, 256}) {
+            TuneResult r;
+            r.variant = v;
+            r.block = b;
+            cands.push_back(r);
+        }
+    // trial launches write into scratch outputs: an xpay whose output aliases
+    // its x operand must not be applied more than once
+    void *scratch[2] = {nullptr, nullptr};
+    auto run = [&](const TuneResult &r, bool trial) -> int {
+        if (!trial) return dispatch(g, s, c, a, r.variant, r.block);
+        size_t bytes = spinor_parity_bytes(g.Vh, c.prec);
+        for (int k = 0; k < (c.full ? 2 : 1); k++)
+            if (!scratch[k] && cudaMalloc(&scratch[k], bytes) != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(PLQCD_ERR_NOMEM, "tune: scratch allocation failed");
+            }
+        dev::DslashArgs t = a;
+        t.out[0] = scratch[0];
+        if (c.full) t.out[1] = scratch[1];
+        return dispatch(g, s, c, t, r.variant, r.block);
+    };
+    int rc = tune_launch(key, s, cands, run);
+    for (void *p : scratch)
+        if (p) {
+            cudaStreamSynchronize(s);
+            cudaFree(p);
+        }
+    return rc;
+}
+
+static int dispatch(const Geom &g, cudaStream_t s, const DslashCall &c, const dev::DslashArgs &a, int variant,
+                    int block) {
+    const bool compat = (c.flags & PLQCD_DSLASH_COMPAT) != 0;
+    const bool xpay = c.x != nullptr;
+    if (block % 32 || block < 32 || block > 256) return set_error(PLQCD_ERR_ARG, "dslash: block size %d invalid", block);
     switch (c.prec * 100 + c.recon) {
-        case PLQCD_F64 * 100 + 18: return dev::launch_pr<PLQCD_F64, 18>(g, s, a, block, compat, xpay, c.full);
-        case PLQCD_F64 * 100 + 12: return dev::launch_pr<PLQCD_F64, 12>(g, s, a, block, compat, xpay, c.full);
-        case PLQCD_F32 * 100 + 18: return dev::launch_pr<PLQCD_F32, 18>(g, s, a, block, compat, xpay, c.full);
-        case PLQCD_F32 * 100 + 12: return dev::launch_pr<PLQCD_F32, 12>(g, s, a, block, compat, xpay, c.full);
-        case PLQCD_F16 * 100 + 12: return dev::launch_pr<PLQCD_F16, 12>(g, s, a, block, compat, xpay, c.full);
-        case PLQCD_BF16 * 100 + 12: return dev::launch_pr<PLQCD_BF16, 12>(g, s, a, block, compat, xpay, c.full);
+        case PLQCD_F64 * 100 + 18: return dev::launch_pr<PLQCD_F64, 18>(g, s, a, variant, block, compat, xpay, c.full);
+        case PLQCD_F64 * 100 + 12: return dev::launch_pr<PLQCD_F64, 12>(g, s, a, variant, block, compat, xpay, c.full);
+        case PLQCD_F32 * 100 + 18: return dev::launch_pr<PLQCD_F32, 18>(g, s, a, variant, block, compat, xpay, c.full);
+        case PLQCD_F32 * 100 + 12: return dev::launch_pr<PLQCD_F32, 12>(g, s, a, variant, block, compat, xpay, c.full);
+        case PLQCD_F16 * 100 + 12: return dev::launch_pr<PLQCD_F16, 12>(g, s, a, variant, block, compat, xpay, c.full);
+        case PLQCD_BF16 * 100 + 12: return dev::launch_pr<PLQCD_BF16, 12>(g, s, a, variant, block, compat, xpay, c.full);
         default:
             return set_error(PLQCD_ERR_ARG, "dslash: unsupported precision/reconstruction %d/%d", c.prec, c.recon);
     }

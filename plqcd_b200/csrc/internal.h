@@ -59,10 +59,9 @@ struct plqcd_lattice {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_kernel_ms = 0.0;
-    // reduction scratch (partials of dot products / norms)
-    double *red = nullptr;
-    size_t red_count = 0;
-    double *red_host = nullptr;  // pinned mirror of the final reduction results
+    // solver workspace (grown on demand, released with the lattice)
+    void *ws = nullptr;
+    size_t ws_bytes = 0;
 };
 
 struct plqcd_gauge {
@@ -107,5 +106,8 @@ struct DslashCall {
     int block = 0;             // 0 = library default
 };
 int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c);
+
+// device workspace of at least `bytes`, owned by the lattice (cg.cu)
+int lattice_workspace(plqcd_lattice *lat, size_t bytes, void **out);
 
 }  // namespace plqcd

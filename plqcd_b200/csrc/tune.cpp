@@ -1,0 +1,220 @@
+// tune.cpp -- launch-configuration autotuner with a persistent JSON cache.
+//
+// A kernel family registers a key (kernel name, storage format, flags,
+// lattice extents) and a list of candidate configurations (load strategy and
+// block size). The first launch with an unknown key times every candidate
+// with CUDA events on the caller's stream, writing into scratch outputs, and
+// keeps the fastest; later launches look it up. Results persist across
+// processes in a JSON file (PLQCD_TUNE_FILE, default
+// $HOME/.cache/plqcd_b200/tunecache.json), one object per line:
+//   {"key": "...", "variant": V, "block": B, "ms": T}
+// Tuning is skipped (the first candidate is used) while the stream is being
+// captured into a CUDA graph, or when PLQCD_TUNE=0.
+#include <cuda_runtime.h>
+#include <sys/stat.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "internal.h"
+#include "tune.h"
+
+namespace plqcd {
+
+namespace {
+
+std::mutex g_mu;
+std::map<std::string, TuneResult> &cache() {
+    static std::map<std::string, TuneResult> c;
+    return c;
+}
+bool g_loaded = false;
+int g_enabled = -1;
+
+std::string default_path() {
+    if (const char *p = getenv("PLQCD_TUNE_FILE")) return p;
+    const char *home = getenv("HOME");
+    std::string dir = std::string(home ? home : "/tmp") + "/.cache/plqcd_b200";
+    return dir + "/tunecache.json";
+}
+
+void mkdirs(const std::string &path) {
+    for (size_t i = 1; i < path.size(); i++)
+        if (path[i] == '/') mkdir(path.substr(0, i).c_str(), 0755);
+}
+
+void load_locked(const std::string &path) {
+    FILE *f = fopen(path.c_str(), "r");
+    if (!f) return;
+    char line[1024];
+    while (fgets(line, sizeof line, f)) {
+        char key[512];
+        TuneResult r;
+        if (sscanf(line, " {\"key\": \"%511[^\"]\", \"variant\": %d, \"block\": %d, \"ms\": %lf}", key, &r.variant,
+                   &r.block, &r.ms) == 4)
+            cache()[key] = r;
+    }
+    fclose(f);
+}
+
+void save_locked(const std::string &path) {
+    mkdirs(path);
+    std::string tmp = path + ".tmp." + std::to_string((long)getpid());
+    FILE *f = fopen(tmp.c_str(), "w");
+    if (!f) return;
+    for (auto &kv : cache())
+        fprintf(f, "{\"key\": \"%s\", \"variant\": %d, \"block\": %d, \"ms\": %.6f}\n", kv.first.c_str(),
+                kv.second.variant, kv.second.block, kv.second.ms);
+    fclose(f);
+    rename(tmp.c_str(), path.c_str());
+}
+
+void ensure_loaded_locked() {
+    if (!g_loaded) {
+        load_locked(default_path());
+        g_loaded = true;
+    }
+}
+
+}  // namespace
+
+bool tune_enabled() {
+    if (g_enabled < 0) {
+        const char *e = getenv("PLQCD_TUNE");
+        g_enabled = !(e && e[0] == '0');
+    }
+    return g_enabled == 1;
+}
+
+const std::string &device_tag() {
+    static thread_local std::string tag;
+    static thread_local int dev = -1;
+    int d = 0;
+    cudaGetDevice(&d);
+    if (d != dev) {
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, d) == cudaSuccess)
+            tag = std::string(p.name) + "/" + std::to_string(p.multiProcessorCount) + "|";
+        else
+            tag = "unknown|";
+        dev = d;
+    }
+    return tag;
+}
+
+// Look up or tune. `run(config, trial)` launches one candidate on `s` and
+// returns a status; the first candidate is the fallback.
+int tune_launch(const std::string &key, cudaStream_t s, const std::vector<TuneResult> &cands,
+                const std::function<int(const TuneResult &, bool)> &run) {
+    if (cands.empty()) return set_error(PLQCD_ERR_ARG, "tune: no candidates for %s", key.c_str());
+    TuneResult chosen = cands[0];
+    bool found = false;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        ensure_loaded_locked();
+        auto it = cache().find(key);
+        if (it != cache().end()) {
+            chosen = it->second;
+            found = true;
+        }
+    }
+    if (found || !tune_enabled()) return run(chosen, false);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return run(chosen, false);
+
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        return run(chosen, false);
+    }
+    double best = 1e30;
+    TuneResult bestc = cands[0];
+    for (const TuneResult &c : cands) {
+        if (run(c, true) != PLQCD_OK) {  // infeasible candidate (e.g. shared memory)
+            clear_error();
+            cudaGetLastError();
+            continue;
+        }
+        const int reps = 3;
+        cudaEventRecord(e0, s);
+        int rc = PLQCD_OK;
+        for (int r = 0; r < reps && rc == PLQCD_OK; r++) rc = run(c, true);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess || rc != PLQCD_OK) {
+            clear_error();
+            cudaGetLastError();
+            continue;
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= reps;
+        if (ms < best) {
+            best = ms;
+            bestc = c;
+            bestc.ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        cache()[key] = bestc;
+        save_locked(default_path());
+    }
+    return run(bestc, false);
+}
+
+bool tune_lookup(const std::string &key, TuneResult *out) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ensure_loaded_locked();
+    auto it = cache().find(key);
+    if (it == cache().end()) return false;
+    if (out) *out = it->second;
+    return true;
+}
+
+}  // namespace plqcd
+
+extern "C" int plqcd_tune_enable(int on) {
+    plqcd::g_enabled = on ? 1 : 0;
+    return PLQCD_OK;
+}
+
+extern "C" int plqcd_tune_clear(void) {
+    std::lock_guard<std::mutex> lk(plqcd::g_mu);
+    plqcd::cache().clear();
+    plqcd::g_loaded = true;  // do not reload the file
+    return PLQCD_OK;
+}
+
+extern "C" int plqcd_tune_save(const char *path) {
+    std::lock_guard<std::mutex> lk(plqcd::g_mu);
+    plqcd::save_locked(path ? path : plqcd::default_path());
+    return PLQCD_OK;
+}
+
+extern "C" int plqcd_tune_load(const char *path) {
+    std::lock_guard<std::mutex> lk(plqcd::g_mu);
+    plqcd::load_locked(path ? path : plqcd::default_path());
+    plqcd::g_loaded = true;
+    return PLQCD_OK;
+}
+
+extern "C" int plqcd_tune_count(void) {
+    std::lock_guard<std::mutex> lk(plqcd::g_mu);
+    plqcd::ensure_loaded_locked();
+    return (int)plqcd::cache().size();
+}
+
+extern "C" int plqcd_tune_get(const char *key, int *variant, int *block, double *ms) {
+    plqcd::TuneResult r;
+    if (!key || !plqcd::tune_lookup(key, &r)) return plqcd::set_error(PLQCD_ERR_ARG, "tune: no entry for key");
+    if (variant) *variant = r.variant;
+    if (block) *block = r.block;
+    if (ms) *ms = r.ms;
+    return PLQCD_OK;
+}
