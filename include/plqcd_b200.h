@@ -127,6 +127,13 @@ int plqcd_spinor_convert(plqcd_lattice *lat, void *dst, int dst_prec, const void
 /* Gaussian N(0,1) complex components, keyed by (seed, parity, site). */
 int plqcd_spinor_gaussian(plqcd_lattice *lat, void *dst, int prec, int parity, uint64_t seed);
 
+/* |x_f|^2 (FP64 accumulation, fixed summation order) of `nfields` one-parity
+ * fields stored back to back in `fields`; results go to the device array
+ * norms_dev[nfields], asynchronously on the lattice stream. Scratch for the
+ * per-block partial sums comes from the lattice's device workspace
+ * (allocated with cudaMalloc on first use or growth). */
+int plqcd_spinor_norm2(plqcd_lattice *lat, const void *fields, int prec, int nfields, double *norms_dev);
+
 /* ---- hopping matrix on device fields ------------------------------------ */
 /* out (parity out_parity) = a * H in (in on the other parity) [+ b * x]
  * where a applies to spins 0,1 and a_low to spins 2,3 (gamma5 folding),

@@ -99,6 +99,7 @@ _SIGS = {
     "plqcd_spinor_export": (_i, [_vp, _vp, _i, _i, _vp]),
     "plqcd_spinor_convert": (_i, [_vp, _vp, _i, _vp, _i]),
     "plqcd_spinor_gaussian": (_i, [_vp, _vp, _i, _i, _u64]),
+    "plqcd_spinor_norm2": (_i, [_vp, _vp, _i, _i, _vp]),
     "plqcd_dslash": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint]),
     "plqcd_dslash_xpay": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint, _d, _vp, _d]),
     "plqcd_dslash_full": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i]),
@@ -241,6 +242,9 @@ class Lattice:
 
     def spinor_convert(self, dst, dprec: int, src, sprec: int):
         check(lib().plqcd_spinor_convert(self.handle, _ptr(dst), dprec, _ptr(src), sprec))
+
+    def spinor_norm2(self, fields, prec: int, nfields: int, out_dev):
+        check(lib().plqcd_spinor_norm2(self.handle, _ptr(fields), prec, nfields, _ptr(out_dev)))
 
     def spinor_gaussian(self, dst, prec: int, parity: int, seed: int):
         check(lib().plqcd_spinor_gaussian(self.handle, _ptr(dst), prec, parity, seed))

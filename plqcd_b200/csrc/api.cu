@@ -315,3 +315,24 @@ extern "C" int plqcd_dslash_full(plqcd_lattice *lat, const plqcd_gauge *g, void 
     c.in2 = in_odd;
     return launch_dslash(lat->geom, lat->stream, c);
 }
+
+// ---- norms ----------------------------------------------------------------------
+
+#include "blas.cuh"
+
+extern "C" int plqcd_spinor_norm2(plqcd_lattice *lat, const void *fields, int prec, int nfields, double *norms_dev) {
+    clear_error();
+    PLQCD_TRY(check_lat(lat));
+    PLQCD_TRY(check_prec(prec));
+    if (!fields || !norms_dev || nfields < 1 || nfields > 65535)
+        return set_error(PLQCD_ERR_ARG, "plqcd_spinor_norm2: bad argument");
+    const int nb = norm2_blocks(lat->geom.Vh);
+    const size_t pbytes = sizeof(double) * (size_t)nb * nfields;
+    const size_t cbytes = sizeof(unsigned) * (size_t)nfields;
+    void *ws = nullptr;
+    PLQCD_TRY(lattice_workspace(lat, pbytes + cbytes, &ws));
+    double *partials = static_cast<double *>(ws);
+    unsigned *counters = reinterpret_cast<unsigned *>(static_cast<char *>(ws) + pbytes);
+    PLQCD_CUDA_TRY(cudaMemsetAsync(counters, 0, cbytes, lat->stream));
+    return launch_norm2_multi(lat->geom, lat->stream, fields, prec, nfields, partials, counters, norms_dev);
+}

@@ -270,3 +270,73 @@ int blas_axpby64(const Geom &g, cudaStream_t s, double a, const void *x, double 
 }
 
 }  // namespace plqcd
+
+// ---------------------------------------------------------------------------
+// |x_f|^2 of nf fields stored back to back (multi-RHS blocks), one grid row
+// per field; partials[f * gridDim.x + b], counters[f], results out[f].
+// ---------------------------------------------------------------------------
+namespace plqcd {
+namespace dev {
+
+template <int P>
+__global__ void __launch_bounds__(kBlasBlock) k_norm2_multi(const char *fields, size_t field_bytes, long Vh,
+                                                            double *partials, unsigned *counters, double *out) {
+    using R = typename SpinorIO<P>::real;
+    const int f = blockIdx.y;
+    const void *x = fields + (size_t)f * field_bytes;
+    double v = 0;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<R> s[12];
+        SpinorIO<P>::load(x, Vh, h, s);
+        v += norm2_site(s);
+    }
+    __shared__ double ws[kBlasBlock / 32];
+    __shared__ bool last;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) ws[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) b += ws[k];
+        partials[(size_t)f * gridDim.x + blockIdx.x] = b;
+        __threadfence();
+        last = atomicAdd(&counters[f], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double t = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x)
+        t += ((volatile double *)partials)[(size_t)f * gridDim.x + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    __syncthreads();
+    if (lane == 0) ws[w] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) tot += ws[k];
+        out[f] = tot;
+        counters[f] = 0;
+    }
+}
+
+}  // namespace dev
+
+int norm2_blocks(long Vh) { return dev::blas_grid(Vh); }
+
+int launch_norm2_multi(const Geom &g, cudaStream_t s, const void *fields, int prec, int nf, double *partials,
+                       unsigned *counters, double *out) {
+    const int nb = dev::blas_grid(g.Vh);
+    const size_t fb = spinor_parity_bytes(g.Vh, prec);
+    dim3 grid(nb, nf);
+#define F(P) dev::k_norm2_multi<P><<<grid, kBlasBlock, 0, s>>>((const char *)fields, fb, g.Vh, partials, counters, out)
+    BLAS_PREC_SWITCH(prec, F)
+#undef F
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+}  // namespace plqcd

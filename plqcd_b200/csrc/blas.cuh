@@ -55,6 +55,11 @@ int blas_accum_zero(const Geom &g, cudaStream_t s, void *x64, void *xs, int xpre
 // out64 = a64 - b64; sum |out|^2 -> op
 int blas_sub_norm2(const Geom &g, cudaStream_t s, void *out, const void *a, const void *b, const RedScratch &r,
                    RedOp op);
+// |x_f|^2 of nf fields stored back to back; scratch: nf * norm2_blocks(Vh)
+// partials and nf counters (zero on entry, left zero on exit)
+int norm2_blocks(long Vh);
+int launch_norm2_multi(const Geom &g, cudaStream_t s, const void *fields, int prec, int nf, double *partials,
+                       unsigned *counters, double *out);
 // y = a x + b y (F64 fields)
 int blas_axpby64(const Geom &g, cudaStream_t s, double a, const void *x, double b, void *y);
 

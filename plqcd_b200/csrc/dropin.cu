@@ -25,8 +25,12 @@ using namespace plqcd;
 
 namespace {
 
+constexpr int kMaxChunks = 8;
+
 struct DropIn {
     int dims[4] = {0, 0, 0, 0};
+    cudaStream_t s_h2d = nullptr, s_d2h = nullptr;  // copy streams
+    cudaEvent_t ev_in[kMaxChunks] = {}, ev_out[kMaxChunks] = {}, ev_k0[kMaxChunks] = {}, ev_k1[kMaxChunks] = {};
     plqcd_lattice *lat = nullptr;
     plqcd_gauge *gauge = nullptr;
     void *aos_in = nullptr, *aos_out = nullptr;  // API layout staging, one parity
@@ -34,7 +38,6 @@ struct DropIn {
     const su3 *cached_u = nullptr;
     uint64_t fingerprint = 0;
     bool dirty = true;
-    cudaEvent_t k0 = nullptr, k1 = nullptr;
     cudaStream_t stream = nullptr;  // owned by the drop-in path
     double kernel_ms = 0, h2d = 0, d2h = 0;
 };
@@ -48,8 +51,11 @@ void release_locked() {
     void *bufs[4] = {g_d.aos_in, g_d.aos_out, g_d.f_in, g_d.f_out};
     for (void *b : bufs)
         if (b) cudaFree(b);
-    if (g_d.k0) cudaEventDestroy(g_d.k0);
-    if (g_d.k1) cudaEventDestroy(g_d.k1);
+    for (int c = 0; c < kMaxChunks; c++)
+        for (cudaEvent_t ev : {g_d.ev_in[c], g_d.ev_out[c], g_d.ev_k0[c], g_d.ev_k1[c]})
+            if (ev) cudaEventDestroy(ev);
+    if (g_d.s_h2d) cudaStreamDestroy(g_d.s_h2d);
+    if (g_d.s_d2h) cudaStreamDestroy(g_d.s_d2h);
     if (g_d.lat) plqcd_lattice_destroy(g_d.lat);
     if (g_d.stream) cudaStreamDestroy(g_d.stream);
     g_d = DropIn();
@@ -105,9 +111,16 @@ int ensure_locked() {
             release_locked();
             return set_error(PLQCD_ERR_NOMEM, "drop-in: device allocation of %zu bytes failed", bytes);
         }
-    if (cudaEventCreate(&g_d.k0) != cudaSuccess || cudaEventCreate(&g_d.k1) != cudaSuccess) {
+    bool ok = cudaStreamCreateWithFlags(&g_d.s_h2d, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&g_d.s_d2h, cudaStreamNonBlocking) == cudaSuccess;
+    for (int c = 0; c < kMaxChunks && ok; c++)
+        ok = cudaEventCreateWithFlags(&g_d.ev_in[c], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&g_d.ev_out[c], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreate(&g_d.ev_k0[c]) == cudaSuccess && cudaEventCreate(&g_d.ev_k1[c]) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
         release_locked();
-        return set_error(PLQCD_ERR_CUDA, "drop-in: event creation failed");
+        return set_error(PLQCD_ERR_CUDA, "drop-in: stream/event creation failed");
     }
     g_d.dirty = true;
     return PLQCD_OK;
@@ -142,40 +155,71 @@ double hop_call(spinor *qin, spinor *qout, su3 *u, int out_parity) {
         g_d.h2d += 8.0 * Vh * sizeof(su3);
     }
 
-    const size_t bytes = (size_t)Vh * sizeof(spinor);
+    // Pipeline over chunks of t-slabs (contiguous half-site ranges): input
+    // chunks go up on the copy stream in the order last, 0, 1, ..., and
+    // output chunk c is computed once input chunks c-1, c, c+1 (periodic)
+    // have arrived, then copied back on a second copy stream while later
+    // chunks are still in flight; host->device and device->host transfers
+    // overlap each other and the kernels.
     const int in_parity = out_parity ^ 1;
-    unsigned flags = env_flag("PLQCD_REF_COMPAT", false) ? PLQCD_DSLASH_COMPAT : 0u;
-    cudaError_t e = cudaMemcpyAsync(g_d.aos_in, qin + in_parity * Vh, bytes, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) {
-        set_error(PLQCD_ERR_CUDA, "hopping matrix: H2D copy: %s", cudaGetErrorString(e));
-        return -1.0;
+    const unsigned flags = env_flag("PLQCD_REF_COMPAT", false) ? PLQCD_DSLASH_COMPAT : 0u;
+    const Geom &geo = lat->geom;
+    const int L3 = geo.L[3];
+    const long slab = geo.Vh / L3;
+    const int nch = L3 < kMaxChunks ? L3 : kMaxChunks;
+    auto first = [&](int c) { return slab * (long)((long)c * L3 / nch); };
+    auto count = [&](int c) { return first(c + 1) - first(c); };
+    const spinor *src = qin + in_parity * Vh;
+    spinor *dst = qout + out_parity * Vh;
+    spinor *ain = static_cast<spinor *>(g_d.aos_in), *aout = static_cast<spinor *>(g_d.aos_out);
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < nch && e == cudaSuccess; k++) {
+        const int c = (k == 0) ? nch - 1 : k - 1;
+        e = cudaMemcpyAsync(ain + first(c), src + first(c), count(c) * sizeof(spinor), cudaMemcpyHostToDevice,
+                            g_d.s_h2d);
+        // staging holds one parity, so it is addressed as parity 0
+        if (e == cudaSuccess &&
+            launch_spinor_import(geo, g_d.s_h2d, ain, 0, g_d.f_in, PLQCD_F64, first(c), count(c)) != PLQCD_OK)
+            return -1.0;
+        if (e == cudaSuccess) e = cudaEventRecord(g_d.ev_in[c], g_d.s_h2d);
     }
-    g_d.h2d += (double)bytes;
-    // staging holds one parity, so it is addressed as parity 0
-    if (launch_spinor_import(lat->geom, s, g_d.aos_in, 0, g_d.f_in, PLQCD_F64) != PLQCD_OK) return -1.0;
-    cudaEventRecord(g_d.k0, s);
-    DslashCall c;
-    c.gauge = g_d.gauge->data;
-    c.prec = PLQCD_F64;
-    c.recon = 18;
-    c.out = g_d.f_out;
-    c.in = g_d.f_in;
-    c.out_parity = out_parity;
-    c.flags = flags;
-    if (launch_dslash(lat->geom, s, c) != PLQCD_OK) return -1.0;
-    cudaEventRecord(g_d.k1, s);
-    if (launch_spinor_export(lat->geom, s, g_d.f_out, PLQCD_F64, 0, g_d.aos_out) != PLQCD_OK) return -1.0;
-    e = cudaMemcpyAsync(qout + out_parity * Vh, g_d.aos_out, bytes, cudaMemcpyDeviceToHost, s);
+    for (int c = 0; c < nch && e == cudaSuccess; c++) {
+        for (int d : {c - 1, c, c + 1}) cudaStreamWaitEvent(s, g_d.ev_in[(d + nch) % nch], 0);
+        cudaEventRecord(g_d.ev_k0[c], s);
+        DslashCall dc;
+        dc.gauge = g_d.gauge->data;
+        dc.prec = PLQCD_F64;
+        dc.recon = 18;
+        dc.out = g_d.f_out;
+        dc.in = g_d.f_in;
+        dc.out_parity = out_parity;
+        dc.flags = flags;
+        dc.h_begin = first(c);
+        dc.h_count = count(c);
+        if (launch_dslash(geo, s, dc) != PLQCD_OK) return -1.0;
+        cudaEventRecord(g_d.ev_k1[c], s);
+        if (launch_spinor_export(geo, s, g_d.f_out, PLQCD_F64, 0, aout, first(c), count(c)) != PLQCD_OK) return -1.0;
+        cudaEventRecord(g_d.ev_out[c], s);
+        cudaStreamWaitEvent(g_d.s_d2h, g_d.ev_out[c], 0);
+        e = cudaMemcpyAsync(dst + first(c), aout + first(c), count(c) * sizeof(spinor), cudaMemcpyDeviceToHost,
+                            g_d.s_d2h);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g_d.s_d2h);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         set_error(PLQCD_ERR_CUDA, "hopping matrix: %s", cudaGetErrorString(e));
         return -1.0;
     }
-    g_d.d2h += (double)bytes;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, g_d.k0, g_d.k1);
-    g_d.kernel_ms = ms;
-    lat->last_kernel_ms = ms;
+    g_d.h2d += (double)Vh * sizeof(spinor);
+    g_d.d2h += (double)Vh * sizeof(spinor);
+    double kms = 0;
+    for (int c = 0; c < nch; c++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, g_d.ev_k0[c], g_d.ev_k1[c]);
+        kms += ms;
+    }
+    g_d.kernel_ms = kms;
+    lat->last_kernel_ms = kms;
     return stop_watch(t0);
 }
 

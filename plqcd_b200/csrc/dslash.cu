@@ -35,6 +35,7 @@ struct DslashArgs {
     void *out[2];       // output field of parity p (FULL) / out[0] = output
     const void *x;      // xpay operand (single parity only)
     long Vh;
+    long h_begin, h_end;  // output half-sites processed: [h_begin, h_end) (single parity)
     int L0, L0h, L1, L2, L3;
     int out_parity;
     double a_up, a_low, b;
@@ -164,9 +165,9 @@ __global__ void __launch_bounds__(256) k_dslash(const DslashArgs a) {
         h = (long)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
     } else {
         par = a.out_parity;
-        h = (long)blockIdx.x * blockDim.x + threadIdx.x;
+        h = a.h_begin + (long)blockIdx.x * blockDim.x + threadIdx.x;
     }
-    if (h >= a.Vh) return;
+    if (h >= a.h_end) return;
     // selects, not a dynamic index into the parameter arrays (which would
     // copy them to local memory)
     const void *in = (FULL && par == 0) ? a.in[1] : a.in[0];
@@ -278,9 +279,9 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
         h = (long)(blockIdx.x >> 1) * B + threadIdx.x;
     } else {
         par = a.out_parity;
-        h = (long)blockIdx.x * B + threadIdx.x;
+        h = a.h_begin + (long)blockIdx.x * B + threadIdx.x;
     }
-    if (h >= a.Vh) return;  // no block-level barrier below
+    if (h >= a.h_end) return;  // no block-level barrier below
     const void *in = (FULL && par == 0) ? a.in[1] : a.in[0];
     void *out = (FULL && par == 1) ? a.out[1] : a.out[0];
     const long Vh = a.Vh;
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
 
 template <class SIO, class LIO, int ST, bool COMPAT, bool XPAY, bool FULL>
 static int launch_pipe(const Geom &g, cudaStream_t s, const DslashArgs &a, int block) {
-    long nblk = (g.Vh + block - 1) / block;
+    long nblk = (a.h_end - a.h_begin + block - 1) / block;
     if (FULL) nblk *= 2;
     constexpr int NS = SIO::NSLOT + LIO::NSLOT;
     const size_t smem = (size_t)ST * NS * 16 * block;
@@ -384,7 +385,7 @@ static int launch_t(const Geom &g, cudaStream_t s, const DslashArgs &a, int vari
 
 template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
 static int launch_direct(const Geom &g, cudaStream_t s, const DslashArgs &a, int block) {
-    long nblk = (g.Vh + block - 1) / block;
+    long nblk = (a.h_end - a.h_begin + block - 1) / block;
     if (FULL) nblk *= 2;
     k_dslash<SIO, LIO, COMPAT, XPAY, FULL><<<(unsigned)nblk, block, 0, s>>>(a);
     PLQCD_CUDA_TRY(cudaGetLastError());
@@ -429,6 +430,10 @@ int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
     }
     a.x = c.x;
     a.Vh = g.Vh;
+    a.h_begin = c.h_begin;
+    a.h_end = c.h_count < 0 ? g.Vh : c.h_begin + c.h_count;
+    if (a.h_begin < 0 || a.h_end > g.Vh || a.h_end <= a.h_begin || (c.full && (a.h_begin != 0 || a.h_end != g.Vh)))
+        return set_error(PLQCD_ERR_ARG, "dslash: site range [%ld, %ld) invalid", a.h_begin, a.h_end);
     a.L0 = g.L[0];
     a.L0h = g.L0h;
     a.L1 = g.L[1];

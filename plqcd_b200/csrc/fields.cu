@@ -27,9 +27,10 @@ __device__ __forceinline__ void to_real(const cx<double> in[12], cx<R> out[12]) 
 
 // ---- spinors ------------------------------------------------------------------
 template <int PREC>
-__global__ void k_spinor_import(const double2 *__restrict__ aos, long Vh, int parity, void *dst) {
-    long h = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= Vh) return;
+__global__ void k_spinor_import(const double2 *__restrict__ aos, long Vh, int parity, void *dst, long first,
+                                long count) {
+    long h = first + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= first + count) return;
     const double2 *p = aos + (parity * Vh + h) * 12;
     cx<double> s[12];
 #pragma unroll
@@ -44,9 +45,10 @@ __global__ void k_spinor_import(const double2 *__restrict__ aos, long Vh, int pa
 }
 
 template <int PREC>
-__global__ void k_spinor_export(const void *src, long Vh, int parity, double2 *__restrict__ aos) {
-    long h = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= Vh) return;
+__global__ void k_spinor_export(const void *src, long Vh, int parity, double2 *__restrict__ aos, long first,
+                                long count) {
+    long h = first + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= first + count) return;
     using R = typename SpinorIO<PREC>::real;
     cx<R> r[12];
     SpinorIO<PREC>::load(src, Vh, h, r);
@@ -214,16 +216,20 @@ __global__ void k_gauge_copy(void *dst, const void *src, long Vh) {
         default: return set_error(PLQCD_ERR_ARG, "unsupported gauge format %d/%d", prec, recon); \
     }
 
-int launch_spinor_import(const Geom &g, cudaStream_t s, const void *aos, int parity, void *dst, int prec) {
-#define F(P) dev::k_spinor_import<P><<<dev::nblocks(g.Vh), dev::kBlock, 0, s>>>((const double2 *)aos, g.Vh, parity, dst)
+int launch_spinor_import(const Geom &g, cudaStream_t s, const void *aos, int parity, void *dst, int prec, long first,
+                         long count) {
+    if (count < 0) count = g.Vh - first;
+#define F(P) dev::k_spinor_import<P><<<dev::nblocks(count), dev::kBlock, 0, s>>>((const double2 *)aos, g.Vh, parity, dst, first, count)
     PLQCD_SPINOR_SWITCH(prec, F)
 #undef F
     PLQCD_CUDA_TRY(cudaGetLastError());
     return PLQCD_OK;
 }
 
-int launch_spinor_export(const Geom &g, cudaStream_t s, const void *src, int prec, int parity, void *aos) {
-#define F(P) dev::k_spinor_export<P><<<dev::nblocks(g.Vh), dev::kBlock, 0, s>>>(src, g.Vh, parity, (double2 *)aos)
+int launch_spinor_export(const Geom &g, cudaStream_t s, const void *src, int prec, int parity, void *aos, long first,
+                         long count) {
+    if (count < 0) count = g.Vh - first;
+#define F(P) dev::k_spinor_export<P><<<dev::nblocks(count), dev::kBlock, 0, s>>>(src, g.Vh, parity, (double2 *)aos, first, count)
     PLQCD_SPINOR_SWITCH(prec, F)
 #undef F
     PLQCD_CUDA_TRY(cudaGetLastError());

@@ -75,8 +75,11 @@ struct plqcd_gauge {
 namespace plqcd {
 
 // ---- kernels (fields.cu) ------------------------------------------------------
-int launch_spinor_import(const Geom &g, cudaStream_t s, const void *aos, int parity, void *dst, int prec);
-int launch_spinor_export(const Geom &g, cudaStream_t s, const void *src, int prec, int parity, void *aos);
+// half-sites [first, first + count) of one parity (count < 0: to the end)
+int launch_spinor_import(const Geom &g, cudaStream_t s, const void *aos, int parity, void *dst, int prec,
+                         long first = 0, long count = -1);
+int launch_spinor_export(const Geom &g, cudaStream_t s, const void *src, int prec, int parity, void *aos,
+                         long first = 0, long count = -1);
 int launch_spinor_convert(const Geom &g, cudaStream_t s, void *dst, int dprec, const void *src, int sprec);
 int launch_spinor_gaussian(const Geom &g, cudaStream_t s, void *dst, int prec, int parity, uint64_t seed);
 int launch_gauge_import(const Geom &g, cudaStream_t s, const void *aos, long first_link, long nlinks,
@@ -104,6 +107,8 @@ struct DslashCall {
     void *out2 = nullptr;      // odd output in full mode (out = even output)
     const void *in2 = nullptr; // odd input in full mode (in = even input)
     int block = 0;             // 0 = library default
+    // output half-sites [h_begin, h_begin + h_count) (single parity; -1 = all)
+    long h_begin = 0, h_count = -1;
 };
 int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c);
 

@@ -131,6 +131,22 @@ int tune_launch(const std::string &key, cudaStream_t s, const std::vector<TuneRe
         cudaGetLastError();
         return run(chosen, false);
     }
+    // each candidate: one warm-up launch, a short probe to size the timed
+    // batch (at least ~2 ms of work), then the best of three batches
+    auto time_batch = [&](const TuneResult &c, int reps, float *ms) -> bool {
+        cudaEventRecord(e0, s);
+        int rc = PLQCD_OK;
+        for (int r = 0; r < reps && rc == PLQCD_OK; r++) rc = run(c, true);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess || rc != PLQCD_OK) {
+            clear_error();
+            cudaGetLastError();
+            return false;
+        }
+        cudaEventElapsedTime(ms, e0, e1);
+        *ms /= reps;
+        return true;
+    };
     double best = 1e30;
     TuneResult bestc = cands[0];
     for (const TuneResult &c : cands) {
@@ -139,23 +155,21 @@ int tune_launch(const std::string &key, cudaStream_t s, const std::vector<TuneRe
             cudaGetLastError();
             continue;
         }
-        const int reps = 3;
-        cudaEventRecord(e0, s);
-        int rc = PLQCD_OK;
-        for (int r = 0; r < reps && rc == PLQCD_OK; r++) rc = run(c, true);
-        cudaEventRecord(e1, s);
-        if (cudaEventSynchronize(e1) != cudaSuccess || rc != PLQCD_OK) {
-            clear_error();
-            cudaGetLastError();
-            continue;
+        float probe = 0;
+        if (!time_batch(c, 2, &probe)) continue;
+        int reps = probe > 0 ? (int)(2.0f / probe) : 50;
+        reps = reps < 2 ? 2 : (reps > 200 ? 200 : reps);
+        float t = 1e30f, ms = 0;
+        bool ok = true;
+        for (int k = 0; k < 3 && ok; k++) {
+            ok = time_batch(c, reps, &ms);
+            if (ok && ms < t) t = ms;
         }
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        ms /= reps;
-        if (ms < best) {
-            best = ms;
+        if (!ok) continue;
+        if (t < best) {
+            best = t;
             bestc = c;
-            bestc.ms = ms;
+            bestc.ms = t;
         }
     }
     cudaEventDestroy(e0);

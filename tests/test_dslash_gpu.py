@@ -296,3 +296,31 @@ def test_dropin_32x32x32x64_matches_oracle(dropin, restatement):
     P.hopping_matrix("oe", q, got, u)
     want = restatement.hop("full", L, q, u)
     assert relmax(got, want) < TOL64
+
+
+@pytest.mark.parametrize("prec", [P.F64, P.F32, P.F16, P.BF16])
+def test_spinor_norm2_batched(cuda, prec):
+    import torch
+    L = (8, 8, 4, 6)
+    lat = new_lattice(L)
+    V = lat.V
+    rng = np.random.default_rng(17)
+    nf = 5
+    bs = lat.spinor_bytes(prec)
+    block = dev_bytes(nf * bs)
+    want = []
+    for f in range(nf):
+        q = O.gaussian_spinor(V, rng) * (f + 1)
+        src = field_from_host(lat, q, 0, P.F64)
+        lat.spinor_convert(block[f * bs:(f + 1) * bs], prec, src, P.F64)
+        back = field_to_host(lat, block[f * bs:(f + 1) * bs], prec, 0)[: V // 2]
+        want.append(float(np.sum(np.abs(back) ** 2)))
+    out = torch.zeros(nf, dtype=torch.float64, device="cuda")
+    lat.spinor_norm2(block, prec, nf, out)
+    lat.synchronize()
+    got = out.cpu().numpy()
+    np.testing.assert_allclose(got, want, rtol=1e-12)
+    out2 = torch.zeros(nf, dtype=torch.float64, device="cuda")
+    lat.spinor_norm2(block, prec, nf, out2)
+    lat.synchronize()
+    assert bool((out == out2).all())  # fixed summation order: reproducible
