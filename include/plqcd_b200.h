@@ -134,6 +134,23 @@ int plqcd_spinor_gaussian(plqcd_lattice *lat, void *dst, int prec, int parity, u
  * (allocated with cudaMalloc on first use or growth). */
 int plqcd_spinor_norm2(plqcd_lattice *lat, const void *fields, int prec, int nfields, double *norms_dev);
 
+/* Same result as plqcd_spinor_norm2, for callers that must not allocate
+ * device memory: code running while a CUDA graph is captured in the global
+ * capture mode (cudaMalloc is prohibited there), applications whose device
+ * memory all comes from their own pool, and loops that cannot take the
+ * device synchronisation of cudaMalloc / cudaFree. It calls no allocating
+ * routine; its scratch is a static device array of about 303 KB that every
+ * GPU loading the library keeps until the process exits.
+ *  - nfields must be 1..PLQCD_NORM2_NOALLOC_MAX_FIELDS; larger batches are
+ *    rejected with PLQCD_ERR_ARG.
+ *  - The first call on each device looks up the scratch address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - All calls on a device share the one scratch array: calls that overlap
+ *    on the GPU (e.g. from two streams at once) race and give wrong sums.
+ * Counterpart in the reference: none (the reference has no device code). */
+#define PLQCD_NORM2_NOALLOC_MAX_FIELDS 32
+int plqcd_spinor_norm2_noalloc(plqcd_lattice *lat, const void *fields, int prec, int nfields, double *norms_dev);
+
 /* ---- hopping matrix on device fields ------------------------------------ */
 /* out (parity out_parity) = a * H in (in on the other parity) [+ b * x]
  * where a applies to spins 0,1 and a_low to spins 2,3 (gamma5 folding),

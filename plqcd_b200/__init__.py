@@ -100,6 +100,7 @@ _SIGS = {
     "plqcd_spinor_convert": (_i, [_vp, _vp, _i, _vp, _i]),
     "plqcd_spinor_gaussian": (_i, [_vp, _vp, _i, _i, _u64]),
     "plqcd_spinor_norm2": (_i, [_vp, _vp, _i, _i, _vp]),
+    "plqcd_spinor_norm2_noalloc": (_i, [_vp, _vp, _i, _i, _vp]),
     "plqcd_dslash": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint]),
     "plqcd_dslash_xpay": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint, _d, _vp, _d]),
     "plqcd_dslash_full": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i]),
