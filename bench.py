@@ -260,7 +260,7 @@ def run_ours(args, d: Dist):
     import plqcd_b200 as P
     torch.cuda.set_device(d.local)
     hbm, peak_kind = measured_peaks()
-    L = L_BENCH
+    L = args.lattice
     lat = P.Lattice(L, d.local, torch.cuda.current_stream().cuda_stream)
     V, Vh = lat.V, lat.Vh
 
@@ -315,8 +315,20 @@ def run_ours(args, d: Dist):
             "eo_gbs": round(Vh * BYTES_PARITY[1] / t32e / 1e9, 1)}
     del g32, f32e, f32o, o32e, o32o
 
+    if args.only == "dslash":
+        if d.rank == 0:
+            print(json.dumps({"metric": "Dslash GFLOP/s", "value": round(value, 1), "unit": "GFLOP/s",
+                              "lattice": list(L), "only": "dslash", "per_parity_f64": parity, "f32": fp32}))
+        return 0
+
     # ---- e2e through the reference-facing C-ABI (host arrays) ---------------
     e2e = run_e2e(torch, P, lat, g64, fe, fo, d, args)
+
+    # ---- even/odd CG: FP64 vs mixed precision, time to 1e-10 ----------------
+    cg = run_cg(torch, P, lat, g64, buf, args) if not args.skip_cg else None
+    del fe, fo, oe_, oo_
+    # ---- reduced precision at 48^3x96: error against FP64 --------------------
+    reduced = run_reduced(torch, P, d, args) if not args.skip_reduced else None
 
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
@@ -346,6 +358,8 @@ def run_ours(args, d: Dist):
         "per_parity_f64": parity,
         "f32": fp32,
         "e2e": e2e,
+        "cg": cg,
+        "reduced_precision": reduced,
         "gpu_launches": K,
         "clocks": clocks,
     }
@@ -410,6 +424,90 @@ def run_e2e(torch, P, lat, g64, fe, fo, d: Dist, args):
     return res
 
 
+def run_cg(torch, P, lat, g64, buf, args):
+    """Even/odd CG on D^dag D at kappa = 0.12, Gaussian source, to a true
+    relative residual of 1e-10: FP64 against mixed precision (F32 and F16
+    inner operators with 12-real links, FP64 reliable updates). Device time
+    of each whole solve; the error of every mixed solution against the FP64
+    one is reported."""
+    kappa, tol = 0.12, 1e-10
+    bs = lat.spinor_bytes(P.F64)
+    be, bo = buf(P.F64), buf(P.F64)
+    lat.spinor_gaussian(be, P.F64, 0, 4242)
+    lat.spinor_gaussian(bo, P.F64, 1, 4242)
+    sloppy = {"f64": None, "f32": (P.F32, 12), "f16": (P.F16, 12)}
+    out, xs = {}, {}
+    for name, fmt in sloppy.items():
+        gs = None
+        if fmt:
+            gs = P.Gauge(lat, *fmt)
+            gs.copy_from(g64)
+        prec = fmt[0] if fmt else P.F64
+        xe, xo = buf(P.F64), buf(P.F64)
+        # warm-up: a few iterations tune every kernel configuration the solve uses
+        P.invert_cg(lat, g64, gs, xe, xo, be, bo, P.cg_param(kappa=kappa, tol=tol, max_iter=4, sloppy_prec=prec),
+                    raise_on_error=False)
+        info = P.invert_cg(lat, g64, gs, xe, xo, be, bo, P.cg_param(kappa=kappa, tol=tol, sloppy_prec=prec))
+        out[name] = {"iterations": info.iterations, "reliable_updates": info.reliable_updates,
+                     "seconds": round(info.seconds, 5), "schur_residual": info.schur_residual,
+                     "true_residual": info.true_residual}
+        xs[name] = (xe, xo)
+        del gs
+    lat.synchronize()
+    # F64 fields are plain doubles: compare the solutions as float64 vectors
+    x64 = torch.cat([xs["f64"][0], xs["f64"][1]]).view(torch.float64)
+    for name in ("f32", "f16"):
+        diff = torch.cat([xs[name][0], xs[name][1]]).view(torch.float64) - x64
+        out[name]["error_vs_f64"] = float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(x64))
+    best = min(("f32", "f16"), key=lambda n: out[n]["seconds"])
+    out["speedup_mixed_vs_f64"] = round(out["f64"]["seconds"] / out[best]["seconds"], 3)
+    out["best_mixed"] = best
+    out["config"] = {"lattice": list(lat.dims), "kappa": kappa, "tol": tol, "source": "Gaussian",
+                     "operator": "even/odd preconditioned Mhat^dag Mhat, CG"}
+    return out
+
+
+def run_reduced(torch, P, d: Dist, args):
+    """Reduced-precision hopping at 48^3x96: relative L2 error of the eo
+    output against the FP64 kernel, and each kernel's bandwidth."""
+    L = (48, 48, 48, 96)
+    lat = P.Lattice(L, d.local, torch.cuda.current_stream().cuda_stream)
+    Vh = lat.Vh
+    g64 = P.Gauge(lat, P.F64, 18)
+    g64.random(77)
+
+    def buf(prec):
+        return torch.empty(lat.spinor_bytes(prec), dtype=torch.uint8, device="cuda")
+
+    fin, ref = buf(P.F64), buf(P.F64)
+    lat.spinor_gaussian(fin, P.F64, 1, 5)
+    lat.dslash(g64, ref, fin, P.EVEN, P.F64)
+    nrm = torch.zeros(1, dtype=torch.float64, device="cuda")
+    lat.spinor_norm2(ref, P.F64, 1, nrm)
+    ref2 = float(nrm)
+    res = {"lattice": list(L)}
+    t64 = time_kernel(torch, lambda: lat.dslash(g64, ref, fin, P.EVEN, P.F64), 20, 3) / 20 / 1e3
+    res["f64_18"] = {"rel_l2_vs_f64": 0.0, "gbs": round(Vh * 1536 / t64 / 1e9, 1),
+                     "gflops": round(Vh * FLOP_PER_SITE / t64 / 1e9, 1)}
+    for name, prec, recon, bps in (("f32_18", P.F32, 18, 768), ("f32_12", P.F32, 12, 576),
+                                   ("f16_12", P.F16, 12, 296), ("bf16_12", P.BF16, 12, 296)):
+        g = P.Gauge(lat, prec, recon)
+        g.copy_from(g64)
+        a, o = buf(prec), buf(prec)
+        lat.spinor_convert(a, prec, fin, P.F64)
+        t = time_kernel(torch, lambda: lat.dslash(g, o, a, P.EVEN, prec), 20, 3) / 20 / 1e3
+        back = buf(P.F64)
+        lat.spinor_convert(back, P.F64, o, prec)
+        diff = back.view(torch.float64) - ref.view(torch.float64)
+        err = float(torch.linalg.vector_norm(diff)) / ref2 ** 0.5
+        res[name] = {"rel_l2_vs_f64": err, "gbs": round(Vh * bps / t / 1e9, 1),
+                     "gflops": round(Vh * FLOP_PER_SITE / t / 1e9, 1)}
+        del g, a, o, back, diff
+    del g64
+    lat.close()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -419,7 +517,14 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-baseline sampling")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--skip-cg", action="store_true")
+    ap.add_argument("--skip-reduced", action="store_true")
+    ap.add_argument("--lattice", default=",".join(map(str, L_BENCH)),
+                    help="L0,L1,L2,L3 of the hopping-matrix workload (default 32,32,32,64)")
+    ap.add_argument("--only", choices=["all", "dslash"], default="all",
+                    help="dslash: only the hopping kernels (profiling runs)")
     args = ap.parse_args()
+    args.lattice = tuple(int(x) for x in args.lattice.split(","))
     d = Dist()
     if args.impl == "reference":
         return run_reference(args, d)
