@@ -45,6 +45,10 @@ BYTES_PARITY = {0: 192 + 8 * 144 + 192, 1: 96 + 8 * 72 + 96}        # F64 / F32,
 BYTES_FULL = {0: 192 + 4 * 144 + 192, 1: 96 + 4 * 72 + 96}          # full lattice: each link read once
 BYTES_F32_12 = 96 + 8 * 48 + 96
 BYTES_HALF_12 = 52 + 8 * 24 + 52
+# DRAM bytes (read + write) per site of the full-lattice F64 kernel from one ncu
+# capture on 24^3x48 (profiles/dslash_f64_full_and_eo_24x24x24x48.txt); traffic
+# grows with the sites processed, so a launch moves this times V bytes.
+DRAM_BYTES_PER_SITE_FULL_F64 = 634.8e6 / (24 * 24 * 24 * 48)
 
 
 def measured_peaks():
@@ -286,7 +290,7 @@ def run_ours(args, d: Dist):
     achieved = V * BYTES_FULL[0] / t_step / 1e9
 
     # ---- per-parity kernels (the drop-in and solver building block) ---------
-    Kp = max(10, K // 2)
+    Kp = K if args.only == "dslash" else max(10, K // 2)
     eo = lambda: lat.dslash(g64, oe_, fo, P.EVEN, P.F64)
     oe = lambda: lat.dslash(g64, oo_, fe, P.ODD, P.F64)
     ms_eo = time_kernel(torch, eo, Kp, W)
@@ -353,8 +357,9 @@ def run_ours(args, d: Dist):
                    "parallelism": f"replicas x{d.world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
-                     "bytes_per_site": BYTES_FULL[0], "kernel": "k_dslash<F64,18,full>",
-                     "traffic": None},
+                     "bytes_per_site": BYTES_FULL[0], "kernel": "k_dslash_pipe<F64,18,full>",
+                     "traffic": round(DRAM_BYTES_PER_SITE_FULL_F64 * V),
+                     "traffic_note": "ncu dram bytes of a 24^3x48 launch scaled by sites"},
         "per_parity_f64": parity,
         "f32": fp32,
         "e2e": e2e,
