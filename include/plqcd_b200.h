@@ -211,6 +211,49 @@ int plqcd_tune_load(const char *path);   /* NULL = default file */
 int plqcd_tune_count(void);
 int plqcd_tune_get(const char *key, int *variant, int *block, double *ms);
 
+/* ---- multiple right-hand sides ------------------------------------------ */
+/* H applied to nrhs one-parity fields stored back to back (field r at
+ * in + r * plqcd_spinor_bytes(lat, prec)). Each link is loaded once per
+ * tile of right-hand sides and the tiles of a site range run together, so
+ * link traffic is shared by all nrhs fields. The RHS tile and block size are
+ * autotuned. */
+int plqcd_dslash_mrhs(plqcd_lattice *lat, const plqcd_gauge *g, void *out, const void *in, int nrhs,
+                      int out_parity, int prec, unsigned flags);
+int plqcd_dslash_mrhs_xpay(plqcd_lattice *lat, const plqcd_gauge *g, void *out, const void *in, int nrhs,
+                           int out_parity, int prec, unsigned flags, double a, const void *x, double b);
+
+/* ---- batched multi-RHS solver ------------------------------------------- */
+/* One lattice of a batch: nrhs sources b (F64 blocks of each parity, field r
+ * at b + r * plqcd_spinor_bytes(lat, PLQCD_F64)) and the solution blocks x. */
+typedef struct {
+    plqcd_lattice *lat;
+    const plqcd_gauge *g64;       /* F64 links (reliable updates, setup) */
+    const plqcd_gauge *g_sloppy;  /* links in param->sloppy_prec (NULL: g64) */
+    int nrhs;
+    void *x_even, *x_odd;
+    const void *b_even, *b_odd;
+} plqcd_solve_item;
+
+typedef struct {
+    int iterations;            /* iterations of the batch loop */
+    int reliable_updates;      /* FP64 reliable updates (batch-wide) */
+    int converged;             /* every RHS reached tol */
+    double max_schur_residual; /* max over RHS of |b' - Mhat x_e| / |b'| */
+    double max_true_residual;  /* max over RHS of |b - D x| / |b| (FP64, after the solve) */
+    double seconds;            /* device time of the solve */
+    int graph_launches;        /* 1 when the loop ran as one CUDA-graph launch */
+} plqcd_batch_info;
+
+/* Solve D x = b for every RHS of every lattice in `items` (same device):
+ * one CG recursion per RHS on Mhat^dag Mhat, hopping kernels on whole RHS
+ * blocks, FP64 reliable updates when param->sloppy_prec is not F64. With
+ * use_graph the iteration loop is captured once into a CUDA graph whose
+ * WHILE and IF conditional nodes are set by device code, and runs as a
+ * single graph launch. true_residuals (optional) receives |b - D x|/|b| per
+ * RHS in item order. */
+int plqcd_invert_cg_batch(plqcd_solve_item *items, int nitems, const plqcd_cg_param *param, int use_graph,
+                          plqcd_batch_info *info, double *true_residuals);
+
 /* ---- drop-in path controls ---------------------------------------------- */
 /* Mark the host gauge field `u` as changed (or a new field) so the next
  * drop-in call uploads it. */

@@ -104,6 +104,8 @@ _SIGS = {
     "plqcd_dslash": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint]),
     "plqcd_dslash_xpay": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint, _d, _vp, _d]),
     "plqcd_dslash_full": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i]),
+    "plqcd_dslash_mrhs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, ctypes.c_uint]),
+    "plqcd_dslash_mrhs_xpay": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, ctypes.c_uint, _d, _vp, _d]),
     "plqcd_tune_enable": (_i, [_i]),
     "plqcd_tune_clear": (_i, []),
     "plqcd_tune_save": (_i, [ctypes.c_char_p]),
@@ -259,6 +261,15 @@ class Lattice:
         check(lib().plqcd_dslash_xpay(self.handle, gauge.handle, _ptr(out), _ptr(inp), out_parity, prec, flags,
                                       a, _ptr(x), b))
 
+    def dslash_mrhs(self, gauge: "Gauge", out, inp, nrhs: int, out_parity: int, prec: int, flags: int = 0):
+        check(lib().plqcd_dslash_mrhs(self.handle, gauge.handle, _ptr(out), _ptr(inp), nrhs, out_parity, prec,
+                                      flags))
+
+    def dslash_mrhs_xpay(self, gauge: "Gauge", out, inp, nrhs: int, out_parity: int, prec: int, a: float, x,
+                         b: float, flags: int = 0):
+        check(lib().plqcd_dslash_mrhs_xpay(self.handle, gauge.handle, _ptr(out), _ptr(inp), nrhs, out_parity, prec,
+                                           flags, a, _ptr(x), b))
+
     def dslash_full(self, gauge: "Gauge", out_even, out_odd, in_even, in_odd, prec: int):
         check(lib().plqcd_dslash_full(self.handle, gauge.handle, _ptr(out_even), _ptr(out_odd), _ptr(in_even),
                                       _ptr(in_odd), prec))
@@ -352,3 +363,44 @@ def invert_cg(lat: Lattice, g64: Gauge, g_sloppy: Gauge | None, x_even, x_odd, b
     if rc != OK and raise_on_error:
         raise PlqcdError(f"plqcd error {rc}: {last_error()}")
     return info
+
+
+class SolveItem(ctypes.Structure):
+    _fields_ = [("lat", _vp), ("g64", _vp), ("g_sloppy", _vp), ("nrhs", ctypes.c_int),
+                ("x_even", _vp), ("x_odd", _vp), ("b_even", _vp), ("b_odd", _vp)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("reliable_updates", ctypes.c_int), ("converged", ctypes.c_int),
+                ("max_schur_residual", ctypes.c_double), ("max_true_residual", ctypes.c_double),
+                ("seconds", ctypes.c_double), ("graph_launches", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_SIGS.update({
+    "plqcd_invert_cg_batch": (_i, [ctypes.POINTER(SolveItem), _i, ctypes.POINTER(CgParam), _i,
+                                   ctypes.POINTER(BatchInfo), _dp]),
+})
+
+
+def invert_cg_batch(items, param: CgParam, use_graph: bool = True, raise_on_error: bool = True):
+    """items: list of dicts with lat, g64, g_sloppy, nrhs, x_even, x_odd,
+    b_even, b_odd. Returns (BatchInfo, per-RHS true residuals)."""
+    arr = (SolveItem * len(items))()
+    n = 0
+    for k, it in enumerate(items):
+        arr[k].lat = it["lat"].handle
+        arr[k].g64 = it["g64"].handle
+        arr[k].g_sloppy = it["g_sloppy"].handle if it.get("g_sloppy") else None
+        arr[k].nrhs = it["nrhs"]
+        for f in ("x_even", "x_odd", "b_even", "b_odd"):
+            setattr(arr[k], f, _ptr(it[f]))
+        n += it["nrhs"]
+    res = (ctypes.c_double * n)()
+    info = BatchInfo()
+    rc = lib().plqcd_invert_cg_batch(arr, len(items), ctypes.byref(param), int(use_graph), ctypes.byref(info), res)
+    if rc != OK and raise_on_error:
+        raise PlqcdError(f"plqcd error {rc}: {last_error()}")
+    return info, list(res)

@@ -1,0 +1,149 @@
+// dslash_core.cuh -- per-direction arithmetic of the Wilson hopping term,
+// shared by the single- and multi-RHS kernels.
+//
+// For output site x and direction mu (reference lib/dirac.c:95-114,
+// 163-195 for the projections, 269-311 and 371-398 for the rebuild):
+//   forward:  chi  = U_mu(x)        h,  h  = upper((1 - g_mu) psi(x+mu))
+//   backward: chi' = U_mu(x-mu)^dag h', h' = upper((1 + g_mu) psi(x-mu))
+#pragma once
+
+#include "device_fields.cuh"
+
+namespace plqcd {
+namespace dev {
+
+struct DslashArgs {
+    const void *gauge;
+    const void *in[2];  // input field of parity p (FULL) / in[0] = input (single parity)
+    void *out[2];       // output field of parity p (FULL) / out[0] = output
+    const void *x;      // xpay operand (single parity only)
+    long Vh;
+    long h_begin, h_end;  // output half-sites processed: [h_begin, h_end) (single parity)
+    int L0, L0h, L1, L2, L3;
+    int out_parity;
+    double a_up, a_low, b;
+    double g5_in;       // +1 or -1: sign applied to input spins 2,3
+};
+
+// projection of the neighbour spinor onto the two upper spin components.
+// FWD: (1 - g_mu) psi(x+mu); backward: (1 + g_mu) psi(x-mu). `sg` is the
+// sign on the lower spins (backward and gamma5-on-input flip it).
+template <int MU, typename R>
+__device__ __forceinline__ void project(const cx<R> s[12], R sg, cx<R> h0[3], cx<R> h1[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const cx<R> s0 = s[c], s1 = s[3 + c], s2 = s[6 + c], s3 = s[9 + c];
+        if (MU == 0) {  // s0 + s2, s1 + s3
+            h0[c] = {fma(sg, s2.re, s0.re), fma(sg, s2.im, s0.im)};
+            h1[c] = {fma(sg, s3.re, s1.re), fma(sg, s3.im, s1.im)};
+        } else if (MU == 1) {  // s0 + i s3, s1 + i s2
+            h0[c] = {fma(-sg, s3.im, s0.re), fma(sg, s3.re, s0.im)};
+            h1[c] = {fma(-sg, s2.im, s1.re), fma(sg, s2.re, s1.im)};
+        } else if (MU == 2) {  // s0 + s3, s1 - s2
+            h0[c] = {fma(sg, s3.re, s0.re), fma(sg, s3.im, s0.im)};
+            h1[c] = {fma(-sg, s2.re, s1.re), fma(-sg, s2.im, s1.im)};
+        } else {  // s0 + i s2, s1 - i s3
+            h0[c] = {fma(-sg, s2.im, s0.re), fma(sg, s2.re, s0.im)};
+            h1[c] = {fma(sg, s3.im, s1.re), fma(-sg, s3.re, s1.im)};
+        }
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void su3_mul(const cx<R> U[9], const cx<R> v[3], cx<R> r[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        R re = U[3 * a].re * v[0].re;
+        R im = U[3 * a].re * v[0].im;
+        re = fma(-U[3 * a].im, v[0].im, re);
+        im = fma(U[3 * a].im, v[0].re, im);
+#pragma unroll
+        for (int b = 1; b < 3; b++) {
+            re = fma(U[3 * a + b].re, v[b].re, re);
+            re = fma(-U[3 * a + b].im, v[b].im, re);
+            im = fma(U[3 * a + b].re, v[b].im, im);
+            im = fma(U[3 * a + b].im, v[b].re, im);
+        }
+        r[a] = {re, im};
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void su3_dag_mul(const cx<R> U[9], const cx<R> v[3], cx<R> r[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        R re = U[a].re * v[0].re;
+        R im = U[a].re * v[0].im;
+        re = fma(U[a].im, v[0].im, re);
+        im = fma(-U[a].im, v[0].re, im);
+#pragma unroll
+        for (int b = 1; b < 3; b++) {
+            re = fma(U[3 * b + a].re, v[b].re, re);
+            re = fma(U[3 * b + a].im, v[b].im, re);
+            im = fma(U[3 * b + a].re, v[b].im, im);
+            im = fma(-U[3 * b + a].im, v[b].re, im);
+        }
+        r[a] = {re, im};
+    }
+}
+
+// rebuild of the lower spins from chi = (c0, c1); LS = +1 forward, -1 backward
+template <int MU, int LS, bool LOWER, typename R>
+__device__ __forceinline__ void accumulate(cx<R> acc[12], const cx<R> c0[3], const cx<R> c1[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        acc[c] = cadd(acc[c], c0[c]);
+        acc[3 + c] = cadd(acc[3 + c], c1[c]);
+        if (!LOWER) continue;
+        cx<R> &r2 = acc[6 + c];
+        cx<R> &r3 = acc[9 + c];
+        if (MU == 0) {  // r2 += LS c0, r3 += LS c1
+            r2 = {r2.re + LS * c0[c].re, r2.im + LS * c0[c].im};
+            r3 = {r3.re + LS * c1[c].re, r3.im + LS * c1[c].im};
+        } else if (MU == 1) {  // r2 += -LS i c1, r3 += -LS i c0
+            r2 = {r2.re + LS * c1[c].im, r2.im - LS * c1[c].re};
+            r3 = {r3.re + LS * c0[c].im, r3.im - LS * c0[c].re};
+        } else if (MU == 2) {  // r2 += -LS c1, r3 += LS c0
+            r2 = {r2.re - LS * c1[c].re, r2.im - LS * c1[c].im};
+            r3 = {r3.re + LS * c0[c].re, r3.im + LS * c0[c].im};
+        } else {  // r2 += -LS i c0, r3 += LS i c1
+            r2 = {r2.re + LS * c0[c].im, r2.im - LS * c0[c].re};
+            r3 = {r3.re - LS * c1[c].im, r3.im + LS * c1[c].re};
+        }
+    }
+}
+
+// Projection, SU(3) product and rebuild of one direction on data already in
+// registers.
+template <int MU, bool FWD, bool COMPAT, typename R>
+__device__ __forceinline__ void compute_dir(cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg_in) {
+    cx<R> h0[3], h1[3];
+    project<MU, R>(s, FWD ? sg_in : -sg_in, h0, h1);
+    cx<R> c0[3], c1[3];
+    if (FWD) {
+        su3_mul(U, h0, c0);
+        su3_mul(U, h1, c1);
+    } else {
+        su3_dag_mul(U, h0, c0);
+        su3_dag_mul(U, h1, c1);
+    }
+    accumulate<MU, FWD ? 1 : -1, !(COMPAT && FWD), R>(acc, c0, c1);
+}
+
+template <bool COMPAT, typename R>
+__device__ __forceinline__ void compute_dir_n(int d, cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg) {
+    // d is a compile-time constant after unrolling, so this switch folds
+    switch (d) {
+        case 0: compute_dir<0, true, COMPAT>(acc, s, U, sg); break;
+        case 1: compute_dir<1, true, COMPAT>(acc, s, U, sg); break;
+        case 2: compute_dir<2, true, COMPAT>(acc, s, U, sg); break;
+        case 3: compute_dir<3, true, COMPAT>(acc, s, U, sg); break;
+        case 4: compute_dir<0, false, COMPAT>(acc, s, U, sg); break;
+        case 5: compute_dir<1, false, COMPAT>(acc, s, U, sg); break;
+        case 6: compute_dir<2, false, COMPAT>(acc, s, U, sg); break;
+        default: compute_dir<3, false, COMPAT>(acc, s, U, sg); break;
+    }
+}
+
+}  // namespace dev
+}  // namespace plqcd

@@ -1,0 +1,244 @@
+// dslash_mrhs.cu -- hopping matrix on a block of right-hand sides.
+//
+// One thread handles one output site for a tile of NR right-hand sides: per
+// direction it loads the link once and applies it to the NR neighbour
+// spinors, so a link's HBM bytes are shared by the tile. Consecutive blocks
+// cover the RHS tiles of the same sites (tile index fastest), so the other
+// tiles find the links in L2 and the link traffic per launch is paid once
+// for all nrhs right-hand sides: bytes per site and RHS =
+// 2 * spinor + 8 * link / nrhs. The per-direction arithmetic is that of the
+// single-RHS kernel (dslash_core.cuh).
+//
+// A block of fields is nrhs one-parity fields back to back (field r at
+// base + r * field_bytes).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "dslash_core.cuh"
+#include "internal.h"
+#include "tune.h"
+
+namespace plqcd {
+namespace dev {
+
+struct MrhsArgs {
+    const void *gauge;
+    const char *in;
+    char *out;
+    const char *x;
+    size_t fbytes;
+    int nrhs, ntiles;
+    long Vh;
+    int L0, L0h, L1, L2, L3;
+    int out_parity;
+    double a_up, a_low, b, g5_in;
+};
+
+template <class SIO, class LIO, int NR, bool XPAY>
+__global__ void __launch_bounds__(256) k_dslash_mrhs(const MrhsArgs a) {
+    using R = typename SIO::real;
+    const int tile = blockIdx.x % a.ntiles;
+    const long h = (long)(blockIdx.x / a.ntiles) * blockDim.x + threadIdx.x;
+    if (h >= a.Vh) return;
+    const int r0 = tile * NR;
+    const int nr = min(NR, a.nrhs - r0);
+    const int par = a.out_parity, opp = par ^ 1;
+    const long Vh = a.Vh;
+    const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
+    const Coords c = site_coords(h, par, L0h, L1, L2);
+    const int xh = (int)(h - c.row * L0h);
+    const long L01 = L1, L012 = (long)L1 * L2;
+    const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
+    const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
+    long nb[8];
+    nb[0] = (xp >> 1) + L0h * c.row;
+    nb[1] = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
+    nb[2] = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
+    nb[3] = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
+    nb[4] = (xm >> 1) + L0h * c.row;
+    nb[5] = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
+    nb[6] = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
+    nb[7] = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
+    const R sg = (R)a.g5_in;
+
+    cx<R> acc[NR][12];
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int k = 0; k < 12; k++) acc[r][k] = {R(0), R(0)};
+
+#pragma unroll
+    for (int d = 0; d < 8; d++) {
+        cx<R> U[9];
+        if (d < 4)
+            LIO::load(a.gauge, Vh, par, d, h, U);
+        else
+            LIO::load(a.gauge, Vh, opp, d - 4, nb[d], U);
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            if (r < nr) {
+                cx<R> s[12];
+                SIO::load(a.in + (size_t)(r0 + r) * a.fbytes, Vh, nb[d], s);
+                compute_dir_n<false, R>(d, acc[r], s, U, sg);
+            }
+        }
+    }
+
+    const R aup = (R)a.a_up, alow = (R)a.a_low, b = (R)a.b;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        if (r >= nr) continue;
+        if (XPAY) {
+            cx<R> xv[12];
+            SIO::load(a.x + (size_t)(r0 + r) * a.fbytes, Vh, h, xv);
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const R ak = k < 6 ? aup : alow;
+                acc[r][k] = {fma(ak, acc[r][k].re, b * xv[k].re), fma(ak, acc[r][k].im, b * xv[k].im)};
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const R ak = k < 6 ? aup : alow;
+                acc[r][k] = {ak * acc[r][k].re, ak * acc[r][k].im};
+            }
+        }
+        SIO::store(a.out + (size_t)(r0 + r) * a.fbytes, Vh, h, acc[r]);
+    }
+}
+
+template <class SIO, class LIO, int NR>
+static int launch_nr(const Geom &g, cudaStream_t s, MrhsArgs a, int block, bool xpay) {
+    a.ntiles = (a.nrhs + NR - 1) / NR;
+    const long nsb = (g.Vh + block - 1) / block;
+    const long nblk = nsb * a.ntiles;
+    if (nblk > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: grid too large");
+    if (xpay)
+        k_dslash_mrhs<SIO, LIO, NR, true><<<(unsigned)nblk, block, 0, s>>>(a);
+    else
+        k_dslash_mrhs<SIO, LIO, NR, false><<<(unsigned)nblk, block, 0, s>>>(a);
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+template <int P, int RC>
+static int launch_pr(const Geom &g, cudaStream_t s, const MrhsArgs &a, int nr, int block, bool xpay) {
+    using S = SpinorIO<P>;
+    using L = LinkIO<P, RC>;
+    switch (nr) {
+        case 1: return launch_nr<S, L, 1>(g, s, a, block, xpay);
+        case 2: return launch_nr<S, L, 2>(g, s, a, block, xpay);
+        case 4:
+            // four FP64 accumulators exceed the register file
+            if constexpr (P != PLQCD_F64) return launch_nr<S, L, 4>(g, s, a, block, xpay);
+            break;
+        default: break;
+    }
+    return set_error(PLQCD_ERR_ARG, "dslash_mrhs: RHS tile %d not available for this precision", nr);
+}
+
+}  // namespace dev
+
+static int mrhs_dispatch(const Geom &g, cudaStream_t s, int prec, int recon, const dev::MrhsArgs &a, int nr,
+                         int block, bool xpay) {
+    if (block % 32 || block < 32 || block > 256) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: block %d", block);
+    switch (prec * 100 + recon) {
+        case PLQCD_F64 * 100 + 18: return dev::launch_pr<PLQCD_F64, 18>(g, s, a, nr, block, xpay);
+        case PLQCD_F64 * 100 + 12: return dev::launch_pr<PLQCD_F64, 12>(g, s, a, nr, block, xpay);
+        case PLQCD_F32 * 100 + 18: return dev::launch_pr<PLQCD_F32, 18>(g, s, a, nr, block, xpay);
+        case PLQCD_F32 * 100 + 12: return dev::launch_pr<PLQCD_F32, 12>(g, s, a, nr, block, xpay);
+        case PLQCD_F16 * 100 + 12: return dev::launch_pr<PLQCD_F16, 12>(g, s, a, nr, block, xpay);
+        case PLQCD_BF16 * 100 + 12: return dev::launch_pr<PLQCD_BF16, 12>(g, s, a, nr, block, xpay);
+        default: return set_error(PLQCD_ERR_ARG, "dslash_mrhs: unsupported format %d/%d", prec, recon);
+    }
+}
+
+// out (nrhs fields) = a_up/a_low * H in + b * x; tuned over RHS tile and block
+int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
+                       const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b) {
+    if (nrhs < 1) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: nrhs must be >= 1");
+    dev::MrhsArgs m{};
+    m.gauge = gauge;
+    m.in = static_cast<const char *>(in);
+    m.out = static_cast<char *>(out);
+    m.x = static_cast<const char *>(x);
+    m.fbytes = spinor_parity_bytes(g.Vh, prec);
+    m.nrhs = nrhs;
+    m.Vh = g.Vh;
+    m.L0 = g.L[0];
+    m.L0h = g.L0h;
+    m.L1 = g.L[1];
+    m.L2 = g.L[2];
+    m.L3 = g.L[3];
+    m.out_parity = out_parity;
+    m.a_up = a;
+    m.a_low = (flags & PLQCD_DSLASH_G5_OUT) ? -a : a;
+    m.b = b;
+    m.g5_in = (flags & PLQCD_DSLASH_G5_IN) ? -1.0 : 1.0;
+    const bool xpay = x != nullptr;
+    char key[256];
+    snprintf(key, sizeof key, "%sdslash_mrhs|p%d|r%d|%s|n%d|%dx%dx%dx%d", device_tag().c_str(), prec, recon,
+             xpay ? "xpay" : "plain", nrhs, g.L[0], g.L[1], g.L[2], g.L[3]);
+    std::vector<TuneResult> cands;
+    for (int nr : {2, 1, 4}) {
+        if (nr == 4 && prec == PLQCD_F64) continue;
+        if (nr > nrhs && nr != 1) continue;
+        for (int blk : {64, 128, 256}) {
+            TuneResult t;
+            t.variant = nr;
+            t.block = blk;
+            cands.push_back(t);
+        }
+    }
+    void *scratch = nullptr;
+    auto run = [&](const TuneResult &t, bool trial) -> int {
+        if (!trial) return mrhs_dispatch(g, s, prec, recon, m, t.variant, t.block, xpay);
+        if (!scratch && cudaMalloc(&scratch, m.fbytes * nrhs) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(PLQCD_ERR_NOMEM, "tune: scratch allocation failed");
+        }
+        dev::MrhsArgs tm = m;
+        tm.out = static_cast<char *>(scratch);
+        return mrhs_dispatch(g, s, prec, recon, tm, t.variant, t.block, xpay);
+    };
+    int rc = tune_launch(key, s, cands, run);
+    if (scratch) {
+        cudaStreamSynchronize(s);
+        cudaFree(scratch);
+    }
+    return rc;
+}
+
+}  // namespace plqcd
+
+using namespace plqcd;
+
+static int mrhs_common(plqcd_lattice *lat, const plqcd_gauge *gf, int prec) {
+    if (!lat || !gf) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: null lattice or gauge");
+    PLQCD_CUDA_TRY(cudaSetDevice(lat->device));
+    if (gf->lat->geom.Vh != lat->geom.Vh) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: gauge of another lattice");
+    if (gf->prec != prec) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: spinor precision != gauge precision");
+    return PLQCD_OK;
+}
+
+extern "C" int plqcd_dslash_mrhs(plqcd_lattice *lat, const plqcd_gauge *gf, void *out, const void *in, int nrhs,
+                                 int out_parity, int prec, unsigned flags) {
+    clear_error();
+    PLQCD_TRY(mrhs_common(lat, gf, prec));
+    if (!out || !in || (out_parity != 0 && out_parity != 1) || (flags & PLQCD_DSLASH_COMPAT))
+        return set_error(PLQCD_ERR_ARG, "dslash_mrhs: bad argument");
+    return launch_dslash_mrhs(lat->geom, lat->stream, gf->data, prec, gf->recon, out, in, nrhs, out_parity, flags,
+                              1.0, nullptr, 0.0);
+}
+
+extern "C" int plqcd_dslash_mrhs_xpay(plqcd_lattice *lat, const plqcd_gauge *gf, void *out, const void *in, int nrhs,
+                                      int out_parity, int prec, unsigned flags, double a, const void *x, double b) {
+    clear_error();
+    PLQCD_TRY(mrhs_common(lat, gf, prec));
+    if (!out || !in || !x || (out_parity != 0 && out_parity != 1) || (flags & PLQCD_DSLASH_COMPAT))
+        return set_error(PLQCD_ERR_ARG, "dslash_mrhs_xpay: bad argument");
+    return launch_dslash_mrhs(lat->geom, lat->stream, gf->data, prec, gf->recon, out, in, nrhs, out_parity, flags, a,
+                              x, b);
+}

@@ -111,6 +111,9 @@ struct DslashCall {
     long h_begin = 0, h_count = -1;
 };
 int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c);
+// nrhs one-parity fields back to back: out = a * H in (+ b * x if x != null)
+int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
+                       const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b);
 
 // device workspace of at least `bytes`, owned by the lattice (cg.cu)
 int lattice_workspace(plqcd_lattice *lat, size_t bytes, void **out);

@@ -1,0 +1,81 @@
+"""Batched multi-RHS, multi-lattice CG (plqcd_invert_cg_batch), eager and as
+one CUDA-graph launch: every RHS must reach the FP64 residual and agree with
+the single-RHS solver; residuals are re-checked on the host with the
+oracle's full-lattice operator."""
+import numpy as np
+import pytest
+
+import plqcd_b200 as P
+from oracle import oracle as O
+from tests.gpu_util import dev_bytes, field_to_host, new_lattice
+
+pytestmark = pytest.mark.gpu
+KAPPA = 0.12
+
+
+def _lattice_item(L, nrhs, seed, sloppy):
+    lat = new_lattice(L)
+    g64 = P.Gauge(lat, P.F64, 18)
+    g64.random(seed)
+    gs = None
+    if sloppy != P.F64:
+        gs = P.Gauge(lat, sloppy, 12)
+        gs.copy_from(g64)
+    bs = lat.spinor_bytes(P.F64)
+    be, bo, xe, xo = (dev_bytes(nrhs * bs) for _ in range(4))
+    for r in range(nrhs):
+        lat.spinor_gaussian(be[r * bs:(r + 1) * bs], P.F64, 0, seed * 100 + r)
+        lat.spinor_gaussian(bo[r * bs:(r + 1) * bs], P.F64, 1, seed * 100 + r)
+    return dict(lat=lat, g64=g64, g_sloppy=gs, nrhs=nrhs, x_even=xe, x_odd=xo, b_even=be, b_odd=bo)
+
+
+def _host_field(item, blk_e, blk_o, r):
+    lat = item["lat"]
+    bs = lat.spinor_bytes(P.F64)
+    sl = slice(r * bs, (r + 1) * bs)
+    f = field_to_host(lat, blk_e[sl], P.F64, 0)
+    f[lat.V // 2:] = field_to_host(lat, blk_o[sl], P.F64, 1)[lat.V // 2:]
+    return f
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+@pytest.mark.parametrize("sloppy", [P.F16, P.F32, P.F64])
+def test_batch_solves_every_rhs(cuda, restatement, use_graph, sloppy):
+    items = [_lattice_item((8, 8, 8, 16), 3, 3, sloppy), _lattice_item((4, 6, 4, 8), 2, 5, sloppy)]
+    info, res = P.invert_cg_batch(items, P.cg_param(kappa=KAPPA, tol=1e-10, sloppy_prec=sloppy), use_graph)
+    assert info.converged and info.max_schur_residual <= 1e-10
+    assert info.graph_launches == (1 if use_graph else 0)
+    assert max(res) < 1e-9 and len(res) == 5
+    if sloppy != P.F64:
+        assert info.reliable_updates >= 1
+    for it in items:
+        lat = it["lat"]
+        u = it["g64"].store_host()
+        bs = lat.spinor_bytes(P.F64)
+        for r in range(it["nrhs"]):
+            x = _host_field(it, it["x_even"], it["x_odd"], r)
+            b = _host_field(it, it["b_even"], it["b_odd"], r)
+            rr = np.linalg.norm(b - restatement.wilson(lat.dims, u, x, KAPPA)) / np.linalg.norm(b)
+            assert rr < 1e-9
+            # the single-RHS solver gives the same solution
+            xe1, xo1 = dev_bytes(bs), dev_bytes(bs)
+            sl = slice(r * bs, (r + 1) * bs)
+            P.invert_cg(lat, it["g64"], None, xe1, xo1, it["b_even"][sl], it["b_odd"][sl],
+                        P.cg_param(kappa=KAPPA, tol=1e-10))
+            x1 = field_to_host(lat, xe1, P.F64, 0)
+            x1[lat.V // 2:] = field_to_host(lat, xo1, P.F64, 1)[lat.V // 2:]
+            assert np.linalg.norm(x - x1) / np.linalg.norm(x1) < 1e-8
+
+
+def test_batch_reports_non_convergence(cuda):
+    items = [_lattice_item((4, 4, 4, 8), 2, 7, P.F32)]
+    info, res = P.invert_cg_batch(items, P.cg_param(kappa=KAPPA, tol=1e-10, sloppy_prec=P.F32, max_iter=2),
+                                  True, raise_on_error=False)
+    assert not info.converged and info.iterations == 2
+    assert "not converged" in P.last_error()
+
+
+def test_batch_rejects_mismatched_sloppy_gauge(cuda):
+    it = _lattice_item((4, 4, 4, 8), 1, 9, P.F16)
+    info, _ = P.invert_cg_batch([it], P.cg_param(kappa=KAPPA, sloppy_prec=P.F32), True, raise_on_error=False)
+    assert "sloppy gauge does not match" in P.last_error()

@@ -324,3 +324,36 @@ def test_spinor_norm2_batched(cuda, prec):
     lat.spinor_norm2(block, prec, nf, out2)
     lat.synchronize()
     assert bool((out == out2).all())  # fixed summation order: reproducible
+
+
+@pytest.mark.parametrize("prec,recon,tol", [(P.F64, 18, 1e-14), (P.F64, 12, 1e-13), (P.F32, 12, 1e-6),
+                                            (P.F16, 12, 1e-3), (P.BF16, 12, 1e-2)])
+@pytest.mark.parametrize("nrhs", [1, 3, 8])
+def test_multi_rhs_equals_single_rhs(cuda, prec, recon, tol, nrhs):
+    """Each field of a multi-RHS block gives what the single-RHS kernel gives
+    (same arithmetic; tolerance covers compiler contraction differences)."""
+    L = (8, 4, 6, 8)
+    lat, g64, u = _device_setup(L, 13)
+    g = P.Gauge(lat, prec, recon)
+    g.copy_from(g64)
+    bs = lat.spinor_bytes(prec)
+    blk_in, blk_out, blk_x = dev_bytes(nrhs * bs), dev_bytes(nrhs * bs), dev_bytes(nrhs * bs)
+    for r in range(nrhs):
+        lat.spinor_gaussian(blk_in[r * bs:(r + 1) * bs], prec, 1, 100 + r)
+        lat.spinor_gaussian(blk_x[r * bs:(r + 1) * bs], prec, 0, 200 + r)
+    for xpay in (False, True):
+        flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT if xpay else 0
+        if xpay:
+            lat.dslash_mrhs_xpay(g, blk_out, blk_in, nrhs, 0, prec, -0.0144, blk_x, 1.0, flags)
+        else:
+            lat.dslash_mrhs(g, blk_out, blk_in, nrhs, 0, prec)
+        for r in range(nrhs):
+            one = dev_bytes(bs)
+            sl = slice(r * bs, (r + 1) * bs)
+            if xpay:
+                lat.dslash_xpay(g, one, blk_in[sl], 0, prec, -0.0144, blk_x[sl], 1.0, flags)
+            else:
+                lat.dslash(g, one, blk_in[sl], 0, prec)
+            a = field_to_host(lat, blk_out[sl], prec, 0)[: lat.V // 2]
+            b = field_to_host(lat, one, prec, 0)[: lat.V // 2]
+            assert relmax(a, b) <= tol, (r, xpay, relmax(a, b))
