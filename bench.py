@@ -331,6 +331,11 @@ def run_ours(args, d: Dist):
     # ---- even/odd CG: FP64 vs mixed precision, time to 1e-10 ----------------
     cg = run_cg(torch, P, lat, g64, buf, args) if not args.skip_cg else None
     del fe, fo, oe_, oo_
+    mrhs = run_mrhs(torch, P, lat, g64, args) if not args.skip_batch else None
+    # ---- batched multi-RHS, multi-lattice solve in one graph launch ----------
+    batch = None
+    if not args.skip_batch:
+        batch = run_batch(torch, P, d, args, cg["f64"]["seconds"] if cg else None)
     # ---- reduced precision at 48^3x96: error against FP64 --------------------
     reduced = run_reduced(torch, P, d, args) if not args.skip_reduced else None
 
@@ -364,6 +369,8 @@ def run_ours(args, d: Dist):
         "f32": fp32,
         "e2e": e2e,
         "cg": cg,
+        "mrhs_dslash": mrhs,
+        "batch": batch,
         "reduced_precision": reduced,
         "gpu_launches": K,
         "clocks": clocks,
@@ -452,7 +459,8 @@ def run_cg(torch, P, lat, g64, buf, args):
         # warm-up: a few iterations tune every kernel configuration the solve uses
         P.invert_cg(lat, g64, gs, xe, xo, be, bo, P.cg_param(kappa=kappa, tol=tol, max_iter=4, sloppy_prec=prec),
                     raise_on_error=False)
-        info = P.invert_cg(lat, g64, gs, xe, xo, be, bo, P.cg_param(kappa=kappa, tol=tol, sloppy_prec=prec))
+        info = P.invert_cg(lat, g64, gs, xe, xo, be, bo,
+                           P.cg_param(kappa=kappa, tol=tol, sloppy_prec=prec, delta=args.delta))
         out[name] = {"iterations": info.iterations, "reliable_updates": info.reliable_updates,
                      "seconds": round(info.seconds, 5), "schur_residual": info.schur_residual,
                      "true_residual": info.true_residual}
@@ -464,11 +472,114 @@ def run_cg(torch, P, lat, g64, buf, args):
     for name in ("f32", "f16"):
         diff = torch.cat([xs[name][0], xs[name][1]]).view(torch.float64) - x64
         out[name]["error_vs_f64"] = float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(x64))
-    best = min(("f32", "f16"), key=lambda n: out[n]["seconds"])
+    # the F16 solve again, as one CUDA-graph launch (no host round trips)
+    gs16 = P.Gauge(lat, P.F16, 12)
+    gs16.copy_from(g64)
+    xe, xo = buf(P.F64), buf(P.F64)
+    item = dict(lat=lat, g64=g64, g_sloppy=gs16, nrhs=1, x_even=xe, x_odd=xo, b_even=be, b_odd=bo)
+    P.invert_cg_batch([item], P.cg_param(kappa=kappa, tol=tol, sloppy_prec=P.F16, max_iter=3), True,
+                      raise_on_error=False)
+    ig, res = P.invert_cg_batch([item], P.cg_param(kappa=kappa, tol=tol, sloppy_prec=P.F16, delta=args.delta), True)
+    lat.synchronize()
+    diff = torch.cat([xe, xo]).view(torch.float64) - x64
+    out["f16_graph"] = {"iterations": ig.iterations, "reliable_updates": ig.reliable_updates,
+                        "seconds": round(ig.seconds, 5), "schur_residual": ig.max_schur_residual,
+                        "true_residual": res[0], "graph_launches": ig.graph_launches,
+                        "error_vs_f64": float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(x64))}
+    del gs16
+    best = min(("f32", "f16", "f16_graph"), key=lambda n: out[n]["seconds"])
     out["speedup_mixed_vs_f64"] = round(out["f64"]["seconds"] / out[best]["seconds"], 3)
     out["best_mixed"] = best
     out["config"] = {"lattice": list(lat.dims), "kappa": kappa, "tol": tol, "source": "Gaussian",
                      "operator": "even/odd preconditioned Mhat^dag Mhat, CG"}
+    return out
+
+
+def run_mrhs(torch, P, lat, g64, args, nrhs=8):
+    """Multi-RHS hopping throughput at the benchmark lattice: bytes per site
+    and RHS = 2 * spinor + 8 * link / nrhs."""
+    res = {"nrhs": nrhs}
+    for name, prec, recon, sb, lb in (("f64_18", P.F64, 18, 192, 144), ("f32_12", P.F32, 12, 96, 48),
+                                      ("f16_12", P.F16, 12, 52, 24)):
+        g = g64 if (prec, recon) == (P.F64, 18) else P.Gauge(lat, prec, recon)
+        if g is not g64:
+            g.copy_from(g64)
+        bs = lat.spinor_bytes(prec)
+        a = torch.empty(nrhs * bs, dtype=torch.uint8, device="cuda")
+        o = torch.empty(nrhs * bs, dtype=torch.uint8, device="cuda")
+        for r in range(nrhs):
+            lat.spinor_gaussian(a[r * bs:(r + 1) * bs], prec, 1, 900 + r)
+        t = time_kernel(torch, lambda: lat.dslash_mrhs(g, o, a, nrhs, P.EVEN, prec), 20, 3) / 20 / 1e3
+        per = lat.Vh * nrhs
+        res[name] = {"gflops": round(per * FLOP_PER_SITE / t / 1e9, 1),
+                     "gbs": round(per * (2 * sb + 8 * lb / nrhs) / t / 1e9, 1),
+                     "site_rhs_per_s": per / t}
+        del a, o
+        if g is not g64:
+            del g
+    return res
+
+
+def run_batch(torch, P, d: Dist, args, f64_single_seconds: float | None):
+    """Batched multi-RHS solves in one graph launch: 16^3x32 (32 RHS),
+    24^3x48 (16 RHS), 32^3x64 (8 RHS), each with its own random SU(3) field
+    and Gaussian sources, kappa = 0.12, mixed precision (F16 inner operator)
+    to 1e-10; against the same solves one at a time in FP64."""
+    kappa, tol = 0.12, 1e-10
+    spec = [((16, 16, 16, 32), 32), ((24, 24, 24, 48), 16), ((32, 32, 32, 64), 8)]
+    stream = torch.cuda.current_stream().cuda_stream
+    items = []
+    for k, (L, n) in enumerate(spec):
+        lat = P.Lattice(L, d.local, stream)
+        g64 = P.Gauge(lat, P.F64, 18)
+        g64.random(31 + k)
+        gs = P.Gauge(lat, P.F16, 12)
+        gs.copy_from(g64)
+        bs = lat.spinor_bytes(P.F64)
+        blk = [torch.empty(n * bs, dtype=torch.uint8, device="cuda") for _ in range(4)]
+        for r in range(n):
+            lat.spinor_gaussian(blk[0][r * bs:(r + 1) * bs], P.F64, 0, 1000 * k + r)
+            lat.spinor_gaussian(blk[1][r * bs:(r + 1) * bs], P.F64, 1, 1000 * k + r)
+        items.append(dict(lat=lat, g64=g64, g_sloppy=gs, nrhs=n, b_even=blk[0], b_odd=blk[1], x_even=blk[2],
+                          x_odd=blk[3]))
+    prm = P.cg_param(kappa=kappa, tol=tol, sloppy_prec=P.F16, delta=args.delta)
+    P.invert_cg_batch(items, P.cg_param(kappa=kappa, tol=tol, sloppy_prec=P.F16, max_iter=3), True,
+                      raise_on_error=False)  # warm-up: tunes every launch configuration
+    info, res = P.invert_cg_batch(items, prm, True)
+    site_rhs = sum(it["lat"].V * it["nrhs"] for it in items)
+    out = {"lattices": [[list(L), n] for L, n in spec], "kappa": kappa, "tol": tol, "sloppy": "f16_12",
+           "graph_launches": info.graph_launches, "iterations": info.iterations,
+           "reliable_updates": info.reliable_updates, "seconds": round(info.seconds, 4),
+           "max_schur_residual": info.max_schur_residual, "max_true_residual": info.max_true_residual,
+           "site_rhs_per_s": site_rhs / info.seconds}
+    # the same solves one at a time, FP64 CG
+    seq = 0.0
+    for it in items:
+        lat, bs = it["lat"], it["lat"].spinor_bytes(P.F64)
+        xe, xo = torch.empty(bs, dtype=torch.uint8, device="cuda"), torch.empty(bs, dtype=torch.uint8, device="cuda")
+        for r in range(it["nrhs"]):
+            sl = slice(r * bs, (r + 1) * bs)
+            if r == 0:  # tune this lattice's FP64 kernels outside the timing
+                P.invert_cg(lat, it["g64"], None, xe, xo, it["b_even"][sl], it["b_odd"][sl],
+                            P.cg_param(kappa=kappa, tol=tol, max_iter=3), raise_on_error=False)
+            inf1 = P.invert_cg(lat, it["g64"], None, xe, xo, it["b_even"][sl], it["b_odd"][sl],
+                               P.cg_param(kappa=kappa, tol=tol))
+            seq += inf1.seconds
+    out["sequential_f64_seconds"] = round(seq, 4)
+    out["sequential_f64_site_rhs_per_s"] = site_rhs / seq
+    out["speedup_vs_sequential_f64"] = round(seq / info.seconds, 3)
+    # multi-RHS mixed CG at 32^3x64 (8 RHS) alone, per RHS, against one plain FP64 CG
+    it = items[2]
+    info8, _ = P.invert_cg_batch([it], prm, True)
+    out["mrhs_32x32x32x64"] = {"nrhs": it["nrhs"], "seconds": round(info8.seconds, 4),
+                               "seconds_per_rhs": round(info8.seconds / it["nrhs"], 5),
+                               "max_true_residual": info8.max_true_residual}
+    if f64_single_seconds:
+        out["mrhs_32x32x32x64"]["speedup_per_rhs_vs_plain_f64_cg"] = round(
+            f64_single_seconds / (info8.seconds / it["nrhs"]), 3)
+    for it in items:
+        it["lat"].synchronize()
+    items.clear()
     return out
 
 
@@ -524,6 +635,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--skip-cg", action="store_true")
     ap.add_argument("--skip-reduced", action="store_true")
+    ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update threshold of the mixed solvers")
     ap.add_argument("--lattice", default=",".join(map(str, L_BENCH)),
                     help="L0,L1,L2,L3 of the hopping-matrix workload (default 32,32,32,64)")
     ap.add_argument("--only", choices=["all", "dslash"], default="all",
