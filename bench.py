@@ -636,7 +636,7 @@ def main():
     ap.add_argument("--skip-cg", action="store_true")
     ap.add_argument("--skip-reduced", action="store_true")
     ap.add_argument("--skip-batch", action="store_true")
-    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update threshold of the mixed solvers")
+    ap.add_argument("--delta", type=float, default=0.01, help="reliable-update threshold of the mixed solvers")
     ap.add_argument("--lattice", default=",".join(map(str, L_BENCH)),
                     help="L0,L1,L2,L3 of the hopping-matrix workload (default 32,32,32,64)")
     ap.add_argument("--only", choices=["all", "dslash"], default="all",

@@ -93,7 +93,7 @@ extern "C" void plqcd_cg_param_default(plqcd_cg_param *p) {
     p->tol = 1e-10;
     p->max_iter = 10000;
     p->sloppy_prec = PLQCD_F64;
-    p->delta = 0.1;
+    p->delta = 0.01;
     p->verbose = 0;
 }
 
@@ -177,6 +177,11 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
         double target = prm->tol * prm->tol * rhs2;  // normal-equation trigger for convergence checks
         const double delta2 = prm->delta * prm->delta;
         const bool mixed = ps != PLQCD_F64;
+        // a sloppy recursion that stops reducing its residual (16-bit storage
+        // with a tiny delta) would never trigger an update: force one after
+        // this many iterations without
+        const int max_sloppy_run = 100;
+        int last_reliable = 0;
 
         for (int it = 1; it <= prm->max_iter; it++) {
             // Ap = Mhat^dag Mhat p ; pAp = |Mhat p|^2
@@ -192,7 +197,7 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
                 rc = set_error(PLQCD_ERR_NOCONV, "plqcd_invert_cg: residual is not finite at iteration %d", it);
                 break;
             }
-            const bool reliable = (mixed && rr < delta2 * maxrr) || rr <= target;
+            const bool reliable = (mixed && rr < delta2 * maxrr) || rr <= target || it - last_reliable >= max_sloppy_run;
             if (reliable) {
                 // defect correction in FP64
                 if ((rc = blas_accum_zero(g, s, x_even, xs, xprec))) break;
@@ -203,6 +208,7 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
                 if ((rc = launch_spinor_convert(g, s, rs, ps, t64, PLQCD_F64))) break;
                 inf.f64_hops += 4;
                 inf.reliable_updates++;
+                last_reliable = it;
                 if ((rc = read_state())) break;
                 sr2 = hst->sr2;
                 maxrr = hst->rr;

@@ -113,6 +113,16 @@ template <>
 struct SpinorIO<PLQCD_F64> {
     using real = double;
     static constexpr int bytes_per_site = 192;
+    // raw loads: values as stored plus the factor that restores them (1 here)
+    static constexpr bool kScaled = false;
+    __device__ static __forceinline__ void load_raw(const void *b, long Vh, long h, cx<double> s[12], double &n) {
+        load(b, Vh, h, s);
+        n = 1.0;
+    }
+    __device__ static __forceinline__ void load_staged_raw(const uint4 *s0, int B, cx<double> s[12], double &n) {
+        load_staged(s0, B, s);
+        n = 1.0;
+    }
     __device__ static __forceinline__ void load(const void *base, long Vh, long h, cx<double> s[12]) {
         const double2 *p = static_cast<const double2 *>(base) + h;
 #pragma unroll
@@ -147,6 +157,15 @@ template <>
 struct SpinorIO<PLQCD_F32> {
     using real = float;
     static constexpr int bytes_per_site = 96;
+    static constexpr bool kScaled = false;
+    __device__ static __forceinline__ void load_raw(const void *b, long Vh, long h, cx<float> s[12], float &n) {
+        load(b, Vh, h, s);
+        n = 1.0f;
+    }
+    __device__ static __forceinline__ void load_staged_raw(const uint4 *s0, int B, cx<float> s[12], float &n) {
+        load_staged(s0, B, s);
+        n = 1.0f;
+    }
     __device__ static __forceinline__ void load(const void *base, long Vh, long h, cx<float> s[12]) {
         const float4 *p = static_cast<const float4 *>(base) + h;
 #pragma unroll
@@ -184,6 +203,35 @@ template <int PREC>
 struct SpinorIO16 {
     using real = float;
     static constexpr int bytes_per_site = 52;
+    // raw loads return the stored values unscaled and the site norm, so
+    // the hopping kernels can apply the norm inside their final FMAs
+    static constexpr bool kScaled = true;
+    __device__ static __forceinline__ void unpack3(const uint4 v[3], cx<float> s[12]) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            float2 a = Half2<PREC>::unpack(v[k].x), b = Half2<PREC>::unpack(v[k].y);
+            float2 c = Half2<PREC>::unpack(v[k].z), d = Half2<PREC>::unpack(v[k].w);
+            s[4 * k + 0] = {a.x, a.y};
+            s[4 * k + 1] = {b.x, b.y};
+            s[4 * k + 2] = {c.x, c.y};
+            s[4 * k + 3] = {d.x, d.y};
+        }
+    }
+    __device__ static __forceinline__ void load_raw(const void *base, long Vh, long h, cx<float> s[12], float &n) {
+        const uint4 *p = static_cast<const uint4 *>(base) + h;
+        uint4 v[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = ld_ro(p + k * Vh);
+        n = ld_ro(norms(base, Vh) + h);
+        unpack3(v, s);
+    }
+    __device__ static __forceinline__ void load_staged_raw(const uint4 *s0, int B, cx<float> s[12], float &n) {
+        uint4 v[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = s0[k * B];
+        n = *reinterpret_cast<const float *>(s0 + 3 * B);
+        unpack3(v, s);
+    }
     __device__ static __forceinline__ const float *norms(const void *base, long Vh) {
         return reinterpret_cast<const float *>(static_cast<const uint4 *>(base) + 3 * Vh);
     }

@@ -36,7 +36,8 @@ __device__ __forceinline__ void hop_dir(cx<typename SIO::real> acc[12], const vo
                                         typename SIO::real sg_in) {
     using R = typename SIO::real;
     cx<R> s[12];
-    SIO::load(in, Vh, h_nbr, s);
+    R n;
+    SIO::load_raw(in, Vh, h_nbr, s, n);
     cx<R> h0[3], h1[3];
     project<MU, R>(s, FWD ? sg_in : -sg_in, h0, h1);
     cx<R> U[9];
@@ -51,7 +52,7 @@ __device__ __forceinline__ void hop_dir(cx<typename SIO::real> acc[12], const vo
     }
     // The reference as shipped drops every forward contribution to spins
     // 2,3 (its backward mu=0 step overwrites them, include/su3.h:135-138).
-    accumulate<MU, FWD ? 1 : -1, !(COMPAT && FWD), R>(acc, c0, c1);
+    accumulate<MU, FWD ? 1 : -1, !(COMPAT && FWD), SIO::kScaled, R>(acc, c0, c1, n);
 }
 
 template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
@@ -64,13 +65,14 @@ __global__ void __launch_bounds__(256) k_dslash(const DslashArgs a) {
         h = (long)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
     } else {
         par = a.out_parity;
-        h = a.h_begin + (long)blockIdx.x * blockDim.x + threadIdx.x;
+        h = a.h_begin + (long)(blockIdx.x / a.nrhs) * blockDim.x + threadIdx.x;
     }
     if (h >= a.h_end) return;
     // selects, not a dynamic index into the parameter arrays (which would
     // copy them to local memory)
-    const void *in = (FULL && par == 0) ? a.in[1] : a.in[0];
-    void *out = (FULL && par == 1) ? a.out[1] : a.out[0];
+    const long roff = FULL ? 0 : (long)(blockIdx.x % a.nrhs) * a.fbytes;  // RHS of this block
+    const void *in = (FULL && par == 0) ? a.in[1] : static_cast<const char *>(a.in[0]) + roff;
+    void *out = (FULL && par == 1) ? a.out[1] : static_cast<char *>(a.out[0]) + roff;
     const long Vh = a.Vh;
     const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
     const Coords c = site_coords(h, par, L0h, L1, L2);
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(256) k_dslash(const DslashArgs a) {
     const R aup = (R)a.a_up, alow = (R)a.a_low;
     if (XPAY) {
         cx<R> xv[12];
-        SIO::load(a.x, Vh, h, xv);
+        SIO::load(static_cast<const char *>(a.x) + roff, Vh, h, xv);
         const R b = (R)a.b;
 #pragma unroll
         for (int k = 0; k < 12; k++) {
@@ -146,11 +148,12 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
         h = (long)(blockIdx.x >> 1) * B + threadIdx.x;
     } else {
         par = a.out_parity;
-        h = a.h_begin + (long)blockIdx.x * B + threadIdx.x;
+        h = a.h_begin + (long)(blockIdx.x / a.nrhs) * B + threadIdx.x;
     }
     if (h >= a.h_end) return;  // no block-level barrier below
-    const void *in = (FULL && par == 0) ? a.in[1] : a.in[0];
-    void *out = (FULL && par == 1) ? a.out[1] : a.out[0];
+    const long roff = FULL ? 0 : (long)(blockIdx.x % a.nrhs) * a.fbytes;  // RHS of this block
+    const void *in = (FULL && par == 0) ? a.in[1] : static_cast<const char *>(a.in[0]) + roff;
+    void *out = (FULL && par == 1) ? a.out[1] : static_cast<char *>(a.out[0]) + roff;
     const long Vh = a.Vh;
     const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
     const Coords c = site_coords(h, par, L0h, L1, L2);
@@ -194,9 +197,10 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
         cp_async_wait<ST - 1>();
         const uint4 *s0 = smem + threadIdx.x + (d % ST) * NS * B;
         cx<R> s[12], U[9];
-        SIO::load_staged(s0, B, s);
+        R n;
+        SIO::load_staged_raw(s0, B, s, n);
         LIO::load_staged(s0 + SIO::NSLOT * B, B, U);
-        compute_dir_n<COMPAT, R>(d, acc, s, U, sg);
+        compute_dir_n<COMPAT, SIO::kScaled, R>(d, acc, s, U, sg, n);
         // the slot just consumed is refilled only after its values were used
         if (d + ST < 8) issue(d + ST);
         cp_async_commit();
@@ -205,7 +209,7 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
     const R aup = (R)a.a_up, alow = (R)a.a_low;
     if (XPAY) {
         cx<R> xv[12];
-        SIO::load(a.x, Vh, h, xv);
+        SIO::load(static_cast<const char *>(a.x) + roff, Vh, h, xv);
         const R b = (R)a.b;
 #pragma unroll
         for (int k = 0; k < 12; k++) {
@@ -223,7 +227,7 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
 
 template <class SIO, class LIO, int ST, bool COMPAT, bool XPAY, bool FULL>
 static int launch_pipe(const Geom &g, cudaStream_t s, const DslashArgs &a, int block) {
-    long nblk = (a.h_end - a.h_begin + block - 1) / block;
+    long nblk = (a.h_end - a.h_begin + block - 1) / block * a.nrhs;
     if (FULL) nblk *= 2;
     constexpr int NS = SIO::NSLOT + LIO::NSLOT;
     const size_t smem = (size_t)ST * NS * 16 * block;
@@ -252,7 +256,7 @@ static int launch_t(const Geom &g, cudaStream_t s, const DslashArgs &a, int vari
 
 template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
 static int launch_direct(const Geom &g, cudaStream_t s, const DslashArgs &a, int block) {
-    long nblk = (a.h_end - a.h_begin + block - 1) / block;
+    long nblk = (a.h_end - a.h_begin + block - 1) / block * a.nrhs;
     if (FULL) nblk *= 2;
     k_dslash<SIO, LIO, COMPAT, XPAY, FULL><<<(unsigned)nblk, block, 0, s>>>(a);
     PLQCD_CUDA_TRY(cudaGetLastError());
@@ -283,9 +287,41 @@ static int env_int(const char *name, int dflt) {
 static int dispatch(const Geom &g, cudaStream_t s, const DslashCall &c, const dev::DslashArgs &a, int variant,
                     int block);
 
+static int build_args(const Geom &g, const DslashCall &c, dev::DslashArgs &a);
+static int tune_dslash(const Geom &g, cudaStream_t s, const DslashCall &c, const dev::DslashArgs &a,
+                       const char *key);
+
+// one launch with an explicit configuration (no tuning)
+int launch_dslash_config(const Geom &g, cudaStream_t s, const DslashCall &c, int variant, int block) {
+    dev::DslashArgs a{};
+    PLQCD_TRY(build_args(g, c, a));
+    return dispatch(g, s, c, a, variant, block);
+}
+
 int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
     dev::DslashArgs a{};
+    PLQCD_TRY(build_args(g, c, a));
+    const bool compat = (c.flags & PLQCD_DSLASH_COMPAT) != 0;
+
+    // explicit configuration (block from the call, or the environment for
+    // experiments) bypasses the tuner
+    const int env_block = env_int("PLQCD_DSLASH_BLOCK", 0), env_var = env_int("PLQCD_DSLASH_STAGES", -1);
+    if (c.block > 0 || env_block > 0 || env_var >= 0) {
+        int block = c.block > 0 ? c.block : (env_block > 0 ? env_block : 128);
+        return dispatch(g, s, c, a, env_var >= 0 ? env_var : 2, block);
+    }
+    char key[256];
+    snprintf(key, sizeof key, "%sdslash|p%d|r%d|%s%s%s|%dx%dx%dx%d|n%d", device_tag().c_str(), c.prec, c.recon,
+             c.full ? "full" : "half", c.x ? "+xpay" : "", compat ? "+compat" : "", g.L[0], g.L[1], g.L[2], g.L[3],
+             c.nrhs);
+    return tune_dslash(g, s, c, a, key);
+}
+
+static int build_args(const Geom &g, const DslashCall &c, dev::DslashArgs &a) {
     a.gauge = c.gauge;
+    if (c.nrhs < 1 || (c.full && c.nrhs != 1)) return set_error(PLQCD_ERR_ARG, "dslash: nrhs = %d invalid", c.nrhs);
+    a.nrhs = c.nrhs;
+    a.fbytes = (long)spinor_parity_bytes(g.Vh, c.prec);
     if (c.full) {
         a.in[0] = c.in;
         a.in[1] = c.in2;
@@ -314,17 +350,11 @@ int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
     const bool compat = (c.flags & PLQCD_DSLASH_COMPAT) != 0;
     if (c.full && (compat || c.x || (c.flags & (PLQCD_DSLASH_G5_IN | PLQCD_DSLASH_G5_OUT))))
         return set_error(PLQCD_ERR_ARG, "dslash_full: flags and xpay are not supported in full-lattice mode");
+    return PLQCD_OK;
+}
 
-    // explicit configuration (block from the call, or the environment for
-    // experiments) bypasses the tuner
-    const int env_block = env_int("PLQCD_DSLASH_BLOCK", 0), env_var = env_int("PLQCD_DSLASH_STAGES", -1);
-    if (c.block > 0 || env_block > 0 || env_var >= 0) {
-        int block = c.block > 0 ? c.block : (env_block > 0 ? env_block : 128);
-        return dispatch(g, s, c, a, env_var >= 0 ? env_var : 2, block);
-    }
-    char key[256];
-    snprintf(key, sizeof key, "%sdslash|p%d|r%d|%s%s%s|%dx%dx%dx%d", device_tag().c_str(), c.prec, c.recon,
-             c.full ? "full" : "half", c.x ? "+xpay" : "", compat ? "+compat" : "", g.L[0], g.L[1], g.L[2], g.L[3]);
+static int tune_dslash(const Geom &g, cudaStream_t s, const DslashCall &c, const dev::DslashArgs &a,
+                       const char *key) {
     std::vector<TuneResult> cands;
     for (int v : {2, 0, 3})
         for (int b : {64, 128, 256}) {
@@ -338,7 +368,7 @@ int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
     void *scratch[2] = {nullptr, nullptr};
     auto run = [&](const TuneResult &r, bool trial) -> int {
         if (!trial) return dispatch(g, s, c, a, r.variant, r.block);
-        size_t bytes = spinor_parity_bytes(g.Vh, c.prec);
+        size_t bytes = spinor_parity_bytes(g.Vh, c.prec) * c.nrhs;
         for (int k = 0; k < (c.full ? 2 : 1); k++)
             if (!scratch[k] && cudaMalloc(&scratch[k], bytes) != cudaSuccess) {
                 cudaGetLastError();

@@ -23,6 +23,10 @@ struct DslashArgs {
     int out_parity;
     double a_up, a_low, b;
     double g5_in;       // +1 or -1: sign applied to input spins 2,3
+    // a block of nrhs fields (field r at base + r * fbytes), single parity
+    // only: blocks cover the RHS of a site range consecutively (RHS fastest)
+    int nrhs;
+    long fbytes;
 };
 
 // projection of the neighbour spinor onto the two upper spin components.
@@ -87,9 +91,36 @@ __device__ __forceinline__ void su3_dag_mul(const cx<R> U[9], const cx<R> v[3], 
     }
 }
 
-// rebuild of the lower spins from chi = (c0, c1); LS = +1 forward, -1 backward
-template <int MU, int LS, bool LOWER, typename R>
-__device__ __forceinline__ void accumulate(cx<R> acc[12], const cx<R> c0[3], const cx<R> c1[3]) {
+// rebuild of the lower spins from chi = (c0, c1); LS = +1 forward, -1 backward.
+// SC: chi still carries the neighbour's storage norm n (16-bit spinors are
+// loaded unscaled); it is applied here by fused multiply-adds, for free.
+template <int MU, int LS, bool LOWER, bool SC, typename R>
+__device__ __forceinline__ void accumulate(cx<R> acc[12], const cx<R> c0[3], const cx<R> c1[3], R n) {
+    if (SC) {
+        const R p = LS * n, q = -LS * n;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            acc[c] = {fma(n, c0[c].re, acc[c].re), fma(n, c0[c].im, acc[c].im)};
+            acc[3 + c] = {fma(n, c1[c].re, acc[3 + c].re), fma(n, c1[c].im, acc[3 + c].im)};
+            if (!LOWER) continue;
+            cx<R> &r2 = acc[6 + c];
+            cx<R> &r3 = acc[9 + c];
+            if (MU == 0) {
+                r2 = {fma(p, c0[c].re, r2.re), fma(p, c0[c].im, r2.im)};
+                r3 = {fma(p, c1[c].re, r3.re), fma(p, c1[c].im, r3.im)};
+            } else if (MU == 1) {
+                r2 = {fma(p, c1[c].im, r2.re), fma(q, c1[c].re, r2.im)};
+                r3 = {fma(p, c0[c].im, r3.re), fma(q, c0[c].re, r3.im)};
+            } else if (MU == 2) {
+                r2 = {fma(q, c1[c].re, r2.re), fma(q, c1[c].im, r2.im)};
+                r3 = {fma(p, c0[c].re, r3.re), fma(p, c0[c].im, r3.im)};
+            } else {
+                r2 = {fma(p, c0[c].im, r2.re), fma(q, c0[c].re, r2.im)};
+                r3 = {fma(q, c1[c].im, r3.re), fma(p, c1[c].re, r3.im)};
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         acc[c] = cadd(acc[c], c0[c]);
@@ -115,8 +146,11 @@ __device__ __forceinline__ void accumulate(cx<R> acc[12], const cx<R> c0[3], con
 
 // Projection, SU(3) product and rebuild of one direction on data already in
 // registers.
-template <int MU, bool FWD, bool COMPAT, typename R>
-__device__ __forceinline__ void compute_dir(cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg_in) {
+// The reference as shipped drops every forward contribution to spins 2,3
+// (its backward mu=0 step overwrites them, include/su3.h:135-138): COMPAT.
+// SC / n: see accumulate (n = 1 and unused when SC is false).
+template <int MU, bool FWD, bool COMPAT, bool SC, typename R>
+__device__ __forceinline__ void compute_dir(cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg_in, R n) {
     cx<R> h0[3], h1[3];
     project<MU, R>(s, FWD ? sg_in : -sg_in, h0, h1);
     cx<R> c0[3], c1[3];
@@ -127,21 +161,22 @@ __device__ __forceinline__ void compute_dir(cx<R> acc[12], const cx<R> s[12], co
         su3_dag_mul(U, h0, c0);
         su3_dag_mul(U, h1, c1);
     }
-    accumulate<MU, FWD ? 1 : -1, !(COMPAT && FWD), R>(acc, c0, c1);
+    accumulate<MU, FWD ? 1 : -1, !(COMPAT && FWD), SC, R>(acc, c0, c1, n);
 }
 
-template <bool COMPAT, typename R>
-__device__ __forceinline__ void compute_dir_n(int d, cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg) {
+template <bool COMPAT, bool SC, typename R>
+__device__ __forceinline__ void compute_dir_n(int d, cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg,
+                                              R n) {
     // d is a compile-time constant after unrolling, so this switch folds
     switch (d) {
-        case 0: compute_dir<0, true, COMPAT>(acc, s, U, sg); break;
-        case 1: compute_dir<1, true, COMPAT>(acc, s, U, sg); break;
-        case 2: compute_dir<2, true, COMPAT>(acc, s, U, sg); break;
-        case 3: compute_dir<3, true, COMPAT>(acc, s, U, sg); break;
-        case 4: compute_dir<0, false, COMPAT>(acc, s, U, sg); break;
-        case 5: compute_dir<1, false, COMPAT>(acc, s, U, sg); break;
-        case 6: compute_dir<2, false, COMPAT>(acc, s, U, sg); break;
-        default: compute_dir<3, false, COMPAT>(acc, s, U, sg); break;
+        case 0: compute_dir<0, true, COMPAT, SC>(acc, s, U, sg, n); break;
+        case 1: compute_dir<1, true, COMPAT, SC>(acc, s, U, sg, n); break;
+        case 2: compute_dir<2, true, COMPAT, SC>(acc, s, U, sg, n); break;
+        case 3: compute_dir<3, true, COMPAT, SC>(acc, s, U, sg, n); break;
+        case 4: compute_dir<0, false, COMPAT, SC>(acc, s, U, sg, n); break;
+        case 5: compute_dir<1, false, COMPAT, SC>(acc, s, U, sg, n); break;
+        case 6: compute_dir<2, false, COMPAT, SC>(acc, s, U, sg, n); break;
+        default: compute_dir<3, false, COMPAT, SC>(acc, s, U, sg, n); break;
     }
 }
 

@@ -80,8 +80,9 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs(const MrhsArgs a) {
         for (int r = 0; r < NR; r++) {
             if (r < nr) {
                 cx<R> s[12];
-                SIO::load(a.in + (size_t)(r0 + r) * a.fbytes, Vh, nb[d], s);
-                compute_dir_n<false, R>(d, acc[r], s, U, sg);
+                R n;
+                SIO::load_raw(a.in + (size_t)(r0 + r) * a.fbytes, Vh, nb[d], s, n);
+                compute_dir_n<false, SIO::kScaled, R>(d, acc[r], s, U, sg, n);
             }
         }
     }
@@ -181,7 +182,19 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
     char key[256];
     snprintf(key, sizeof key, "%sdslash_mrhs|p%d|r%d|%s|n%d|%dx%dx%dx%d", device_tag().c_str(), prec, recon,
              xpay ? "xpay" : "plain", nrhs, g.L[0], g.L[1], g.L[2], g.L[3]);
+    // two families of candidates: the RHS-tile kernel above (variant = tile
+    // size 1, 2, 4), and the single-RHS kernels with the RHS index folded
+    // into the grid, RHS fastest, so the blocks of one site range run
+    // together and share links through L2 (variant = 100 + single-RHS
+    // variant: 0 direct loads, 2/3 cp.async pipeline depth)
     std::vector<TuneResult> cands;
+    for (int v : {102, 100, 103})
+        for (int blk : {64, 128, 256}) {
+            TuneResult t;
+            t.variant = v;
+            t.block = blk;
+            cands.push_back(t);
+        }
     for (int nr : {2, 1, 4}) {
         if (nr == 4 && prec == PLQCD_F64) continue;
         if (nr > nrhs && nr != 1) continue;
@@ -192,16 +205,36 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
             cands.push_back(t);
         }
     }
+    DslashCall dc;
+    dc.gauge = gauge;
+    dc.prec = prec;
+    dc.recon = recon;
+    dc.out = out;
+    dc.in = in;
+    dc.out_parity = out_parity;
+    dc.flags = flags;
+    dc.x = x;
+    dc.a_up = dc.a_low = a;
+    dc.b = b;
+    dc.nrhs = nrhs;
     void *scratch = nullptr;
+    auto launch = [&](const TuneResult &t, char *dst) -> int {
+        if (t.variant >= 100) {
+            DslashCall c2 = dc;
+            c2.out = dst;
+            return launch_dslash_config(g, s, c2, t.variant - 100, t.block);
+        }
+        dev::MrhsArgs tm = m;
+        tm.out = dst;
+        return mrhs_dispatch(g, s, prec, recon, tm, t.variant, t.block, xpay);
+    };
     auto run = [&](const TuneResult &t, bool trial) -> int {
-        if (!trial) return mrhs_dispatch(g, s, prec, recon, m, t.variant, t.block, xpay);
+        if (!trial) return launch(t, static_cast<char *>(out));
         if (!scratch && cudaMalloc(&scratch, m.fbytes * nrhs) != cudaSuccess) {
             cudaGetLastError();
             return set_error(PLQCD_ERR_NOMEM, "tune: scratch allocation failed");
         }
-        dev::MrhsArgs tm = m;
-        tm.out = static_cast<char *>(scratch);
-        return mrhs_dispatch(g, s, prec, recon, tm, t.variant, t.block, xpay);
+        return launch(t, static_cast<char *>(scratch));
     };
     int rc = tune_launch(key, s, cands, run);
     if (scratch) {

@@ -109,8 +109,12 @@ struct DslashCall {
     int block = 0;             // 0 = library default
     // output half-sites [h_begin, h_begin + h_count) (single parity; -1 = all)
     long h_begin = 0, h_count = -1;
+    // single parity: in/out/x are blocks of nrhs fields back to back
+    int nrhs = 1;
 };
 int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c);
+// variant 0: direct loads, 2/3: cp.async pipeline depth; no tuning
+int launch_dslash_config(const Geom &g, cudaStream_t s, const DslashCall &c, int variant, int block);
 // nrhs one-parity fields back to back: out = a * H in (+ b * x if x != null)
 int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
                        const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b);

@@ -42,7 +42,7 @@ struct McgState {  // device arrays of length nrhs, plus reduction scratch
 
 struct McgControl {
     int iter, need_reliable, any_active, max_iter;
-    int reliable_count, pad0;
+    int reliable_count, last_reliable;  // iteration of the last reliable update
     double tol2, delta2;
 };
 
@@ -260,7 +260,10 @@ __global__ void k_ctl_iter(McgControl *c, const McgState *st, int nst, int mixed
         for (int f = threadIdx.x; f < st[s].nrhs; f += blockDim.x) {
             if (!st[s].active[f]) continue;
             const double rr = st[s].rr[f];
-            if ((mixed && rr < c->delta2 * st[s].maxrr[f]) || rr <= st[s].target[f] || !isfinite(rr))
+            // (an update is also forced after 100 iterations without one, in
+            // case a 16-bit recursion stops reducing its residual)
+            if ((mixed && rr < c->delta2 * st[s].maxrr[f]) || rr <= st[s].target[f] || !isfinite(rr) ||
+                c->iter - c->last_reliable >= 100)
                 atomicOr(&need, 1);
         }
     __syncthreads();
@@ -286,7 +289,10 @@ __global__ void k_ctl_reliable(McgControl *c, const McgState *st, int nst) {
                 st[s].target[f] *= 0.25;
             }
         }
-    if (threadIdx.x == 0) c->reliable_count++;
+    if (threadIdx.x == 0) {
+        c->reliable_count++;
+        c->last_reliable = c->iter;
+    }
 }
 
 // end of an iteration: continue while any RHS is active and iterations remain
