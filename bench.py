@@ -65,11 +65,15 @@ def measured_peaks():
 # ---------------------------------------------------------------------------
 
 class Dist:
+    """Replica bookkeeping: one process per GPU, no collective on the data
+    path; only the timing uses a barrier and a max over ranks."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = "cuda"
 
     def init(self, backend="nccl"):
         if self.world > 1:
@@ -78,6 +82,7 @@ class Dist:
             import torch.distributed as dist
             dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
+            self.device = "cuda" if backend == "nccl" else "cpu"
 
     def barrier(self):
         if self.pg:
@@ -87,7 +92,7 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -95,7 +100,7 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t)
         return float(t.item())
 
