@@ -52,6 +52,38 @@ double plqcd_hopping_matrix_oe_sse3_intrin(spinor *qin, spinor *qout, su3 *u);
 double plqcd_hopping_matrix_eo_sse3_intrin_blocking(spinor *qin, spinor *qout, su3 *u);
 double plqcd_hopping_matrix_oe_sse3_intrin_blocking(spinor *qin, spinor *qout, su3 *u);
 
+/*
+ * Split real/imaginary layout (reference include/dirac.h:31-32, 39-40,
+ * 55-62; note the argument order, output first). The reference packs 2/4/8
+ * x-sites per SIMD lane with its own site tables and gamma convention; here
+ * the split layout is the API arrays with real and imaginary parts in
+ * separate planes, in even/odd site order, whatever the SIMD width:
+ *   qin_re[12*i + 3*spin + colour], u_re[9*(4*i + mu) + 3*row + col]
+ * and every name computes the same operator as the AoS entry points above.
+ * The *_short names read link rows 0,1 only and rebuild row 2 as
+ * conj(row0 x row1), which is exact for SU(3) links.
+ */
+double plqcd_hopping_matrix_eo_sse3_intrin_nohalfspinor(double *qout_re, double *qout_im, double *u_re,
+                                                        double *u_im, double *qin_re, double *qin_im);
+double plqcd_hopping_matrix_oe_sse3_intrin_nohalfspinor(double *qout_re, double *qout_im, double *u_re,
+                                                        double *u_im, double *qin_re, double *qin_im);
+double plqcd_hopping_matrix_eo_avx_nohalfspinor(double *qout_re, double *qout_im, double *u_re, double *u_im,
+                                                double *qin_re, double *qin_im);
+double plqcd_hopping_matrix_oe_avx_nohalfspinor(double *qout_re, double *qout_im, double *u_re, double *u_im,
+                                                double *qin_re, double *qin_im);
+double plqcd_hopping_matrix_eo_single_mic_split(double *qout_re, double *qout_im, double *u_re, double *u_im,
+                                                double *qin_re, double *qin_im);
+double plqcd_hopping_matrix_oe_single_mic_split(double *qout_re, double *qout_im, double *u_re, double *u_im,
+                                                double *qin_re, double *qin_im);
+double plqcd_hopping_matrix_eo_single_mic_split_nohalfspinor(double *qout_re, double *qout_im, double *u_re,
+                                                             double *u_im, double *qin_re, double *qin_im);
+double plqcd_hopping_matrix_oe_single_mic_split_nohalfspinor(double *qout_re, double *qout_im, double *u_re,
+                                                             double *u_im, double *qin_re, double *qin_im);
+double plqcd_hopping_matrix_eo_single_mic_split_nohalfspinor_short(double *qout_re, double *qout_im, double *u_re,
+                                                                   double *u_im, double *qin_re, double *qin_im);
+double plqcd_hopping_matrix_oe_single_mic_split_nohalfspinor_short(double *qout_re, double *qout_im, double *u_re,
+                                                                   double *u_im, double *qin_re, double *qin_im);
+
 #ifdef __cplusplus
 }
 #endif

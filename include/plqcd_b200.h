@@ -254,6 +254,14 @@ typedef struct {
 int plqcd_invert_cg_batch(plqcd_solve_item *items, int nitems, const plqcd_cg_param *param, int use_graph,
                           plqcd_batch_info *info, double *true_residuals);
 
+/* ---- self-test ------------------------------------------------------------ */
+/* Known-answer test on `device`: with unit links, H applied to a point
+ * source is non-zero at exactly the 8 neighbours, carrying columns of
+ * (1 -/+ g_mu) (the neighbour pattern of the reference's
+ * tests/test_comms.c:167-497, here with the gamma structure); then
+ * gamma5-hermiticity on random fields. Returns PLQCD_OK or an error. */
+int plqcd_selftest(int device, int verbose);
+
 /* ---- drop-in path controls ---------------------------------------------- */
 /* Mark the host gauge field `u` as changed (or a new field) so the next
  * drop-in call uploads it. */

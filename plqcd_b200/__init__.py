@@ -72,6 +72,10 @@ _SIGS = {
     "plqcd_hopping_matrix_oe_sse3_intrin": (_d, [_vp, _vp, _vp]),
     "plqcd_hopping_matrix_eo_sse3_intrin_blocking": (_d, [_vp, _vp, _vp]),
     "plqcd_hopping_matrix_oe_sse3_intrin_blocking": (_d, [_vp, _vp, _vp]),
+    **{f"plqcd_hopping_matrix_{p}_{v}": (_d, [_vp] * 6)
+       for p in ("eo", "oe")
+       for v in ("sse3_intrin_nohalfspinor", "avx_nohalfspinor", "single_mic_split",
+                 "single_mic_split_nohalfspinor", "single_mic_split_nohalfspinor_short")},
     # include/plqcd_b200.h
     "plqcd_last_error": (ctypes.c_char_p, []),
     "plqcd_last_status": (_i, []),
@@ -112,6 +116,7 @@ _SIGS = {
     "plqcd_tune_load": (_i, [ctypes.c_char_p]),
     "plqcd_tune_count": (_i, []),
     "plqcd_tune_get": (_i, [ctypes.c_char_p, _ip, _ip, _dp]),
+    "plqcd_selftest": (_i, [_i, _i]),
     "plqcd_gauge_update": (_i, [_vp]),
     "plqcd_dropin_last_stats": (_i, [_dp, _dp, _dp]),
 }
@@ -187,6 +192,22 @@ def hopping_matrix(which: str, qin: np.ndarray, qout: np.ndarray, u: np.ndarray,
     t = f(qin.ctypes.data, qout.ctypes.data, u.ctypes.data)
     if t < 0:
         raise PlqcdError(f"hopping matrix failed: {last_error()}")
+    return t
+
+
+def hopping_matrix_split(which: str, qin: np.ndarray, qout: np.ndarray, u: np.ndarray,
+                         variant: str = "sse3_intrin_nohalfspinor") -> float:
+    """The split real/imaginary entry points on the same arrays: the complex
+    inputs are split into planes, the output planes are merged back into
+    qout (only the output parity changes)."""
+    qre, qim = np.ascontiguousarray(qin.real), np.ascontiguousarray(qin.imag)
+    ure, uim = np.ascontiguousarray(u.real), np.ascontiguousarray(u.imag)
+    ore, oim = np.ascontiguousarray(qout.real), np.ascontiguousarray(qout.imag)
+    f = getattr(lib(), f"plqcd_hopping_matrix_{which}_{variant}")
+    t = f(ore.ctypes.data, oim.ctypes.data, ure.ctypes.data, uim.ctypes.data, qre.ctypes.data, qim.ctypes.data)
+    if t < 0:
+        raise PlqcdError(f"hopping matrix failed: {last_error()}")
+    qout[:] = ore + 1j * oim
     return t
 
 

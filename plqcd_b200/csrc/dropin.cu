@@ -27,7 +27,15 @@ namespace {
 
 constexpr int kMaxChunks = 8;
 
+struct SplitCache {  // gauge field of the split entry points, by host address
+    const double *re = nullptr, *im = nullptr;
+    uint64_t fp = 0;
+};
+
 struct DropIn {
+    plqcd_gauge *gauge_split = nullptr, *gauge12 = nullptr;
+    SplitCache split18, split12;
+    bool dirty_split = true;
     int dims[4] = {0, 0, 0, 0};
     cudaStream_t s_h2d = nullptr, s_d2h = nullptr;  // copy streams
     cudaEvent_t ev_in[kMaxChunks] = {}, ev_out[kMaxChunks] = {}, ev_k0[kMaxChunks] = {}, ev_k1[kMaxChunks] = {};
@@ -48,6 +56,8 @@ DropIn g_d;
 void release_locked() {
     if (g_d.lat) cudaSetDevice(g_d.lat->device);
     if (g_d.gauge) plqcd_gauge_destroy(g_d.gauge);
+    if (g_d.gauge_split) plqcd_gauge_destroy(g_d.gauge_split);
+    if (g_d.gauge12) plqcd_gauge_destroy(g_d.gauge12);
     void *bufs[4] = {g_d.aos_in, g_d.aos_out, g_d.f_in, g_d.f_out};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -223,6 +233,128 @@ double hop_call(spinor *qin, spinor *qout, su3 *u, int out_parity) {
     return stop_watch(t0);
 }
 
+// ---- split real / imaginary planes --------------------------------------------
+// The reference's split-layout kernels (lib/dirac.c:2506, 4586, 7884, 9153)
+// pack 2/4/8 x-sites per SIMD lane with their own site tables and gamma
+// convention. This boundary keeps their names and argument order
+// (qout_re, qout_im, u_re, u_im, qin_re, qin_im) but defines the split
+// layout independently of any SIMD width: the API arrays with real and
+// imaginary parts in separate planes, in even/odd site order,
+//   qin_re[12*i + 3*spin + colour], u_re[9*(4*i + mu) + 3*row + col],
+// and computes the same operator as the AoS entry points. With `short12`
+// only link rows 0 and 1 are read and row 2 is rebuilt as
+// conj(row0 x row1) (the reference's 2x3 variant, include/su3_intrin_
+// highlevel_512.h:85-111, omits the conjugation).
+
+uint64_t fingerprint_split(const double *re, const double *im, long n) {
+    uint64_t h = 1469598103934665603ULL;
+    const uint64_t *a = reinterpret_cast<const uint64_t *>(re), *b = reinterpret_cast<const uint64_t *>(im);
+    for (int k = 0; k < 512; k++) {
+        long idx = (long)((double)k / 512 * n);
+        h = (h ^ a[idx]) * 1099511628211ULL;
+        h = (h ^ b[idx]) * 1099511628211ULL;
+    }
+    return (h ^ a[n - 1] ^ (b[n - 1] << 1)) * 1099511628211ULL;
+}
+
+int load_gauge_split(plqcd_gauge *g, const double *ure, const double *uim) {
+    const Geom &geo = g->lat->geom;
+    cudaStream_t s = g->lat->stream;
+    const long nlinks = 8 * geo.Vh, chunk = 1L << 20;
+    const long per = nlinks < chunk ? nlinks : chunk;
+    double *st = nullptr;
+    if (cudaMalloc(&st, sizeof(double) * 18 * per) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(PLQCD_ERR_NOMEM, "split gauge upload: staging allocation failed");
+    }
+    int rc = PLQCD_OK;
+    for (long first = 0; first < nlinks && rc == PLQCD_OK; first += per) {
+        const long n = nlinks - first < per ? nlinks - first : per;
+        cudaError_t e = cudaMemcpyAsync(st, ure + 9 * first, sizeof(double) * 9 * n, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(st + 9 * per, uim + 9 * first, sizeof(double) * 9 * n, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            rc = set_error(PLQCD_ERR_CUDA, "split gauge upload: %s", cudaGetErrorString(e));
+            break;
+        }
+        rc = launch_gauge_import_split(geo, s, st, st + 9 * per, first, n, g->data, g->prec, g->recon);
+        if (rc == PLQCD_OK && cudaStreamSynchronize(s) != cudaSuccess)
+            rc = set_error(PLQCD_ERR_CUDA, "split gauge upload failed");
+    }
+    cudaFree(st);
+    return rc;
+}
+
+double hop_call_split(double *qout_re, double *qout_im, double *u_re, double *u_im, double *qin_re,
+                      double *qin_im, int out_parity, bool short12) {
+    double t0 = stop_watch(0.0);
+    clear_error();
+    if (!qout_re || !qout_im || !u_re || !u_im || !qin_re || !qin_im) {
+        set_error(PLQCD_ERR_ARG, "split hopping matrix: null argument");
+        return -1.0;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (ensure_locked() != PLQCD_OK) return -1.0;
+    plqcd_lattice *lat = g_d.lat;
+    const Geom &geo = lat->geom;
+    const long Vh = geo.Vh;
+    cudaStream_t s = lat->stream;
+    if (cudaSetDevice(lat->device) != cudaSuccess) {
+        set_error(PLQCD_ERR_CUDA, "split hopping matrix: cudaSetDevice failed");
+        return -1.0;
+    }
+    g_d.h2d = g_d.d2h = 0;
+    plqcd_gauge *&gf = short12 ? g_d.gauge12 : g_d.gauge_split;
+    if (!gf && plqcd_gauge_create(lat, PLQCD_F64, short12 ? 12 : 18, &gf) != PLQCD_OK) return -1.0;
+    const uint64_t fp = fingerprint_split(u_re, u_im, 8 * Vh * 9);
+    SplitCache &sc = short12 ? g_d.split12 : g_d.split18;
+    if (!env_flag("PLQCD_GAUGE_CACHE", true) || g_d.dirty_split || sc.re != u_re || sc.im != u_im || sc.fp != fp) {
+        if (load_gauge_split(gf, u_re, u_im) != PLQCD_OK) return -1.0;
+        sc.re = u_re;
+        sc.im = u_im;
+        sc.fp = fp;
+        g_d.h2d += 2.0 * sizeof(double) * 9 * 8 * Vh;
+    }
+    g_d.dirty_split = false;
+    const int in_parity = out_parity ^ 1;
+    const size_t half = sizeof(double) * 12 * Vh;
+    double *dre = static_cast<double *>(g_d.aos_in), *dim = dre + 12 * Vh;
+    double *ore = static_cast<double *>(g_d.aos_out), *oim = ore + 12 * Vh;
+    cudaError_t e = cudaMemcpyAsync(dre, qin_re + 12 * in_parity * Vh, half, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dim, qin_im + 12 * in_parity * Vh, half, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        set_error(PLQCD_ERR_CUDA, "split hopping matrix: H2D: %s", cudaGetErrorString(e));
+        return -1.0;
+    }
+    if (launch_spinor_import_split(geo, s, dre, dim, g_d.f_in, PLQCD_F64) != PLQCD_OK) return -1.0;
+    DslashCall dc;
+    dc.gauge = gf->data;
+    dc.prec = PLQCD_F64;
+    dc.recon = gf->recon;
+    dc.out = g_d.f_out;
+    dc.in = g_d.f_in;
+    dc.out_parity = out_parity;
+    dc.flags = (env_flag("PLQCD_REF_COMPAT", false) && !short12) ? PLQCD_DSLASH_COMPAT : 0u;
+    cudaEventRecord(g_d.ev_k0[0], s);
+    if (launch_dslash(geo, s, dc) != PLQCD_OK) return -1.0;
+    cudaEventRecord(g_d.ev_k1[0], s);
+    if (launch_spinor_export_split(geo, s, g_d.f_out, PLQCD_F64, ore, oim) != PLQCD_OK) return -1.0;
+    e = cudaMemcpyAsync(qout_re + 12 * out_parity * Vh, ore, half, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(qout_im + 12 * out_parity * Vh, oim, half, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error(PLQCD_ERR_CUDA, "split hopping matrix: %s", cudaGetErrorString(e));
+        return -1.0;
+    }
+    g_d.h2d += 2.0 * half;
+    g_d.d2h += 2.0 * half;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, g_d.ev_k0[0], g_d.ev_k1[0]);
+    g_d.kernel_ms = ms;
+    lat->last_kernel_ms = ms;
+    return stop_watch(t0);
+}
+
 }  // namespace
 
 namespace plqcd {
@@ -236,8 +368,27 @@ extern "C" int plqcd_gauge_update(const su3 *u) {
     std::lock_guard<std::mutex> lk(g_mu);
     (void)u;
     g_d.dirty = true;
+    g_d.dirty_split = true;
     return PLQCD_OK;
 }
+
+// split-layout names: include/dirac.h:31-32 (SSE3), 39-40 (AVX), 55-62 (MIC)
+#define PLQCD_SPLIT_ENTRY(name, parity, short12)                                                               \
+    extern "C" double name(double *qout_re, double *qout_im, double *u_re, double *u_im, double *qin_re,       \
+                           double *qin_im) {                                                                   \
+        return hop_call_split(qout_re, qout_im, u_re, u_im, qin_re, qin_im, parity, short12);                  \
+    }
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_eo_sse3_intrin_nohalfspinor, 0, false)
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_oe_sse3_intrin_nohalfspinor, 1, false)
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_eo_avx_nohalfspinor, 0, false)
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_oe_avx_nohalfspinor, 1, false)
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_eo_single_mic_split, 0, false)
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_oe_single_mic_split, 1, false)
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_eo_single_mic_split_nohalfspinor, 0, false)
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_oe_single_mic_split_nohalfspinor, 1, false)
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_eo_single_mic_split_nohalfspinor_short, 0, true)
+PLQCD_SPLIT_ENTRY(plqcd_hopping_matrix_oe_single_mic_split_nohalfspinor_short, 1, true)
+#undef PLQCD_SPLIT_ENTRY
 
 extern "C" int plqcd_dropin_last_stats(double *kernel_ms, double *h2d, double *d2h) {
     std::lock_guard<std::mutex> lk(g_mu);

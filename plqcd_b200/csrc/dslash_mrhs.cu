@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "dslash_core.cuh"
@@ -110,6 +111,127 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs(const MrhsArgs a) {
     }
 }
 
+// Pipelined RHS-tile kernel: per direction the link and the NR neighbour
+// spinors are copied global->shared with cp.async into slots private to the
+// thread, ST directions ahead of the one being computed (no block-level
+// synchronisation). The link crosses L2->SM once per tile and the copies
+// stay in flight without holding registers.
+template <class SIO, class LIO, int NR, int ST, bool XPAY>
+__global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
+    using R = typename SIO::real;
+    extern __shared__ uint4 smem[];
+    constexpr int NS = LIO::NSLOT + NR * SIO::NSLOT;
+    const int B = blockDim.x;
+    const int tile = blockIdx.x % a.ntiles;
+    const long h = (long)(blockIdx.x / a.ntiles) * B + threadIdx.x;
+    if (h >= a.Vh) return;  // no block-level barrier below
+    const int r0 = tile * NR;
+    const int nr = min(NR, a.nrhs - r0);
+    const int par = a.out_parity, opp = par ^ 1;
+    const long Vh = a.Vh;
+    const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
+    const Coords c = site_coords(h, par, L0h, L1, L2);
+    const int xh = (int)(h - c.row * L0h);
+    const long L01 = L1, L012 = (long)L1 * L2;
+    const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
+    const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
+    long nb[8];
+    nb[0] = (xp >> 1) + L0h * c.row;
+    nb[1] = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
+    nb[2] = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
+    nb[3] = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
+    nb[4] = (xm >> 1) + L0h * c.row;
+    nb[5] = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
+    nb[6] = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
+    nb[7] = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
+    const R sg = (R)a.g5_in;
+
+    const int stride = B * 16;
+    const uint32_t s_thread = smem_addr(smem) + threadIdx.x * 16;
+    auto issue = [&](int d) {
+        const uint32_t s0 = s_thread + (uint32_t)((d % ST) * NS) * stride;
+        if (d < 4)
+            LIO::issue(a.gauge, Vh, par, d, h, s0, stride);
+        else
+            LIO::issue(a.gauge, Vh, opp, d - 4, nb[d], s0, stride);
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+            if (r < nr)
+                SIO::issue(a.in + (size_t)(r0 + r) * a.fbytes, Vh, nb[d],
+                           s0 + (uint32_t)(LIO::NSLOT + r * SIO::NSLOT) * stride, stride);
+    };
+#pragma unroll
+    for (int d = 0; d < ST; d++) {
+        issue(d);
+        cp_async_commit();
+    }
+    cx<R> acc[NR][12];
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int k = 0; k < 12; k++) acc[r][k] = {R(0), R(0)};
+#pragma unroll
+    for (int d = 0; d < 8; d++) {
+        cp_async_wait<ST - 1>();
+        const uint4 *s0 = smem + threadIdx.x + (d % ST) * NS * B;
+        cx<R> U[9];
+        LIO::load_staged(s0, B, U);
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+            if (r < nr) {
+                cx<R> s[12];
+                R n;
+                SIO::load_staged_raw(s0 + (LIO::NSLOT + r * SIO::NSLOT) * B, B, s, n);
+                compute_dir_n<false, SIO::kScaled, R>(d, acc[r], s, U, sg, n);
+            }
+        }
+        // the slot just consumed is refilled only after its values were used
+        if (d + ST < 8) issue(d + ST);
+        cp_async_commit();
+    }
+
+    const R aup = (R)a.a_up, alow = (R)a.a_low, b = (R)a.b;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        if (r >= nr) continue;
+        if (XPAY) {
+            cx<R> xv[12];
+            SIO::load(a.x + (size_t)(r0 + r) * a.fbytes, Vh, h, xv);
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const R ak = k < 6 ? aup : alow;
+                acc[r][k] = {fma(ak, acc[r][k].re, b * xv[k].re), fma(ak, acc[r][k].im, b * xv[k].im)};
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const R ak = k < 6 ? aup : alow;
+                acc[r][k] = {ak * acc[r][k].re, ak * acc[r][k].im};
+            }
+        }
+        SIO::store(a.out + (size_t)(r0 + r) * a.fbytes, Vh, h, acc[r]);
+    }
+}
+
+template <class SIO, class LIO, int NR, int ST>
+static int launch_nr_pipe(const Geom &g, cudaStream_t s, MrhsArgs a, int block, bool xpay) {
+    a.ntiles = (a.nrhs + NR - 1) / NR;
+    const long nblk = (g.Vh + block - 1) / block * a.ntiles;
+    if (nblk > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: grid too large");
+    constexpr int NS = LIO::NSLOT + NR * SIO::NSLOT;
+    const size_t smem = (size_t)ST * NS * 16 * block;
+    if (smem > 227 * 1024) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: %zu bytes of shared memory", smem);
+    auto k = xpay ? k_dslash_mrhs_pipe<SIO, LIO, NR, ST, true> : k_dslash_mrhs_pipe<SIO, LIO, NR, ST, false>;
+    static bool attr_set[2] = {false, false};  // per instantiation and epilogue
+    if (!attr_set[xpay]) {
+        PLQCD_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        attr_set[xpay] = true;
+    }
+    k<<<(unsigned)nblk, block, smem, s>>>(a);
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
 template <class SIO, class LIO, int NR>
 static int launch_nr(const Geom &g, cudaStream_t s, MrhsArgs a, int block, bool xpay) {
     a.ntiles = (a.nrhs + NR - 1) / NR;
@@ -129,6 +251,11 @@ static int launch_pr(const Geom &g, cudaStream_t s, const MrhsArgs &a, int nr, i
     using S = SpinorIO<P>;
     using L = LinkIO<P, RC>;
     switch (nr) {
+        // 1000 + 10 * tile + depth: pipelined RHS-tile kernel
+        case 1022: return launch_nr_pipe<S, L, 2, 2>(g, s, a, block, xpay);
+        case 1042:
+            if constexpr (P != PLQCD_F64) return launch_nr_pipe<S, L, 4, 2>(g, s, a, block, xpay);
+            break;
         case 1: return launch_nr<S, L, 1>(g, s, a, block, xpay);
         case 2: return launch_nr<S, L, 2>(g, s, a, block, xpay);
         case 4:
@@ -195,9 +322,10 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
             t.block = blk;
             cands.push_back(t);
         }
-    for (int nr : {2, 1, 4}) {
-        if (nr == 4 && prec == PLQCD_F64) continue;
-        if (nr > nrhs && nr != 1) continue;
+    for (int nr : {1022, 1042, 2, 1, 4}) {
+        const int tile = nr >= 1000 ? (nr / 10) % 10 : nr;
+        if (tile == 4 && prec == PLQCD_F64) continue;
+        if (tile > nrhs && tile != 1) continue;
         for (int blk : {64, 128, 256}) {
             TuneResult t;
             t.variant = nr;
@@ -218,6 +346,18 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
     dc.b = b;
     dc.nrhs = nrhs;
     void *scratch = nullptr;
+    // explicit configuration for experiments and tests: bypasses the tuner
+    if (const char *ev = getenv("PLQCD_MRHS_VARIANT")) {
+        const char *eb = getenv("PLQCD_MRHS_BLOCK");
+        TuneResult t;
+        t.variant = atoi(ev);
+        t.block = eb ? atoi(eb) : 128;
+        if (t.variant >= 100 && t.variant < 1000) {
+            DslashCall c2 = dc;
+            return launch_dslash_config(g, s, c2, t.variant - 100, t.block);
+        }
+        return mrhs_dispatch(g, s, prec, recon, m, t.variant, t.block, xpay);
+    }
     auto launch = [&](const TuneResult &t, char *dst) -> int {
         if (t.variant >= 100) {
             DslashCall c2 = dc;

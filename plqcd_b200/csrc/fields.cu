@@ -57,6 +57,33 @@ __global__ void k_spinor_export(const void *src, long Vh, int parity, double2 *_
     for (int k = 0; k < 12; k++) p[k] = make_double2((double)r[k].re, (double)r[k].im);
 }
 
+// split real / imaginary planes: component k of staged site h at re[12*h+k]
+template <int PREC>
+__global__ void k_spinor_import_split(const double *__restrict__ re, const double *__restrict__ im, long Vh,
+                                      void *dst) {
+    long h = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= Vh) return;
+    using R = typename SpinorIO<PREC>::real;
+    cx<R> r[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) r[k] = {(R)re[12 * h + k], (R)im[12 * h + k]};
+    SpinorIO<PREC>::store(dst, Vh, h, r);
+}
+
+template <int PREC>
+__global__ void k_spinor_export_split(const void *src, long Vh, double *__restrict__ re, double *__restrict__ im) {
+    long h = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= Vh) return;
+    using R = typename SpinorIO<PREC>::real;
+    cx<R> r[12];
+    SpinorIO<PREC>::load(src, Vh, h, r);
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        re[12 * h + k] = (double)r[k].re;
+        im[12 * h + k] = (double)r[k].im;
+    }
+}
+
 template <int DP, int SP>
 __global__ void k_spinor_convert(void *dst, const void *src, long Vh) {
     long h = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -105,6 +132,23 @@ __global__ void k_gauge_import(const double2 *__restrict__ aos, long first, long
         double2 v = p[e];
         U[e] = {v.x, v.y};
     }
+    LinkIO<PREC, RECON>::store(dst, Vh, par, mu, h, U);
+}
+
+// links from split planes: element e of staged link k at re[9*k+e]
+template <int PREC, int RECON>
+__global__ void k_gauge_import_split(const double *__restrict__ re, const double *__restrict__ im, long first,
+                                     long n, long Vh, void *dst) {
+    long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    long l = first + k;
+    long i = l >> 2;
+    int mu = (int)(l & 3);
+    int par = i >= Vh;
+    long h = i - par * Vh;
+    cx<double> U[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) U[e] = {re[9 * k + e], im[9 * k + e]};
     LinkIO<PREC, RECON>::store(dst, Vh, par, mu, h, U);
 }
 
@@ -231,6 +275,32 @@ int launch_spinor_export(const Geom &g, cudaStream_t s, const void *src, int pre
     if (count < 0) count = g.Vh - first;
 #define F(P) dev::k_spinor_export<P><<<dev::nblocks(count), dev::kBlock, 0, s>>>(src, g.Vh, parity, (double2 *)aos, first, count)
     PLQCD_SPINOR_SWITCH(prec, F)
+#undef F
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int launch_spinor_import_split(const Geom &g, cudaStream_t s, const double *re, const double *im, void *dst,
+                               int prec) {
+#define F(P) dev::k_spinor_import_split<P><<<dev::nblocks(g.Vh), dev::kBlock, 0, s>>>(re, im, g.Vh, dst)
+    PLQCD_SPINOR_SWITCH(prec, F)
+#undef F
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int launch_spinor_export_split(const Geom &g, cudaStream_t s, const void *src, int prec, double *re, double *im) {
+#define F(P) dev::k_spinor_export_split<P><<<dev::nblocks(g.Vh), dev::kBlock, 0, s>>>(src, g.Vh, re, im)
+    PLQCD_SPINOR_SWITCH(prec, F)
+#undef F
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int launch_gauge_import_split(const Geom &g, cudaStream_t s, const double *re, const double *im, long first, long n,
+                              void *dst, int prec, int recon) {
+#define F(P, R) dev::k_gauge_import_split<P, R><<<dev::nblocks(n), dev::kBlock, 0, s>>>(re, im, first, n, g.Vh, dst)
+    PLQCD_GAUGE_SWITCH(prec, recon, F)
 #undef F
     PLQCD_CUDA_TRY(cudaGetLastError());
     return PLQCD_OK;

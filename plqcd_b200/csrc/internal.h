@@ -81,6 +81,13 @@ int launch_spinor_import(const Geom &g, cudaStream_t s, const void *aos, int par
 int launch_spinor_export(const Geom &g, cudaStream_t s, const void *src, int prec, int parity, void *aos,
                          long first = 0, long count = -1);
 int launch_spinor_convert(const Geom &g, cudaStream_t s, void *dst, int dprec, const void *src, int sprec);
+// split real / imaginary planes of one parity (12 doubles per site each)
+int launch_spinor_import_split(const Geom &g, cudaStream_t s, const double *re, const double *im, void *dst,
+                               int prec);
+int launch_spinor_export_split(const Geom &g, cudaStream_t s, const void *src, int prec, double *re, double *im);
+// links [first, first + n) from split planes (9 doubles per link each)
+int launch_gauge_import_split(const Geom &g, cudaStream_t s, const double *re, const double *im, long first, long n,
+                              void *dst, int prec, int recon);
 int launch_spinor_gaussian(const Geom &g, cudaStream_t s, void *dst, int prec, int parity, uint64_t seed);
 int launch_gauge_import(const Geom &g, cudaStream_t s, const void *aos, long first_link, long nlinks,
                         void *dst, int prec, int recon);

@@ -357,3 +357,69 @@ def test_multi_rhs_equals_single_rhs(cuda, prec, recon, tol, nrhs):
             a = field_to_host(lat, blk_out[sl], prec, 0)[: lat.V // 2]
             b = field_to_host(lat, one, prec, 0)[: lat.V // 2]
             assert relmax(a, b) <= tol, (r, xpay, relmax(a, b))
+
+
+@pytest.mark.parametrize("variant,block", [(1, 128), (2, 64), (4, 128), (100, 128), (102, 64), (103, 64),
+                                           (1022, 64), (1042, 128)])
+@pytest.mark.parametrize("prec,recon,tol", [(P.F64, 18, 1e-14), (P.F32, 12, 1e-6), (P.F16, 12, 1e-3)])
+def test_multi_rhs_every_variant(cuda, monkeypatch, variant, block, prec, recon, tol):
+    """Each launch variant of the multi-RHS kernel (RHS tile 1/2/4, RHS folded
+    into the single-RHS kernels' grid, pipelined RHS tiles), forced past the
+    tuner, agrees with the single-RHS kernel for every field of the block."""
+    if prec == P.F64 and variant in (4, 1042):
+        pytest.skip("no four-RHS FP64 tile (register file)")
+    L = (8, 4, 6, 8)
+    nrhs = 5
+    lat, g64, u = _device_setup(L, 21)
+    g = g64 if (prec, recon) == (P.F64, 18) else P.Gauge(lat, prec, recon)
+    if g is not g64:
+        g.copy_from(g64)
+    bs = lat.spinor_bytes(prec)
+    blk_in, blk_out, blk_x = dev_bytes(nrhs * bs), dev_bytes(nrhs * bs), dev_bytes(nrhs * bs)
+    for r in range(nrhs):
+        lat.spinor_gaussian(blk_in[r * bs:(r + 1) * bs], prec, 0, 300 + r)
+        lat.spinor_gaussian(blk_x[r * bs:(r + 1) * bs], prec, 1, 400 + r)
+    monkeypatch.setenv("PLQCD_MRHS_VARIANT", str(variant))
+    monkeypatch.setenv("PLQCD_MRHS_BLOCK", str(block))
+    flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
+    lat.dslash_mrhs_xpay(g, blk_out, blk_in, nrhs, 1, prec, 0.37, blk_x, -1.5, flags)
+    monkeypatch.delenv("PLQCD_MRHS_VARIANT")
+    for r in range(nrhs):
+        sl = slice(r * bs, (r + 1) * bs)
+        one = dev_bytes(bs)
+        lat.dslash_xpay(g, one, blk_in[sl], 1, prec, 0.37, blk_x[sl], -1.5, flags)
+        a = field_to_host(lat, blk_out[sl], prec, 1)[lat.V // 2:]
+        b = field_to_host(lat, one, prec, 1)[lat.V // 2:]
+        assert relmax(a, b) <= tol, (variant, r, relmax(a, b))
+
+
+@pytest.mark.parametrize("variant", ["sse3_intrin_nohalfspinor", "avx_nohalfspinor", "single_mic_split",
+                                     "single_mic_split_nohalfspinor", "single_mic_split_nohalfspinor_short"])
+def test_split_layout_entry_points(dropin, restatement, variant):
+    """Split real/imaginary names (reference include/dirac.h:31-32, 39-40,
+    55-62) compute the same operator as the AoS ones; the *_short names
+    read link rows 0,1 only (exact for SU(3) links)."""
+    L = (4, 6, 8, 10)
+    dropin(L)
+    V = O.volume(L)
+    rng = np.random.default_rng(31)
+    q, u = O.gaussian_spinor(V, rng), O.random_su3(4 * V, rng)
+    want = restatement.hop("full", L, q, u)
+    got = np.zeros_like(q)
+    P.hopping_matrix_split("eo", q, got, u, variant)
+    P.hopping_matrix_split("oe", q, got, u, variant)
+    tol = 1e-13 if variant.endswith("short") else TOL64
+    assert relmax(got, want) < tol
+    if variant.endswith("short"):
+        # row 2 really is rebuilt: garbage in row 2 of the input changes nothing
+        u2 = u.copy()
+        u2[:, 6:] = 123.0
+        P.lib().plqcd_gauge_update(None)
+        got2 = np.zeros_like(q)
+        P.hopping_matrix_split("eo", q, got2, u2, variant)
+        P.hopping_matrix_split("oe", q, got2, u2, variant)
+        assert relmax(got2, want) < tol
+
+
+def test_shipped_selftest(cuda):
+    assert P.lib().plqcd_selftest(0, 1) == 0, P.last_error()
