@@ -25,7 +25,7 @@ using namespace plqcd;
 
 namespace {
 
-constexpr int kMaxChunks = 8;
+constexpr int kMaxChunks = 16;
 
 struct SplitCache {  // gauge field of the split entry points, by host address
     const double *re = nullptr, *im = nullptr;

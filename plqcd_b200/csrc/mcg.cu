@@ -426,11 +426,21 @@ struct Batch {
                 dev::k_maccum_zero<PLQCD_F32><<<grid, kBlasBlock, 0, s>>>((char *)it.in.x_even, it.fb64, it.xs,
                                                                          it.fbx, it.g->Vh);
             PLQCD_CUDA_TRY(cudaGetLastError());
+            // FP64: solution and Schur residual b' - Mhat x (convergence)
             PLQCD_TRY(mhat(it, it.in.g64, it.t64, it.in.x_even, it.tmp64, false));
             PLQCD_TRY(sub_norm2(it, it.r64, it.bprime, it.t64, M_SR2));
-            PLQCD_TRY(mhat(it, it.in.g64, it.t64, it.r64, it.tmp64, true));
-            PLQCD_TRY(norm2(it, it.t64, PLQCD_F64, M_RR_TRUE, false));
-            PLQCD_TRY(convert(it, it.rs, it.ps, it.t64, PLQCD_F64));
+            // restart direction Mhat^dag r: the sloppy operator's accuracy
+            // suffices (FP64 when the solve is FP64)
+            if (mixed) {
+                const plqcd_gauge *gs = it.in.g_sloppy ? it.in.g_sloppy : it.in.g64;
+                PLQCD_TRY(convert(it, it.t, it.ps, it.r64, PLQCD_F64));
+                PLQCD_TRY(mhat(it, gs, it.rs, it.t, it.tmps, true));
+                PLQCD_TRY(norm2(it, it.rs, it.ps, M_RR_TRUE, false));
+            } else {
+                PLQCD_TRY(mhat(it, it.in.g64, it.t64, it.r64, it.tmp64, true));
+                PLQCD_TRY(norm2(it, it.t64, PLQCD_F64, M_RR_TRUE, false));
+                PLQCD_TRY(convert(it, it.rs, it.ps, it.t64, PLQCD_F64));
+            }
         }
         return PLQCD_OK;
     }
