@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdlib>
+#include <type_traits>
 
 #include "dslash_core.cuh"
 #include "internal.h"
@@ -243,14 +244,111 @@ static int launch_pipe(const Geom &g, cudaStream_t s, const DslashArgs &a, int b
     return PLQCD_OK;
 }
 
+// Two sites per thread (sites h and h + blockDim of a 2*blockDim tile),
+// direct loads, the direction loops of both sites interleaved: twice the
+// independent loads in flight per thread and shared index arithmetic, for
+// the 32- and 16-bit formats whose kernels are latency / issue bound.
+// Single parity only (RHS blocks allowed), no bug-compatible mode.
+template <class SIO, class LIO, bool XPAY>
+__global__ void __launch_bounds__(256) k_dslash_spt2(const DslashArgs a) {
+    using R = typename SIO::real;
+    constexpr int S = 2;
+    const int par = a.out_parity, opp = par ^ 1;
+    const long tile = blockIdx.x / a.nrhs;
+    const long roff = (long)(blockIdx.x % a.nrhs) * a.fbytes;
+    const void *in = static_cast<const char *>(a.in[0]) + roff;
+    void *out = static_cast<char *>(a.out[0]) + roff;
+    const long Vh = a.Vh;
+    const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
+    const long L01 = L1, L012 = (long)L1 * L2;
+    long hs[S], nb[S][8];
+    bool ok[S];
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        long h = a.h_begin + tile * (S * blockDim.x) + j * blockDim.x + threadIdx.x;
+        ok[j] = h < a.h_end;
+        if (!ok[j]) h = a.h_begin;  // compute on a valid site, store nothing
+        hs[j] = h;
+        const Coords c = site_coords(h, par, L0h, L1, L2);
+        const int xh = (int)(h - c.row * L0h);
+        const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
+        const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
+        nb[j][0] = (xp >> 1) + L0h * c.row;
+        nb[j][1] = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
+        nb[j][2] = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
+        nb[j][3] = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
+        nb[j][4] = (xm >> 1) + L0h * c.row;
+        nb[j][5] = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
+        nb[j][6] = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
+        nb[j][7] = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
+    }
+    if (!ok[0]) return;
+    const R sg = (R)a.g5_in;
+    cx<R> acc[S][12];
+#pragma unroll
+    for (int j = 0; j < S; j++)
+#pragma unroll
+        for (int k = 0; k < 12; k++) acc[j][k] = {R(0), R(0)};
+#pragma unroll
+    for (int d = 0; d < 8; d++) {
+        cx<R> s[S][12], U[S][9];
+        R n[S];
+#pragma unroll
+        for (int j = 0; j < S; j++) {
+            SIO::load_raw(in, Vh, nb[j][d], s[j], n[j]);
+            if (d < 4)
+                LIO::load(a.gauge, Vh, par, d, hs[j], U[j]);
+            else
+                LIO::load(a.gauge, Vh, opp, d - 4, nb[j][d], U[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < S; j++) compute_dir_n<false, SIO::kScaled, R>(d, acc[j], s[j], U[j], sg, n[j]);
+    }
+    const R aup = (R)a.a_up, alow = (R)a.a_low;
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        if (!ok[j]) continue;
+        if (XPAY) {
+            cx<R> xv[12];
+            SIO::load(static_cast<const char *>(a.x) + roff, Vh, hs[j], xv);
+            const R b = (R)a.b;
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const R ak = k < 6 ? aup : alow;
+                acc[j][k] = {fma(ak, acc[j][k].re, b * xv[k].re), fma(ak, acc[j][k].im, b * xv[k].im)};
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const R ak = k < 6 ? aup : alow;
+                acc[j][k] = {ak * acc[j][k].re, ak * acc[j][k].im};
+            }
+        }
+        SIO::store(out, Vh, hs[j], acc[j]);
+    }
+}
+
 template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
 static int launch_direct(const Geom &g, cudaStream_t s, const DslashArgs &a, int block);
+
+template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
+static int launch_spt2(const Geom &g, cudaStream_t s, const DslashArgs &a, int block) {
+    if constexpr (COMPAT || FULL || std::is_same<typename SIO::real, double>::value) {
+        return set_error(PLQCD_ERR_ARG, "dslash: two sites per thread exists for 32/16-bit single-parity calls");
+    } else {
+        const long nblk = (a.h_end - a.h_begin + 2L * block - 1) / (2L * block) * a.nrhs;
+        k_dslash_spt2<SIO, LIO, XPAY><<<(unsigned)nblk, block, 0, s>>>(a);
+        PLQCD_CUDA_TRY(cudaGetLastError());
+        return PLQCD_OK;
+    }
+}
 
 // variant 0: direct loads; 2, 3: cp.async pipeline of that depth
 template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
 static int launch_t(const Geom &g, cudaStream_t s, const DslashArgs &a, int variant, int block) {
     if (variant == 2) return launch_pipe<SIO, LIO, 2, COMPAT, XPAY, FULL>(g, s, a, block);
     if (variant == 3) return launch_pipe<SIO, LIO, 3, COMPAT, XPAY, FULL>(g, s, a, block);
+    if (variant == 12) return launch_spt2<SIO, LIO, COMPAT, XPAY, FULL>(g, s, a, block);
     return launch_direct<SIO, LIO, COMPAT, XPAY, FULL>(g, s, a, block);
 }
 
@@ -355,14 +453,19 @@ static int build_args(const Geom &g, const DslashCall &c, dev::DslashArgs &a) {
 
 static int tune_dslash(const Geom &g, cudaStream_t s, const DslashCall &c, const dev::DslashArgs &a,
                        const char *key) {
+    // load strategy (0 direct, 2/3 cp.async pipeline depth, 12 two sites per
+    // thread) x block size
     std::vector<TuneResult> cands;
-    for (int v : {2, 0, 3})
+    const bool spt_ok = c.prec != PLQCD_F64 && !c.full && !(c.flags & PLQCD_DSLASH_COMPAT);
+    for (int v : {2, 0, 3, 12}) {
+        if (v == 12 && !spt_ok) continue;
         for (int b : {64, 128, 256}) {
             TuneResult r;
             r.variant = v;
             r.block = b;
             cands.push_back(r);
         }
+    }
     // trial launches write into scratch outputs: an xpay whose output aliases
     // its x operand must not be applied more than once
     void *scratch[2] = {nullptr, nullptr};

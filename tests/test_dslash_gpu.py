@@ -423,3 +423,36 @@ def test_split_layout_entry_points(dropin, restatement, variant):
 
 def test_shipped_selftest(cuda):
     assert P.lib().plqcd_selftest(0, 1) == 0, P.last_error()
+
+
+@pytest.mark.parametrize("variant,block", [(0, 64), (2, 64), (2, 128), (3, 64), (12, 64), (12, 128)])
+@pytest.mark.parametrize("prec,recon,tol", [(P.F64, 18, 1e-14), (P.F32, 12, 1e-6), (P.F16, 12, 1e-3),
+                                            (P.BF16, 12, 1e-2)])
+def test_dslash_every_load_strategy(cuda, monkeypatch, variant, block, prec, recon, tol):
+    """Each load strategy of the single-RHS kernel, forced past the tuner
+    (direct, cp.async pipeline depth 2/3, two sites per thread), matches the
+    FP64 oracle-checked kernel within the precision's tolerance, with the
+    xpay and gamma5 epilogue and on a lattice whose half volume is not a
+    multiple of the block."""
+    if variant == 12 and prec == P.F64:
+        pytest.skip("two sites per thread is built for 32/16-bit formats")
+    L = (6, 4, 6, 10)
+    lat, g64, u = _device_setup(L, 41)
+    g = g64 if (prec, recon) == (P.F64, 18) else P.Gauge(lat, prec, recon)
+    if g is not g64:
+        g.copy_from(g64)
+    bs = lat.spinor_bytes(prec)
+    a, x, o = dev_bytes(bs), dev_bytes(bs), dev_bytes(bs)
+    lat.spinor_gaussian(a, prec, 0, 5)
+    lat.spinor_gaussian(x, prec, 1, 6)
+    flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
+    monkeypatch.setenv("PLQCD_DSLASH_STAGES", "0")
+    monkeypatch.setenv("PLQCD_DSLASH_BLOCK", "128")
+    ref = dev_bytes(bs)
+    lat.dslash_xpay(g, ref, a, 1, prec, 0.25, x, -2.0, flags)
+    monkeypatch.setenv("PLQCD_DSLASH_STAGES", str(variant))
+    monkeypatch.setenv("PLQCD_DSLASH_BLOCK", str(block))
+    lat.dslash_xpay(g, o, a, 1, prec, 0.25, x, -2.0, flags)
+    want = field_to_host(lat, ref, prec, 1)[lat.V // 2:]
+    got = field_to_host(lat, o, prec, 1)[lat.V // 2:]
+    assert relmax(got, want) <= tol
