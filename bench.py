@@ -282,8 +282,14 @@ def run_ours(args, d: Dist):
     lat.spinor_gaussian(fe, P.F64, 0, 77 + d.rank)
     lat.spinor_gaussian(fo, P.F64, 1, 77 + d.rank)
 
-    # ---- headline: full lattice H, FP64, device resident ------------------
     K, W = args.steps, args.warmup
+    if args.only == "cg":  # profiling runs of the solver section alone
+        cg = run_cg(torch, P, lat, g64, buf, args)
+        if d.rank == 0:
+            print(json.dumps({"only": "cg", "cg": cg}))
+        return 0
+
+    # ---- headline: full lattice H, FP64, device resident ------------------
     full = lambda: lat.dslash_full(g64, oe_, oo_, fe, fo, P.F64)
     clk = ClockSampler(d.local)
     clk.start()
@@ -644,8 +650,8 @@ def main():
     ap.add_argument("--delta", type=float, default=0.01, help="reliable-update threshold of the mixed solvers")
     ap.add_argument("--lattice", default=",".join(map(str, L_BENCH)),
                     help="L0,L1,L2,L3 of the hopping-matrix workload (default 32,32,32,64)")
-    ap.add_argument("--only", choices=["all", "dslash"], default="all",
-                    help="dslash: only the hopping kernels (profiling runs)")
+    ap.add_argument("--only", choices=["all", "dslash", "cg"], default="all",
+                    help="dslash / cg: only that section (profiling runs)")
     args = ap.parse_args()
     args.lattice = tuple(int(x) for x in args.lattice.split(","))
     d = Dist()
