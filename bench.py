@@ -49,6 +49,18 @@ BYTES_HALF_12 = 52 + 8 * 24 + 52
 # capture on 24^3x48 (profiles/dslash_f64_full_and_eo_24x24x24x48.txt); traffic
 # grows with the sites processed, so a launch moves this times V bytes.
 DRAM_BYTES_PER_SITE_FULL_F64 = 634.8e6 / (24 * 24 * 24 * 48)
+# the same for the TMA-staged kernel, from one capture per configuration on
+# 32^3x24 (profiles/dslash_tma_f64_full_32x32x32x24.txt): variant -> bytes/site
+DRAM_BYTES_PER_SITE_TMA_F64 = {1204: 865.05e6 / (32 * 32 * 32 * 24), 1408: 808.10e6 / (32 * 32 * 32 * 24)}
+
+
+def dram_bytes_per_site(cfg) -> float:
+    """ncu DRAM bytes per site of the full-lattice F64 kernel `cfg` runs
+    (TMA configurations without their own capture use the nearest one)."""
+    if cfg is not None and cfg[0] >= 1000:
+        v = cfg[0]
+        return DRAM_BYTES_PER_SITE_TMA_F64.get(v, DRAM_BYTES_PER_SITE_TMA_F64[1204 if v % 100 <= 4 else 1408])
+    return DRAM_BYTES_PER_SITE_FULL_F64
 
 
 def measured_peaks():
@@ -245,6 +257,36 @@ def run_reference(args, d: Dist):
 # our arm
 # ---------------------------------------------------------------------------
 
+def tuned_config(P, pattern: str):
+    """(variant, block) the autotuner chose for the first cache key that
+    contains `pattern`, or None."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "tune.json")
+        if P.lib().plqcd_tune_save(path.encode()) != 0 or not os.path.exists(path):
+            return None
+        for line in open(path):
+            try:
+                e = json.loads(line)
+            except ValueError:
+                continue
+            if pattern in e.get("key", ""):
+                return e["variant"], e["block"]
+    return None
+
+
+def kernel_name(cfg) -> str:
+    """Name of the hopping kernel a (variant, block) configuration runs."""
+    if cfg is None:
+        return "k_dslash_pipe<F64,18,full>"
+    v, b = cfg
+    if v >= 1000:
+        return f"k_dslash_tma<F64,18> ({(v // 100) % 10} stages, {v % 100} rows per tile, full lattice)"
+    if v in (2, 3):
+        return f"k_dslash_pipe<F64,18,full> (depth {v}, block {b})"
+    return f"k_dslash<F64,18,full> (block {b})"
+
+
 def time_kernel(torch, fn, steps: int, warmup: int, d: Dist | None = None):
     for _ in range(warmup):
         fn()
@@ -297,6 +339,9 @@ def run_ours(args, d: Dist):
     clocks = clk.stop()
     ms_max = d.max(ms)
     t_step = ms_max / 1e3 / K
+    head_cfg = tuned_config(P, f"dslash|p{P.F64}|r18|full|{'x'.join(map(str, L))}|")
+    if os.environ.get("PLQCD_DSLASH_FULL_STAGES"):  # forced (profiling runs)
+        head_cfg = (int(os.environ["PLQCD_DSLASH_FULL_STAGES"]), 0)
     value = d.world * V * FLOP_PER_SITE / t_step / 1e9
     achieved = V * BYTES_FULL[0] / t_step / 1e9
 
@@ -373,9 +418,10 @@ def run_ours(args, d: Dist):
                    "parallelism": f"replicas x{d.world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
-                     "bytes_per_site": BYTES_FULL[0], "kernel": "k_dslash_pipe<F64,18,full>",
-                     "traffic": round(DRAM_BYTES_PER_SITE_FULL_F64 * V),
-                     "traffic_note": "ncu dram bytes of a 24^3x48 launch scaled by sites"},
+                     "bytes_per_site": BYTES_FULL[0], "kernel": kernel_name(head_cfg),
+                     "traffic": round(dram_bytes_per_site(head_cfg) * V),
+                     "traffic_note": "ncu dram bytes of one launch of this kernel on a smaller lattice "
+                                     "(inputs > L2), scaled by sites"},
         "per_parity_f64": parity,
         "f32": fp32,
         "e2e": e2e,

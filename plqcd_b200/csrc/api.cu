@@ -79,6 +79,8 @@ extern "C" int plqcd_lattice_set_stream(plqcd_lattice *lat, void *stream) {
 extern "C" int plqcd_lattice_synchronize(plqcd_lattice *lat) {
     PLQCD_TRY(check_lat(lat));
     PLQCD_CUDA_TRY(cudaStreamSynchronize(lat->stream));
+    if (dslash_tma_status(true))
+        return set_error(PLQCD_ERR_TIMEOUT, "dslash: a TMA stage wait ran out; that launch's output is incomplete");
     return PLQCD_OK;
 }
 

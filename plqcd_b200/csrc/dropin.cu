@@ -25,12 +25,26 @@ using namespace plqcd;
 
 namespace {
 
-constexpr int kMaxChunks = 16;
+// t-slab chunks of the copy/compute pipeline (chunk_plan)
+constexpr int kMaxChunks = 64;
 
 struct SplitCache {  // gauge field of the split entry points, by host address
     const double *re = nullptr, *im = nullptr;
     uint64_t fp = 0;
 };
+
+// what a captured pipeline graph depends on besides the device buffers
+struct GraphKey {
+    const void *src = nullptr, *dst = nullptr;
+    int parity = 0, plan = 0;  // plan: chunk_plan's id
+    unsigned flags = 0;
+    const void *gauge = nullptr;
+    bool operator==(const GraphKey &o) const {
+        return src == o.src && dst == o.dst && parity == o.parity && plan == o.plan && flags == o.flags &&
+               gauge == o.gauge;
+    }
+};
+constexpr int kGraphSlots = 4;
 
 struct DropIn {
     plqcd_gauge *gauge_split = nullptr, *gauge12 = nullptr;
@@ -48,6 +62,12 @@ struct DropIn {
     bool dirty = true;
     cudaStream_t stream = nullptr;  // owned by the drop-in path
     double kernel_ms = 0, h2d = 0, d2h = 0;
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};  // capture fork / join
+    GraphKey graph_key[kGraphSlots];
+    cudaGraphExec_t graph_exec[kGraphSlots] = {};
+    int graph_next = 0;
+    GraphKey last_key;
+    bool last_valid = false;
 };
 
 std::mutex g_mu;
@@ -61,9 +81,13 @@ void release_locked() {
     void *bufs[4] = {g_d.aos_in, g_d.aos_out, g_d.f_in, g_d.f_out};
     for (void *b : bufs)
         if (b) cudaFree(b);
+    for (cudaGraphExec_t x : g_d.graph_exec)
+        if (x) cudaGraphExecDestroy(x);
     for (int c = 0; c < kMaxChunks; c++)
         for (cudaEvent_t ev : {g_d.ev_in[c], g_d.ev_out[c], g_d.ev_k0[c], g_d.ev_k1[c]})
             if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : {g_d.ev_fork, g_d.ev_join[0], g_d.ev_join[1]})
+        if (ev) cudaEventDestroy(ev);
     if (g_d.s_h2d) cudaStreamDestroy(g_d.s_h2d);
     if (g_d.s_d2h) cudaStreamDestroy(g_d.s_d2h);
     if (g_d.lat) plqcd_lattice_destroy(g_d.lat);
@@ -75,6 +99,47 @@ bool env_flag(const char *name, bool dflt) {
     const char *v = getenv(name);
     if (!v || !*v) return dflt;
     return !(v[0] == '0' || v[0] == 'n' || v[0] == 'N' || v[0] == 'f' || v[0] == 'F');
+}
+
+int env_int_dropin(const char *name, int dflt) {
+    const char *v = getenv(name);
+    return (v && *v) ? atoi(v) : dflt;
+}
+
+// Chunk boundaries in t-slabs, bound[0] = 0 ... bound[nch] = L3. Default:
+// chunk sizes 1, 1, 2, 4, ... up to `cap` slabs, from both ends inward, so
+// the chunks that cross PCIe alone (the first three up, the last two or
+// three down) are one slab each and the middle ones are large.
+// PLQCD_DROPIN_CHUNKS=n: n equal chunks instead; PLQCD_DROPIN_CAP: the cap
+// (default L3/8).
+int chunk_plan(int L3, int *bound, int *plan_id) {
+    const int uniform = env_int_dropin("PLQCD_DROPIN_CHUNKS", 0);
+    if (uniform > 0) {
+        const int n = uniform > kMaxChunks ? kMaxChunks : (uniform > L3 ? L3 : uniform);
+        for (int c = 0; c <= n; c++) bound[c] = (int)((long)c * L3 / n);
+        *plan_id = n;
+        return n;
+    }
+    int cap = env_int_dropin("PLQCD_DROPIN_CAP", L3 / 8);
+    cap = cap < 1 ? 1 : cap;
+    int left[kMaxChunks], right[kMaxChunks], nl = 0, nr = 0, rem = L3, step = 1, k = 0;
+    while (rem > 0 && nl + nr < kMaxChunks - 1) {
+        int sz = step < cap ? step : cap;
+        left[nl++] = sz < rem ? sz : rem;
+        rem -= left[nl - 1];
+        if (rem > 0) {
+            right[nr++] = sz < rem ? sz : rem;
+            rem -= right[nr - 1];
+        }
+        if (k++ > 0) step *= 2;  // 1, 1, 2, 4, ...
+    }
+    if (rem > 0) left[nl++] = rem;  // chunk budget exhausted: one more
+    int n = 0;
+    bound[0] = 0;
+    for (int i = 0; i < nl; i++, n++) bound[n + 1] = bound[n] + left[i];
+    for (int i = nr - 1; i >= 0; i--, n++) bound[n + 1] = bound[n] + right[i];
+    *plan_id = -cap;
+    return n;
 }
 
 uint64_t fingerprint(const su3 *u, long nlinks) {
@@ -127,6 +192,8 @@ int ensure_locked() {
         ok = cudaEventCreateWithFlags(&g_d.ev_in[c], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreateWithFlags(&g_d.ev_out[c], cudaEventDisableTiming) == cudaSuccess &&
              cudaEventCreate(&g_d.ev_k0[c]) == cudaSuccess && cudaEventCreate(&g_d.ev_k1[c]) == cudaSuccess;
+    for (cudaEvent_t *ev : {&g_d.ev_fork, &g_d.ev_join[0], &g_d.ev_join[1]})
+        ok = ok && cudaEventCreateWithFlags(ev, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         release_locked();
@@ -134,6 +201,136 @@ int ensure_locked() {
     }
     g_d.dirty = true;
     return PLQCD_OK;
+}
+
+// Enqueue the copy / compute pipeline of one call over chunks of t-slabs
+// (contiguous half-site ranges). The host->device stream carries copies
+// only, back to back, in the order last, 0, 1, ...; the compute stream
+// converts each chunk to the device layout as it lands and computes the
+// output chunk whose neighbours have all arrived; the device->host stream
+// copies each output chunk back while later chunks are still in flight, so
+// the two transfer directions overlap each other and the kernels.
+// `capture`: kernel-time events become graph event-record nodes.
+int enqueue_pipeline(plqcd_lattice *lat, const spinor *src, spinor *dst, int out_parity, unsigned flags, int nch,
+                     const int *bound, bool capture) {
+    const Geom &geo = lat->geom;
+    cudaStream_t s = lat->stream;
+    const int L3 = geo.L[3];
+    const long slab = geo.Vh / L3;
+    auto first = [&](int c) { return slab * (long)bound[c]; };
+    auto count = [&](int c) { return first(c + 1) - first(c); };
+    auto mark = [&](cudaEvent_t ev) {
+        return capture ? cudaEventRecordWithFlags(ev, s, cudaEventRecordExternal) : cudaEventRecord(ev, s);
+    };
+    spinor *ain = static_cast<spinor *>(g_d.aos_in), *aout = static_cast<spinor *>(g_d.aos_out);
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < nch && e == cudaSuccess; k++) {
+        const int c = (k == 0) ? nch - 1 : k - 1;
+        e = cudaMemcpyAsync(ain + first(c), src + first(c), count(c) * sizeof(spinor), cudaMemcpyHostToDevice,
+                            g_d.s_h2d);
+        if (e == cudaSuccess) e = cudaEventRecord(g_d.ev_in[c], g_d.s_h2d);
+    }
+    auto import = [&](int c) -> int {
+        if (cudaStreamWaitEvent(s, g_d.ev_in[c], 0) != cudaSuccess)
+            return set_error(PLQCD_ERR_CUDA, "hopping matrix: stream wait failed");
+        // staging holds one parity, so it is addressed as parity 0
+        return launch_spinor_import(geo, s, ain, 0, g_d.f_in, PLQCD_F64, first(c), count(c));
+    };
+    // Output chunk c is shifted one slab back from input chunk c: it covers
+    // slabs [bound[c] - 1, bound[c+1] - 1) (chunk 0 starts at slab 0, the
+    // last one ends at L3), whose neighbours lie in input chunks <= c and the
+    // first-sent last chunk. It is computed as soon as input chunk c is in,
+    // so results go back while the next input chunk is still coming up.
+    auto out_first = [&](int c) { return c == 0 ? 0L : first(c) - slab; };
+    auto out_end = [&](int c) { return c == nch - 1 ? geo.Vh : first(c + 1) - slab; };
+    auto compute = [&](int c) -> int {
+        const long h0 = out_first(c), n = out_end(c) - h0;
+        mark(g_d.ev_k0[c]);
+        if (n > 0) {
+            DslashCall dc;
+            dc.gauge = g_d.gauge->data;
+            dc.prec = PLQCD_F64;
+            dc.recon = 18;
+            dc.out = g_d.f_out;
+            dc.in = g_d.f_in;
+            dc.out_parity = out_parity;
+            dc.flags = flags;
+            dc.h_begin = h0;
+            dc.h_count = n;
+            PLQCD_TRY(launch_dslash(geo, s, dc));
+        }
+        mark(g_d.ev_k1[c]);
+        if (n <= 0) return PLQCD_OK;
+        PLQCD_TRY(launch_spinor_export(geo, s, g_d.f_out, PLQCD_F64, 0, aout, h0, n));
+        cudaError_t r = cudaEventRecord(g_d.ev_out[c], s);
+        if (r == cudaSuccess) r = cudaStreamWaitEvent(g_d.s_d2h, g_d.ev_out[c], 0);
+        if (r == cudaSuccess)
+            r = cudaMemcpyAsync(dst + h0, aout + h0, n * sizeof(spinor), cudaMemcpyDeviceToHost, g_d.s_d2h);
+        if (r != cudaSuccess) return set_error(PLQCD_ERR_CUDA, "hopping matrix: %s", cudaGetErrorString(r));
+        return PLQCD_OK;
+    };
+    if (e == cudaSuccess) {
+        if (nch > 1) PLQCD_TRY(import(nch - 1));
+        for (int c = 0; c <= nch - 2; c++) {
+            PLQCD_TRY(import(c));
+            PLQCD_TRY(compute(c));
+        }
+        if (nch == 1) PLQCD_TRY(import(0));
+        PLQCD_TRY(compute(nch - 1));
+    }
+    if (e != cudaSuccess) return set_error(PLQCD_ERR_CUDA, "hopping matrix: %s", cudaGetErrorString(e));
+    return PLQCD_OK;
+}
+
+bool host_pinned(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+cudaGraphExec_t find_graph(const GraphKey &k) {
+    for (int i = 0; i < kGraphSlots; i++)
+        if (g_d.graph_exec[i] && g_d.graph_key[i] == k) return g_d.graph_exec[i];
+    return nullptr;
+}
+
+// Capture the pipeline of `k` into a graph (fork to the copy streams and
+// join back on the compute stream); nullptr when anything fails, and the
+// caller runs the pipeline eagerly.
+cudaGraphExec_t capture_graph(plqcd_lattice *lat, const GraphKey &k, const spinor *src, spinor *dst, int nch,
+                              const int *bound) {
+    cudaStream_t s = lat->stream;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    bool ok = cudaEventRecord(g_d.ev_fork, s) == cudaSuccess &&
+              cudaStreamWaitEvent(g_d.s_h2d, g_d.ev_fork, 0) == cudaSuccess &&
+              cudaStreamWaitEvent(g_d.s_d2h, g_d.ev_fork, 0) == cudaSuccess;
+    ok = ok && enqueue_pipeline(lat, src, dst, k.parity, k.flags, nch, bound, true) == PLQCD_OK;
+    ok = ok && cudaEventRecord(g_d.ev_join[0], g_d.s_h2d) == cudaSuccess &&
+         cudaEventRecord(g_d.ev_join[1], g_d.s_d2h) == cudaSuccess &&
+         cudaStreamWaitEvent(s, g_d.ev_join[0], 0) == cudaSuccess &&
+         cudaStreamWaitEvent(s, g_d.ev_join[1], 0) == cudaSuccess;
+    cudaGraph_t graph = nullptr;
+    const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
+    cudaGraphExec_t exec = nullptr;
+    if (ok && ended && graph && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) exec = nullptr;
+    if (graph) cudaGraphDestroy(graph);
+    if (!exec) {
+        cudaGetLastError();
+        clear_error();
+        return nullptr;
+    }
+    const int slot = g_d.graph_next;
+    g_d.graph_next = (slot + 1) % kGraphSlots;
+    if (g_d.graph_exec[slot]) cudaGraphExecDestroy(g_d.graph_exec[slot]);
+    g_d.graph_exec[slot] = exec;
+    g_d.graph_key[slot] = k;
+    return exec;
 }
 
 // out_parity 0: eo (qout even half from qin odd half); 1: oe.
@@ -165,56 +362,32 @@ double hop_call(spinor *qin, spinor *qout, su3 *u, int out_parity) {
         g_d.h2d += 8.0 * Vh * sizeof(su3);
     }
 
-    // Pipeline over chunks of t-slabs (contiguous half-site ranges): input
-    // chunks go up on the copy stream in the order last, 0, 1, ..., and
-    // output chunk c is computed once input chunks c-1, c, c+1 (periodic)
-    // have arrived, then copied back on a second copy stream while later
-    // chunks are still in flight; host->device and device->host transfers
-    // overlap each other and the kernels.
     const int in_parity = out_parity ^ 1;
     const unsigned flags = env_flag("PLQCD_REF_COMPAT", false) ? PLQCD_DSLASH_COMPAT : 0u;
-    const Geom &geo = lat->geom;
-    const int L3 = geo.L[3];
-    const long slab = geo.Vh / L3;
-    const int nch = L3 < kMaxChunks ? L3 : kMaxChunks;
-    auto first = [&](int c) { return slab * (long)((long)c * L3 / nch); };
-    auto count = [&](int c) { return first(c + 1) - first(c); };
+    int bound[kMaxChunks + 1], plan_id = 0;
+    const int nch = chunk_plan(lat->geom.L[3], bound, &plan_id);
     const spinor *src = qin + in_parity * Vh;
     spinor *dst = qout + out_parity * Vh;
-    spinor *ain = static_cast<spinor *>(g_d.aos_in), *aout = static_cast<spinor *>(g_d.aos_out);
-    cudaError_t e = cudaSuccess;
-    for (int k = 0; k < nch && e == cudaSuccess; k++) {
-        const int c = (k == 0) ? nch - 1 : k - 1;
-        e = cudaMemcpyAsync(ain + first(c), src + first(c), count(c) * sizeof(spinor), cudaMemcpyHostToDevice,
-                            g_d.s_h2d);
-        // staging holds one parity, so it is addressed as parity 0
-        if (e == cudaSuccess &&
-            launch_spinor_import(geo, g_d.s_h2d, ain, 0, g_d.f_in, PLQCD_F64, first(c), count(c)) != PLQCD_OK)
-            return -1.0;
-        if (e == cudaSuccess) e = cudaEventRecord(g_d.ev_in[c], g_d.s_h2d);
+
+    // Replay the pipeline as one CUDA graph when the same host arrays come
+    // back (the usual solver loop): one launch instead of ~10 API calls per
+    // chunk. Captured on the second call with a key, so the first call has
+    // tuned the kernels eagerly; pinned host arrays only.
+    const GraphKey key{src, dst, out_parity, plan_id, flags, g_d.gauge->data};
+    cudaGraphExec_t exec = nullptr;
+    bool graphed = false;
+    if (env_flag("PLQCD_DROPIN_GRAPH", true) && host_pinned(src) && host_pinned(dst)) {
+        exec = find_graph(key);
+        if (!exec && g_d.last_valid && g_d.last_key == key) exec = capture_graph(lat, key, src, dst, nch, bound);
+        g_d.last_key = key;
+        g_d.last_valid = true;
     }
-    for (int c = 0; c < nch && e == cudaSuccess; c++) {
-        for (int d : {c - 1, c, c + 1}) cudaStreamWaitEvent(s, g_d.ev_in[(d + nch) % nch], 0);
-        cudaEventRecord(g_d.ev_k0[c], s);
-        DslashCall dc;
-        dc.gauge = g_d.gauge->data;
-        dc.prec = PLQCD_F64;
-        dc.recon = 18;
-        dc.out = g_d.f_out;
-        dc.in = g_d.f_in;
-        dc.out_parity = out_parity;
-        dc.flags = flags;
-        dc.h_begin = first(c);
-        dc.h_count = count(c);
-        if (launch_dslash(geo, s, dc) != PLQCD_OK) return -1.0;
-        cudaEventRecord(g_d.ev_k1[c], s);
-        if (launch_spinor_export(geo, s, g_d.f_out, PLQCD_F64, 0, aout, first(c), count(c)) != PLQCD_OK) return -1.0;
-        cudaEventRecord(g_d.ev_out[c], s);
-        cudaStreamWaitEvent(g_d.s_d2h, g_d.ev_out[c], 0);
-        e = cudaMemcpyAsync(dst + first(c), aout + first(c), count(c) * sizeof(spinor), cudaMemcpyDeviceToHost,
-                            g_d.s_d2h);
+    if (exec) {
+        graphed = cudaGraphLaunch(exec, s) == cudaSuccess;
+        if (!graphed) cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(g_d.s_d2h);
+    if (!graphed && enqueue_pipeline(lat, src, dst, out_parity, flags, nch, bound, false) != PLQCD_OK) return -1.0;
+    cudaError_t e = cudaStreamSynchronize(g_d.s_d2h);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         set_error(PLQCD_ERR_CUDA, "hopping matrix: %s", cudaGetErrorString(e));

@@ -20,8 +20,10 @@
 // is read from HBM once: 192 + 4*144 + 192 = 960 B per site.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <type_traits>
+#include <vector>
 
 #include "dslash_core.cuh"
 #include "internal.h"
@@ -377,6 +379,9 @@ static int launch_pr(const Geom &g, cudaStream_t s, const DslashArgs &a, int var
 
 }  // namespace dev
 
+int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, int prec, int recon, bool full,
+                      bool xpay, int nstage, int ny);
+
 static int env_int(const char *name, int dflt) {
     const char *e = getenv(name);
     return e ? atoi(e) : dflt;
@@ -403,15 +408,23 @@ int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
 
     // explicit configuration (block from the call, or the environment for
     // experiments) bypasses the tuner
-    const int env_block = env_int("PLQCD_DSLASH_BLOCK", 0), env_var = env_int("PLQCD_DSLASH_STAGES", -1);
+    int env_block = env_int("PLQCD_DSLASH_BLOCK", 0), env_var = env_int("PLQCD_DSLASH_STAGES", -1);
+    // PLQCD_DSLASH_FULL_STAGES: the variant of full-lattice F64 calls only
+    if (c.full && c.prec == PLQCD_F64 && env_int("PLQCD_DSLASH_FULL_STAGES", -1) >= 0) {
+        env_var = env_int("PLQCD_DSLASH_FULL_STAGES", -1);
+        if (env_block <= 0) env_block = 64;
+    }
     if (c.block > 0 || env_block > 0 || env_var >= 0) {
         int block = c.block > 0 ? c.block : (env_block > 0 ? env_block : 128);
         return dispatch(g, s, c, a, env_var >= 0 ? env_var : 2, block);
     }
     char key[256];
-    snprintf(key, sizeof key, "%sdslash|p%d|r%d|%s%s%s|%dx%dx%dx%d|n%d", device_tag().c_str(), c.prec, c.recon,
-             c.full ? "full" : "half", c.x ? "+xpay" : "", compat ? "+compat" : "", g.L[0], g.L[1], g.L[2], g.L[3],
-             c.nrhs);
+    // a partial site range (the drop-in path's t-slab chunks) is a separate
+    // entry: the TMA kernel takes whole fields only
+    const bool part = a.h_begin != 0 || a.h_end != g.Vh;
+    snprintf(key, sizeof key, "%sdslash|p%d|r%d|%s%s%s%s|%dx%dx%dx%d|n%d", device_tag().c_str(), c.prec, c.recon,
+             c.full ? "full" : "half", c.x ? "+xpay" : "", compat ? "+compat" : "", part ? "+range" : "", g.L[0],
+             g.L[1], g.L[2], g.L[3], c.nrhs);
     return tune_dslash(g, s, c, a, key);
 }
 
@@ -466,11 +479,45 @@ static int tune_dslash(const Geom &g, cudaStream_t s, const DslashCall &c, const
             cands.push_back(r);
         }
     }
+    // TMA-staged rows: ring depth x rows per tile, where the tile fits
+    const bool tma_ok = !(c.flags & PLQCD_DSLASH_COMPAT) && c.nrhs == 1 && a.h_begin == 0 && a.h_end == g.Vh &&
+                        getenv("PLQCD_NO_TMA") == nullptr;
+    if (tma_ok)
+        for (int ny : {4, 8, 16, 2})
+            for (int ns : {2, 3, 4, 6}) {
+                int blk = 0;
+                if (dslash_tma_plan(g, c.prec, c.recon, ns, ny, &blk, nullptr) != PLQCD_OK) {
+                    clear_error();
+                    continue;
+                }
+                TuneResult r;
+                r.variant = 1000 + 100 * ns + ny;
+                r.block = blk;
+                cands.push_back(r);
+            }
     // trial launches write into scratch outputs: an xpay whose output aliases
     // its x operand must not be applied more than once
     void *scratch[2] = {nullptr, nullptr};
+    std::vector<int> tma_checked;
     auto run = [&](const TuneResult &r, bool trial) -> int {
         if (!trial) return dispatch(g, s, c, a, r.variant, r.block);
+        if (r.variant >= 1000 && std::find(tma_checked.begin(), tma_checked.end(), r.variant) == tma_checked.end()) {
+            // first trial of a TMA configuration: run it alone and check that
+            // no stage wait ran out before it is timed
+            tma_checked.push_back(r.variant);
+            dev::DslashArgs t = a;
+            size_t bytes = spinor_parity_bytes(g.Vh, c.prec);
+            for (int k = 0; k < (c.full ? 2 : 1); k++)
+                if (!scratch[k] && cudaMalloc(&scratch[k], bytes) != cudaSuccess) {
+                    cudaGetLastError();
+                    return set_error(PLQCD_ERR_NOMEM, "tune: scratch allocation failed");
+                }
+            t.out[0] = scratch[0];
+            if (c.full) t.out[1] = scratch[1];
+            PLQCD_TRY(dispatch(g, s, c, t, r.variant, r.block));
+            PLQCD_CUDA_TRY(cudaStreamSynchronize(s));
+            if (dslash_tma_status(true)) return set_error(PLQCD_ERR_CUDA, "dslash: TMA stage wait timed out");
+        }
         size_t bytes = spinor_parity_bytes(g.Vh, c.prec) * c.nrhs;
         for (int k = 0; k < (c.full ? 2 : 1); k++)
             if (!scratch[k] && cudaMalloc(&scratch[k], bytes) != cudaSuccess) {
@@ -495,6 +542,10 @@ static int dispatch(const Geom &g, cudaStream_t s, const DslashCall &c, const de
                     int block) {
     const bool compat = (c.flags & PLQCD_DSLASH_COMPAT) != 0;
     const bool xpay = c.x != nullptr;
+    if (variant >= 1000) {  // TMA-staged rows; the block follows from the tile
+        if (compat) return set_error(PLQCD_ERR_ARG, "dslash: no bug-compatible TMA kernel");
+        return launch_dslash_tma(g, s, a, c.prec, c.recon, c.full, xpay, (variant / 100) % 10, variant % 100);
+    }
     if (block % 32 || block < 32 || block > 256) return set_error(PLQCD_ERR_ARG, "dslash: block size %d invalid", block);
     switch (c.prec * 100 + c.recon) {
         case PLQCD_F64 * 100 + 18: return dev::launch_pr<PLQCD_F64, 18>(g, s, a, variant, block, compat, xpay, c.full);

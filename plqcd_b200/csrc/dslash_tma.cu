@@ -1,0 +1,489 @@
+// dslash_tma.cu -- hopping matrix with TMA-staged neighbour rows (sm_100a).
+//
+// Same operator and arithmetic order as the gather kernels of dslash.cu
+// (lib/dirac.c:35-408 eo, 414-791 oe; results are bit-identical), with a
+// different way of feeding the SMs. The cp.async kernels copy every
+// neighbour spinor and link global->shared with per-thread LDGSTS and read
+// it back with LDS: both passes go through the LSU data pipe, which ncu
+// shows as the limit of the full-lattice kernel (l1tex data-pipe wavefronts
+// ~78% of peak, ~74% of them shared-memory wavefronts). Here one producer
+// warp moves whole rows with tensor-memory-access tile loads, which write
+// shared memory without LSU wavefronts, and the consumer warps only read.
+//
+// Work unit ("tile"): NY consecutive rows (a row is the L0/2 half-sites of
+// one (y, z, t) line) of one output parity; a CTA has NY*L0/2 consumer
+// threads, one output site each, plus one producer warp. CTAs are
+// persistent and take tiles round-robin; with both parities (full lattice)
+// the tile index runs parity-fastest, so the two parities of the same rows
+// are processed at the same time and a link read from HBM for one parity's
+// forward term serves the other's backward term from L2.
+//
+// Per tile the producer fills 8 stages, one per direction, in a ring of
+// `nstage` shared-memory buffers (full / empty mbarrier pairs):
+//   x+, x-:  the tile's own rows of the input (the x neighbours sit in the
+//            same rows) and the mu=0 links (own parity / opposite parity);
+//   y+, y-:  own rows plus one extra row across the tile edge (y0+NY or
+//            y0-1, periodic); for y- also the extra link row;
+//   z+-, t+-: the NY rows of the neighbouring (z, t) line, links likewise.
+// Every coordinate passed to a tile load is a wrapped, in-range coordinate
+// and the innermost one is always 0, so no load reads out of bounds.
+//
+// Every mbarrier wait is bounded (2 s by %globaltimer). A wait that runs
+// out sets a device status flag (read by dslash_tma_status()), the CTA's
+// threads stop, and the producer waits (bounded again) for the copies it
+// issued before it returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <atomic>
+#include <cstring>
+#include <mutex>
+
+#include "dslash_core.cuh"
+#include "internal.h"
+#include "tma.cuh"
+
+namespace plqcd {
+namespace dev {
+
+struct TmaGeom {
+    long Vh;
+    int L0, L0h, L1, L2, L3;
+    int NY;       // rows per tile (divides L1)
+    int nty;      // L1 / NY
+    int nitems;   // tiles (x 2 parities in full mode)
+    int nstage;   // shared-memory buffers in the ring
+    int ncw;      // consumer warps = NY * L0h / 32
+    int full, out_parity;
+    // byte offsets inside one stage buffer and the bytes each load brings
+    uint32_t off_sp_row, off_lk_main, off_lk_row, stage_bytes;
+    uint32_t sp_main_bytes, sp_row_bytes, lk_main_bytes, lk_row_bytes;
+    double a_up, a_low, b, g5_in;
+    void *out0, *out1;  // output of parity 0 / 1 (full); out0 otherwise
+    const void *x;      // xpay operand (single parity)
+};
+
+// tensor maps: input spinor field f (full mode: field 0 = even input, read
+// by the odd output; field 1 = odd input), NY-row and one-row boxes
+struct __align__(64) TmaMaps {
+    CUtensorMap sp_main[2], sp_row[2], lk_main, lk_row;
+};
+
+__device__ int g_tma_status;  // set to 1 when a stage wait ran out
+
+struct TileCoord {
+    int p, y0, zt, z, t;
+};
+
+__device__ __forceinline__ TileCoord tile_coord(const TmaGeom &g, int item) {
+    TileCoord c;
+    int tile;
+    if (g.full) {
+        c.p = item & 1;
+        tile = item >> 1;
+    } else {
+        c.p = g.out_parity;
+        tile = item;
+    }
+    c.zt = tile / g.nty;
+    c.y0 = (tile - c.zt * g.nty) * g.NY;
+    c.t = c.zt / g.L2;
+    c.z = c.zt - c.t * g.L2;
+    return c;
+}
+
+// loads of direction d (0..3 forward mu, 4..7 backward mu) into the stage
+// buffer at shared address dst, completing on `bar`
+__device__ __forceinline__ void tma_issue_dir(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, int d,
+                                              uint32_t dst, uint32_t bar) {
+    const int f = g.full ? (c.p == 0 ? 1 : 0) : 0;
+    const int q = c.p ^ 1;
+    const int mu = d & 3;
+    const bool fwd = d < 4;
+    int szt = c.zt;  // (z, t) line of the neighbour rows
+    if (mu == 2) {
+        const int z2 = fwd ? (c.z + 1 == g.L2 ? 0 : c.z + 1) : (c.z == 0 ? g.L2 - 1 : c.z - 1);
+        szt = z2 + g.L2 * c.t;
+    } else if (mu == 3) {
+        const int t2 = fwd ? (c.t + 1 == g.L3 ? 0 : c.t + 1) : (c.t == 0 ? g.L3 - 1 : c.t - 1);
+        szt = c.z + g.L2 * t2;
+    }
+    // forward links sit at the output site, backward ones at the neighbour
+    const int lzt = fwd ? c.zt : szt;
+    const int lplane = (fwd ? c.p : q) * 4 + mu;
+    uint32_t bytes = g.sp_main_bytes + g.lk_main_bytes;
+    if (d == 1) bytes += g.sp_row_bytes;
+    if (d == 5) bytes += g.sp_row_bytes + g.lk_row_bytes;
+    mbar_arrive_expect_tx(bar, bytes);
+    const void *spm = f ? (const void *)&m.sp_main[1] : (const void *)&m.sp_main[0];
+    const void *spr = f ? (const void *)&m.sp_row[1] : (const void *)&m.sp_row[0];
+    tma_load_4d(dst, spm, bar, 0, c.y0, szt, 0);
+    tma_load_5d(dst + g.off_lk_main, &m.lk_main, bar, 0, c.y0, lzt, 0, lplane);
+    if (d == 1) {
+        const int yr = (c.y0 + g.NY == g.L1) ? 0 : c.y0 + g.NY;
+        tma_load_4d(dst + g.off_sp_row, spr, bar, 0, yr, c.zt, 0);
+    } else if (d == 5) {
+        const int yr = (c.y0 == 0) ? g.L1 - 1 : c.y0 - 1;
+        tma_load_4d(dst + g.off_sp_row, spr, bar, 0, yr, c.zt, 0);
+        tma_load_5d(dst + g.off_lk_row, &m.lk_row, bar, 0, yr, c.zt, 0, q * 4 + 1);
+    }
+}
+
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+constexpr uint64_t kDrainLimitNs = 200000000ull;  // 0.2 s
+
+template <class SIO, class LIO, bool XPAY>
+__global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ TmaMaps m,
+                                                        const __grid_constant__ TmaGeom g) {
+    using R = typename SIO::real;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ int s_abort;
+    const uint32_t raw = smem_addr(smem_raw);
+    const uint32_t pad = ((raw + 127u) & ~127u) - raw;
+    const uint8_t *sbase = smem_raw + pad;
+    const uint32_t base = raw + pad;
+    const uint32_t full_bar = base + (uint32_t)g.nstage * g.stage_bytes;
+    const uint32_t empty_bar = full_bar + 8u * g.nstage;
+    const int bid = blockIdx.x;
+    const int nmine = bid < g.nitems ? (g.nitems - 1 - bid) / (int)gridDim.x + 1 : 0;
+    const int nthr_c = g.ncw * 32;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_abort = 0;
+        for (int b = 0; b < g.nstage; b++) {
+            mbar_init(full_bar + 8u * b, 1);
+            mbar_init(empty_bar + 8u * b, (uint32_t)g.ncw);
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (nmine == 0) return;
+    volatile int *abort = &s_abort;
+
+    if (tid >= nthr_c) {
+        // producer warp: lane 0 issues every stage of every tile of this CTA
+        if (tid != nthr_c) return;
+        tma_prefetch_map(&m.lk_main);
+        int b = 0;
+        uint32_t k = 0;  // completed passes over the ring
+        long issued = 0;
+        bool ok = true;
+        for (int it = 0; it < nmine && ok; it++) {
+            const TileCoord c = tile_coord(g, bid + it * (int)gridDim.x);
+#pragma unroll 1
+            for (int d = 0; d < 8; d++) {
+                // the consumers released this buffer's previous use
+                if (!mbar_wait(empty_bar + 8u * b, (k + 1) & 1, kWaitLimitNs, abort)) {
+                    ok = false;
+                    break;
+                }
+                tma_issue_dir(m, g, c, d, base + (uint32_t)b * g.stage_bytes, full_bar + 8u * b);
+                issued++;
+                if (++b == g.nstage) {
+                    b = 0;
+                    k++;
+                }
+            }
+        }
+        if (!ok) {
+            *abort = 1;
+            atomicExch(&g_tma_status, 1);
+        }
+        // never leave with copies in flight: wait for the last stages issued
+        const long first = issued > g.nstage ? issued - g.nstage : 0;
+        for (long s = first; s < issued; s++) {
+            const int bb = (int)(s % g.nstage);
+            const uint32_t par = (uint32_t)(s / g.nstage) & 1;
+            if (!mbar_wait(full_bar + 8u * bb, par, kDrainLimitNs, nullptr)) atomicExch(&g_tma_status, 1);
+        }
+        return;
+    }
+
+    // consumers: thread (row j, half-x xh) of the tile
+    const int L0h = g.L0h;
+    const int j = tid / L0h, xh = tid - j * L0h;
+    const int own = j * L0h + xh;
+    const int SM = g.NY * L0h;  // plane stride of an NY-row box, 16-byte units
+    const R sg = (R)g.g5_in;
+    const R aup = (R)g.a_up, alow = (R)g.a_low;
+    int b = 0;
+    uint32_t k = 0;
+    for (int it = 0; it < nmine; it++) {
+        const TileCoord c = tile_coord(g, bid + it * (int)gridDim.x);
+        const int y = c.y0 + j;
+        const int x = 2 * xh + ((y + c.z + c.t + c.p) & 1);
+        const int xph = ((x + 1 == g.L0) ? 0 : x + 1) >> 1;
+        const int xmh = ((x == 0) ? g.L0 - 1 : x - 1) >> 1;
+        cx<R> acc[12];
+#pragma unroll
+        for (int e = 0; e < 12; e++) acc[e] = {R(0), R(0)};
+#pragma unroll
+        for (int d = 0; d < 8; d++) {
+            if (!mbar_wait(full_bar + 8u * b, k & 1, kWaitLimitNs, abort)) {
+                *abort = 1;
+                atomicExch(&g_tma_status, 1);
+                return;
+            }
+            const uint8_t *st = sbase + (size_t)b * g.stage_bytes;
+            const uint4 *spm = reinterpret_cast<const uint4 *>(st);
+            const uint4 *spr = reinterpret_cast<const uint4 *>(st + g.off_sp_row);
+            const uint4 *lkm = reinterpret_cast<const uint4 *>(st + g.off_lk_main);
+            const uint4 *lkr = reinterpret_cast<const uint4 *>(st + g.off_lk_row);
+            const uint4 *sp, *lk;
+            int sst = SM, lst = SM;
+            if (d == 0) {
+                sp = spm + (own - xh + xph);
+                lk = lkm + own;
+            } else if (d == 4) {
+                sp = spm + (own - xh + xmh);
+                lk = lkm + (own - xh + xmh);
+            } else if (d == 1) {
+                lk = lkm + own;
+                if (j + 1 < g.NY) {
+                    sp = spm + own + L0h;
+                } else {
+                    sp = spr + xh;
+                    sst = L0h;
+                }
+            } else if (d == 5) {
+                if (j > 0) {
+                    sp = spm + own - L0h;
+                    lk = lkm + own - L0h;
+                } else {
+                    sp = spr + xh;
+                    lk = lkr + xh;
+                    sst = L0h;
+                    lst = L0h;
+                }
+            } else {
+                sp = spm + own;
+                lk = lkm + own;
+            }
+            cx<R> s[12], U[9];
+            R n;
+            SIO::load_staged_raw(sp, sst, s, n);
+            LIO::load_staged(lk, lst, U);
+            // the values are in registers: release the buffer to the producer
+            __syncwarp();
+            if ((tid & 31) == 0) mbar_arrive(empty_bar + 8u * b);
+            compute_dir_n<false, SIO::kScaled, R>(d, acc, s, U, sg, n);
+            if (++b == g.nstage) {
+                b = 0;
+                k++;
+            }
+        }
+        const long h = xh + (long)L0h * (y + (long)g.L1 * c.zt);
+        void *out = (g.full && c.p == 1) ? g.out1 : g.out0;
+        if (XPAY) {
+            cx<R> xv[12];
+            SIO::load(g.x, g.Vh, h, xv);
+            const R bb = (R)g.b;
+#pragma unroll
+            for (int e = 0; e < 12; e++) {
+                const R ak = e < 6 ? aup : alow;
+                acc[e] = {fma(ak, acc[e].re, bb * xv[e].re), fma(ak, acc[e].im, bb * xv[e].im)};
+            }
+        } else {
+#pragma unroll
+            for (int e = 6; e < 12; e++) acc[e] = {alow * acc[e].re, alow * acc[e].im};
+#pragma unroll
+            for (int e = 0; e < 6; e++) acc[e] = {aup * acc[e].re, aup * acc[e].im};
+        }
+        SIO::store(out, g.Vh, h, acc);
+    }
+}
+
+}  // namespace dev
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// a field of `planes` 16-byte planes over the half lattice, viewed as
+// (2*L0h u64, L1, L2*L3, planes[, 8 parity-mu blocks])
+int encode_map(CUtensorMap *m, const void *base, const Geom &g, int planes, bool links, int rows) {
+    auto fn = encode_fn();
+    if (!fn) return set_error(PLQCD_ERR_CUDA, "dslash: cuTensorMapEncodeTiled is not available");
+    const cuuint64_t row_b = (cuuint64_t)g.L0h * 16;
+    cuuint64_t dims[5] = {(cuuint64_t)2 * g.L0h, (cuuint64_t)g.L[1], (cuuint64_t)g.L[2] * g.L[3],
+                          (cuuint64_t)planes, 8};
+    cuuint64_t strides[4] = {row_b, row_b * g.L[1], (cuuint64_t)g.Vh * 16, (cuuint64_t)g.Vh * 16 * planes};
+    cuuint32_t box[5] = {(cuuint32_t)(2 * g.L0h), (cuuint32_t)rows, 1, (cuuint32_t)planes, 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, links ? 5 : 4, const_cast<void *>(base), dims, strides, box,
+                    es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(PLQCD_ERR_CUDA, "dslash: tensor map encoding failed (%d)", (int)r);
+    return PLQCD_OK;
+}
+
+std::atomic<bool> g_tma_launched{false};
+
+int sm_count() {
+    static int n[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!n[dev]) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        n[dev] = v > 0 ? v : 1;
+    }
+    return n[dev];
+}
+
+inline uint32_t round128(uint32_t v) { return (v + 127u) & ~127u; }
+
+template <class SIO, class LIO, bool XPAY>
+int launch_tma_t(cudaStream_t s, const dev::TmaMaps &m, const dev::TmaGeom &tg, int block, size_t smem) {
+    auto k = dev::k_dslash_tma<SIO, LIO, XPAY>;
+    static size_t attr_bytes = 0;  // per instantiation: the opt-in granted so far
+    if (smem > attr_bytes) {
+        PLQCD_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_bytes = smem;
+    }
+    int occ = 0;
+    PLQCD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, block, smem));
+    if (occ < 1) return set_error(PLQCD_ERR_ARG, "dslash: TMA tile does not fit on an SM (%zu B)", smem);
+    long grid = (long)sm_count() * occ;
+    if (grid > tg.nitems) grid = tg.nitems;
+    g_tma_launched.store(true, std::memory_order_relaxed);
+    k<<<(unsigned)grid, block, smem, s>>>(m, tg);
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+}  // namespace
+
+int dslash_tma_plan(const Geom &g, int prec, int recon, int nstage, int ny, int *block, size_t *smem) {
+    int nsp, nlk;
+    if (prec == PLQCD_F64 && recon == 18) {
+        nsp = 12;
+        nlk = 9;
+    } else if (prec == PLQCD_F64 && recon == 12) {
+        nsp = 12;
+        nlk = 6;
+    } else if (prec == PLQCD_F32 && recon == 12) {
+        nsp = 6;
+        nlk = 3;
+    } else {
+        return set_error(PLQCD_ERR_ARG, "dslash: no TMA kernel for precision/reconstruction %d/%d", prec, recon);
+    }
+    if (nstage < 2 || nstage > 8 || ny < 1 || g.L0h > 128 || g.L[1] % ny || (ny * g.L0h) % 32 ||
+        ny * g.L0h > 256)
+        return set_error(PLQCD_ERR_ARG, "dslash: TMA tile %d rows x %d stages does not fit %dx%dx%dx%d", ny, nstage,
+                         g.L[0], g.L[1], g.L[2], g.L[3]);
+    const uint32_t row = (uint32_t)g.L0h * 16;
+    const uint32_t stage = round128(nsp * row * ny) + round128(nsp * row) + round128(nlk * row * ny) +
+                           round128(nlk * row);
+    const size_t bytes = (size_t)nstage * stage + 16u * nstage + 128;
+    if (bytes > 227u * 1024 - 64) return set_error(PLQCD_ERR_ARG, "dslash: TMA ring of %zu bytes too large", bytes);
+    if (block) *block = ny * g.L0h + 32;
+    if (smem) *smem = bytes;
+    return PLQCD_OK;
+}
+
+int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, int prec, int recon, bool full,
+                      bool xpay, int nstage, int ny) {
+    int block = 0;
+    size_t smem = 0;
+    PLQCD_TRY(dslash_tma_plan(g, prec, recon, nstage, ny, &block, &smem));
+    if (a.nrhs != 1 || a.h_begin != 0 || a.h_end != g.Vh || (full && xpay))
+        return set_error(PLQCD_ERR_ARG, "dslash: the TMA kernel takes whole single fields");
+    const int nsp = prec == PLQCD_F64 ? 12 : 6;
+    const int nlk = prec == PLQCD_F64 ? (recon == 18 ? 9 : 6) : 3;
+    const uint32_t row = (uint32_t)g.L0h * 16;
+
+    dev::TmaGeom tg;
+    memset(&tg, 0, sizeof tg);
+    tg.Vh = g.Vh;
+    tg.L0 = g.L[0];
+    tg.L0h = g.L0h;
+    tg.L1 = g.L[1];
+    tg.L2 = g.L[2];
+    tg.L3 = g.L[3];
+    tg.NY = ny;
+    tg.nty = g.L[1] / ny;
+    const long ntiles = (long)tg.nty * g.L[2] * g.L[3];
+    if (ntiles * (full ? 2 : 1) > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash: lattice too large");
+    tg.nitems = (int)(ntiles * (full ? 2 : 1));
+    tg.nstage = nstage;
+    tg.ncw = ny * g.L0h / 32;
+    tg.full = full ? 1 : 0;
+    tg.out_parity = a.out_parity;
+    tg.sp_main_bytes = nsp * row * ny;
+    tg.sp_row_bytes = nsp * row;
+    tg.lk_main_bytes = nlk * row * ny;
+    tg.lk_row_bytes = nlk * row;
+    tg.off_sp_row = round128(tg.sp_main_bytes);
+    tg.off_lk_main = tg.off_sp_row + round128(tg.sp_row_bytes);
+    tg.off_lk_row = tg.off_lk_main + round128(tg.lk_main_bytes);
+    tg.stage_bytes = tg.off_lk_row + round128(tg.lk_row_bytes);
+    tg.a_up = a.a_up;
+    tg.a_low = a.a_low;
+    tg.b = a.b;
+    tg.g5_in = a.g5_in;
+    tg.out0 = a.out[0];
+    tg.out1 = full ? a.out[1] : a.out[0];
+    tg.x = a.x;
+
+    dev::TmaMaps m;
+    memset(&m, 0, sizeof m);
+    const int nf = full ? 2 : 1;
+    for (int f = 0; f < nf; f++) {
+        PLQCD_TRY(encode_map(&m.sp_main[f], a.in[f], g, nsp, false, ny));
+        PLQCD_TRY(encode_map(&m.sp_row[f], a.in[f], g, nsp, false, 1));
+    }
+    if (!full) {
+        m.sp_main[1] = m.sp_main[0];
+        m.sp_row[1] = m.sp_row[0];
+    }
+    PLQCD_TRY(encode_map(&m.lk_main, a.gauge, g, nlk, true, ny));
+    PLQCD_TRY(encode_map(&m.lk_row, a.gauge, g, nlk, true, 1));
+
+    using namespace dev;
+    if (prec == PLQCD_F64 && recon == 18)
+        return xpay ? launch_tma_t<SpinorIO<PLQCD_F64>, LinkIO<PLQCD_F64, 18>, true>(s, m, tg, block, smem)
+                    : launch_tma_t<SpinorIO<PLQCD_F64>, LinkIO<PLQCD_F64, 18>, false>(s, m, tg, block, smem);
+    if (prec == PLQCD_F64)
+        return xpay ? launch_tma_t<SpinorIO<PLQCD_F64>, LinkIO<PLQCD_F64, 12>, true>(s, m, tg, block, smem)
+                    : launch_tma_t<SpinorIO<PLQCD_F64>, LinkIO<PLQCD_F64, 12>, false>(s, m, tg, block, smem);
+    return xpay ? launch_tma_t<SpinorIO<PLQCD_F32>, LinkIO<PLQCD_F32, 12>, true>(s, m, tg, block, smem)
+                : launch_tma_t<SpinorIO<PLQCD_F32>, LinkIO<PLQCD_F32, 12>, false>(s, m, tg, block, smem);
+}
+
+// Reads (and with `reset`, clears) the timeout flag of the TMA kernel on the
+// current device. Only touches the device when a TMA kernel was launched
+// since the last reset.
+int dslash_tma_status(bool reset) {
+    if (!g_tma_launched.load(std::memory_order_relaxed)) return 0;
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, dev::g_tma_status, sizeof v) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (reset) {
+        if (v) {
+            const int z = 0;
+            cudaMemcpyToSymbol(dev::g_tma_status, &z, sizeof z);
+        }
+        g_tma_launched.store(false, std::memory_order_relaxed);
+    }
+    return v;
+}
+
+}  // namespace plqcd

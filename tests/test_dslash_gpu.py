@@ -3,6 +3,7 @@
 FP64 results must match the reference's operator to 1e-14 relative
 (max |diff| / max |value|); reduced precisions are bounded in relative L2
 against the FP64 kernel."""
+import ctypes
 import os
 
 import numpy as np
@@ -87,6 +88,54 @@ def test_dropin_gauge_cache_sees_in_place_update(dropin, restatement):
     P.hopping_matrix("eo", q, out, u)
     want = restatement.hop("eo", L, q, u)
     assert relmax(out[: V // 2], want[: V // 2]) < TOL64
+
+
+def _pinned(lib, shape):
+    """complex128 array on amalloc'd (pinned) host memory, and its block"""
+    n = int(np.prod(shape)) * 16
+    p = lib.amalloc(n, 6)
+    a = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_double)), (n // 8,)).view(np.complex128)
+    return a.reshape(shape), p
+
+
+@pytest.mark.parametrize("chunks", ["ramp", "1", "3", "16", "64"])
+def test_dropin_pipeline_graph_and_chunking(dropin, restatement, monkeypatch, chunks):
+    """Pinned host arrays: the first call runs the chunked copy/compute
+    pipeline eagerly, the second captures it as a CUDA graph, later calls
+    replay it. Every call, for every chunk count, gives the oracle's result
+    and the same bits as the eager pipeline; a new output array is a new
+    graph (no stale pointers)."""
+    L = (8, 8, 4, 16)
+    dropin(L)
+    V = O.volume(L)
+    lib = P.lib()
+    rng = np.random.default_rng(17)
+    qin, pq = _pinned(lib, (V, 12))
+    u, pu = _pinned(lib, (4 * V, 9))
+    qin[:] = O.gaussian_spinor(V, rng)
+    u[:] = O.random_su3(4 * V, rng)
+    want = restatement.hop("full", L, qin, u)
+    if chunks == "ramp":  # the default plan: 1, 1, 2, ... slab chunks from both ends
+        monkeypatch.delenv("PLQCD_DROPIN_CHUNKS", raising=False)
+    else:
+        monkeypatch.setenv("PLQCD_DROPIN_CHUNKS", chunks)
+    outs = []
+    try:
+        for graph in ("0", "1"):
+            monkeypatch.setenv("PLQCD_DROPIN_GRAPH", graph)
+            for _ in range(3):
+                qout, po = _pinned(lib, (V, 12))
+                for rep in range(3):
+                    qout[:] = 0
+                    P.hopping_matrix("eo", qin, qout, u)
+                    P.hopping_matrix("oe", qin, qout, u)
+                    assert relmax(qout, want) < TOL64
+                    outs.append(np.array(qout))
+                lib.afree(po)
+    finally:
+        lib.afree(pq)
+        lib.afree(pu)
+    assert all(bool((o == outs[0]).all()) for o in outs)
 
 
 def _device_setup(L, seed=1):
@@ -456,3 +505,72 @@ def test_dslash_every_load_strategy(cuda, monkeypatch, variant, block, prec, rec
     want = field_to_host(lat, ref, prec, 1)[lat.V // 2:]
     got = field_to_host(lat, o, prec, 1)[lat.V // 2:]
     assert relmax(got, want) <= tol
+
+
+# TMA-staged kernel: variant 1000 + 100 * ring depth + rows per tile
+TMA_CASES = [((16, 8, 4, 6), 1204), ((16, 8, 4, 6), 1308), ((16, 8, 6, 4), 1404), ((32, 8, 4, 4), 1602),
+             ((8, 8, 4, 4), 1208), ((32, 16, 4, 2), 1216)]
+
+
+@pytest.mark.parametrize("L,variant", TMA_CASES)
+@pytest.mark.parametrize("prec,recon", [(P.F64, 18), (P.F64, 12), (P.F32, 12)])
+def test_tma_kernel_bit_identical(cuda, monkeypatch, L, variant, prec, recon):
+    """The TMA-staged kernel (tile loads of whole rows into a shared-memory
+    ring, one producer warp) computes exactly what the gather kernel
+    computes: bit-identical outputs for the full lattice, for one parity with
+    the xpay and gamma5 epilogue, and no stage wait runs out."""
+    lat, g64, u = _device_setup(L, 43)
+    g = g64 if (prec, recon) == (P.F64, 18) else P.Gauge(lat, prec, recon)
+    if g is not g64:
+        g.copy_from(g64)
+    bs = lat.spinor_bytes(prec)
+    fe, fo, x = dev_bytes(bs), dev_bytes(bs), dev_bytes(bs)
+    lat.spinor_gaussian(fe, prec, 0, 7)
+    lat.spinor_gaussian(fo, prec, 1, 8)
+    lat.spinor_gaussian(x, prec, 1, 9)
+    flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
+    outs = {}
+    for v in ("2", str(variant)):
+        monkeypatch.setenv("PLQCD_DSLASH_STAGES", v)
+        monkeypatch.setenv("PLQCD_DSLASH_BLOCK", "64")
+        oe, oo, ox = dev_bytes(bs), dev_bytes(bs), dev_bytes(bs)
+        lat.dslash_full(g, oe, oo, fe, fo, prec)
+        lat.dslash_xpay(g, ox, fe, 1, prec, 0.25, x, -2.0, flags)
+        lat.synchronize()  # raises if a stage wait ran out
+        outs[v] = (oe, oo, ox)
+    for a, b in zip(outs["2"], outs[str(variant)]):
+        assert bool((a == b).all())
+
+
+def test_tma_kernel_matches_oracle(cuda, restatement):
+    """Full-lattice TMA kernel against the C restatement of the reference."""
+    L = (16, 8, 6, 4)
+    lat, g64, u = _device_setup(L, 44)
+    V = lat.V
+    q = O.gaussian_spinor(V, np.random.default_rng(5))
+    want = restatement.hop("full", L, q, u)
+    fe, fo = field_from_host(lat, q, 0, P.F64), field_from_host(lat, q, 1, P.F64)
+    bs = lat.spinor_bytes(P.F64)
+    oe, oo = dev_bytes(bs), dev_bytes(bs)
+    os.environ["PLQCD_DSLASH_STAGES"] = "1408"
+    try:
+        lat.dslash_full(g64, oe, oo, fe, fo, P.F64)
+        lat.synchronize()
+    finally:
+        os.environ.pop("PLQCD_DSLASH_STAGES", None)
+    got = field_to_host(lat, oe, P.F64, 0)
+    got[V // 2:] = field_to_host(lat, oo, P.F64, 1)[V // 2:]
+    assert relmax(got, want) < TOL64
+
+
+def test_tma_kernel_rejects_misfit_tiles(cuda, monkeypatch):
+    """A tile that does not divide the lattice (rows per tile not dividing L1,
+    or not a whole number of warps) is refused on the host with an argument
+    error; nothing is launched."""
+    lat, g64, u = _device_setup((6, 4, 6, 10), 45)
+    bs = lat.spinor_bytes(P.F64)
+    a, o = dev_bytes(bs), dev_bytes(bs)
+    for v in ("1408", "1203"):
+        monkeypatch.setenv("PLQCD_DSLASH_STAGES", v)
+        with pytest.raises(P.PlqcdError):
+            lat.dslash(g64, o, a, 0, P.F64)
