@@ -51,7 +51,7 @@ BYTES_HALF_12 = 52 + 8 * 24 + 52
 DRAM_BYTES_PER_SITE_FULL_F64 = 634.8e6 / (24 * 24 * 24 * 48)
 # the same for the TMA-staged kernel, from one capture per configuration on
 # 32^3x24 (profiles/dslash_tma_f64_full_32x32x32x24.txt): variant -> bytes/site
-DRAM_BYTES_PER_SITE_TMA_F64 = {1204: 865.05e6 / (32 * 32 * 32 * 24), 1408: 808.10e6 / (32 * 32 * 32 * 24)}
+DRAM_BYTES_PER_SITE_TMA_F64 = {1204: 859.31e6 / (32 * 32 * 32 * 24), 1408: 799.29e6 / (32 * 32 * 32 * 24)}
 
 
 def dram_bytes_per_site(cfg) -> float:
@@ -378,7 +378,9 @@ def run_ours(args, d: Dist):
     if args.only == "dslash":
         if d.rank == 0:
             print(json.dumps({"metric": "Dslash GFLOP/s", "value": round(value, 1), "unit": "GFLOP/s",
-                              "lattice": list(L), "only": "dslash", "per_parity_f64": parity, "f32": fp32}))
+                              "lattice": list(L), "only": "dslash", "kernel": kernel_name(head_cfg),
+                              "frac": round(achieved / hbm, 4), "clocks": clocks, "per_parity_f64": parity,
+                              "f32": fp32}))
         return 0
 
     # ---- e2e through the reference-facing C-ABI (host arrays) ---------------

@@ -384,7 +384,7 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
 
 static int env_int(const char *name, int dflt) {
     const char *e = getenv(name);
-    return e ? atoi(e) : dflt;
+    return (e && *e) ? atoi(e) : dflt;  // unset or empty: the default
 }
 
 static int dispatch(const Geom &g, cudaStream_t s, const DslashCall &c, const dev::DslashArgs &a, int variant,

@@ -347,11 +347,12 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
     dc.nrhs = nrhs;
     void *scratch = nullptr;
     // explicit configuration for experiments and tests: bypasses the tuner
-    if (const char *ev = getenv("PLQCD_MRHS_VARIANT")) {
+    const char *ev = getenv("PLQCD_MRHS_VARIANT");
+    if (ev && *ev) {
         const char *eb = getenv("PLQCD_MRHS_BLOCK");
         TuneResult t;
         t.variant = atoi(ev);
-        t.block = eb ? atoi(eb) : 128;
+        t.block = (eb && *eb) ? atoi(eb) : 128;
         if (t.variant >= 100 && t.variant < 1000) {
             DslashCall c2 = dc;
             return launch_dslash_config(g, s, c2, t.variant - 100, t.block);
