@@ -270,6 +270,17 @@ int plqcd_gauge_update(const su3 *u);
  * host<->device byte counts. */
 int plqcd_dropin_last_stats(double *kernel_ms, double *h2d_bytes, double *d2h_bytes);
 
+/* ---- host layout converters for the split entry points ------------------- */
+/* No reference counterpart: the reference leaves packing to its callers.
+ * API-layout arrays (interleaved complex doubles: spinors 12 per site,
+ * links 9 per link, in even/odd site order) <-> the split real / imaginary
+ * planes that the split family of include/dirac.h takes (re[k], im[k] =
+ * parts of complex number k). n = number of complex numbers. Host memory,
+ * multi-threaded for large n. Returns PLQCD_OK, or PLQCD_ERR_ARG for a null
+ * pointer or a negative n. */
+int plqcd_aos_to_split(const double *aos, double *re, double *im, long n);
+int plqcd_split_to_aos(const double *re, const double *im, double *aos, long n);
+
 #ifdef __cplusplus
 }
 #endif

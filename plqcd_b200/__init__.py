@@ -31,6 +31,7 @@ PREC_NAMES = {F64: "f64", F32: "f32", F16: "f16", BF16: "bf16"}
 SPINOR_BYTES_PER_SITE = {F64: 192, F32: 96, F16: 52, BF16: 52}
 
 OK = 0
+ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_TIMEOUT, ERR_NOCONV, ERR_NODEV = -1, -2, -3, -4, -5, -6, -7
 
 
 class PlqcdError(RuntimeError):
@@ -119,6 +120,8 @@ _SIGS = {
     "plqcd_selftest": (_i, [_i, _i]),
     "plqcd_gauge_update": (_i, [_vp]),
     "plqcd_dropin_last_stats": (_i, [_dp, _dp, _dp]),
+    "plqcd_aos_to_split": (_i, [_vp, _vp, _vp, ctypes.c_long]),
+    "plqcd_split_to_aos": (_i, [_vp, _vp, _vp, ctypes.c_long]),
 }
 
 _lib = None
@@ -195,19 +198,36 @@ def hopping_matrix(which: str, qin: np.ndarray, qout: np.ndarray, u: np.ndarray,
     return t
 
 
+def aos_to_split(a: np.ndarray):
+    """(re, im) planes of a complex128 API-layout array, by the library's
+    converter (plqcd_aos_to_split)."""
+    a = np.ascontiguousarray(a, np.complex128)
+    re, im = np.empty(a.shape, np.float64), np.empty(a.shape, np.float64)
+    check(lib().plqcd_aos_to_split(a.ctypes.data, re.ctypes.data, im.ctypes.data, a.size))
+    return re, im
+
+
+def split_to_aos(re: np.ndarray, im: np.ndarray, out: np.ndarray) -> np.ndarray:
+    """Merge split planes into the complex128 array `out` (plqcd_split_to_aos)."""
+    assert out.dtype == np.complex128 and out.flags.c_contiguous and re.size == im.size == out.size
+    re, im = np.ascontiguousarray(re, np.float64), np.ascontiguousarray(im, np.float64)
+    check(lib().plqcd_split_to_aos(re.ctypes.data, im.ctypes.data, out.ctypes.data, out.size))
+    return out
+
+
 def hopping_matrix_split(which: str, qin: np.ndarray, qout: np.ndarray, u: np.ndarray,
                          variant: str = "sse3_intrin_nohalfspinor") -> float:
     """The split real/imaginary entry points on the same arrays: the complex
     inputs are split into planes, the output planes are merged back into
     qout (only the output parity changes)."""
-    qre, qim = np.ascontiguousarray(qin.real), np.ascontiguousarray(qin.imag)
-    ure, uim = np.ascontiguousarray(u.real), np.ascontiguousarray(u.imag)
-    ore, oim = np.ascontiguousarray(qout.real), np.ascontiguousarray(qout.imag)
+    qre, qim = aos_to_split(qin)
+    ure, uim = aos_to_split(u)
+    ore, oim = aos_to_split(qout)
     f = getattr(lib(), f"plqcd_hopping_matrix_{which}_{variant}")
     t = f(ore.ctypes.data, oim.ctypes.data, ure.ctypes.data, uim.ctypes.data, qre.ctypes.data, qim.ctypes.data)
     if t < 0:
         raise PlqcdError(f"hopping matrix failed: {last_error()}")
-    qout[:] = ore + 1j * oim
+    split_to_aos(ore, oim, qout)
     return t
 
 

@@ -14,7 +14,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
+#include <thread>
 #include <unordered_map>
+#include <vector>
 
 #include "internal.h"
 #include "utils.h"
@@ -107,4 +109,50 @@ extern "C" double stop_watch(double t) {
     struct timeval tv;
     gettimeofday(&tv, nullptr);
     return (tv.tv_sec + tv.tv_usec * 1e-6) - t;
+}
+
+// ---- API layout <-> split real / imaginary planes ------------------------------
+// A memory-bound copy: n complex numbers, split across host threads in
+// contiguous ranges when n is large.
+namespace {
+
+template <class F>
+void parallel_ranges(long n, F f) {
+    const long per_thread = 1L << 20;
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = nt < 1 ? 1 : (nt > 16 ? 16 : nt);
+    if (n < 2 * per_thread || nt == 1) {
+        f(0L, n);
+        return;
+    }
+    long parts = n / per_thread;
+    if (parts > (long)nt) parts = nt;
+    std::vector<std::thread> pool;
+    for (long p = 1; p < parts; p++) pool.emplace_back(f, n * p / parts, n * (p + 1) / parts);
+    f(0L, n / parts);
+    for (auto &t : pool) t.join();
+}
+
+}  // namespace
+
+extern "C" int plqcd_aos_to_split(const double *aos, double *re, double *im, long n) {
+    if (!aos || !re || !im || n < 0) return plqcd::set_error(PLQCD_ERR_ARG, "plqcd_aos_to_split: bad argument");
+    parallel_ranges(n, [=](long a, long b) {
+        for (long k = a; k < b; k++) {
+            re[k] = aos[2 * k];
+            im[k] = aos[2 * k + 1];
+        }
+    });
+    return PLQCD_OK;
+}
+
+extern "C" int plqcd_split_to_aos(const double *re, const double *im, double *aos, long n) {
+    if (!aos || !re || !im || n < 0) return plqcd::set_error(PLQCD_ERR_ARG, "plqcd_split_to_aos: bad argument");
+    parallel_ranges(n, [=](long a, long b) {
+        for (long k = a; k < b; k++) {
+            aos[2 * k] = re[k];
+            aos[2 * k + 1] = im[k];
+        }
+    });
+    return PLQCD_OK;
 }

@@ -11,11 +11,15 @@ oracle/_ref/, on seeded inputs, and stores inputs and outputs:
                     commit; the inputs are regenerated from the seed)
   geom_4x6x8x10.npz the reference's ipt_eo/ipt_lex/iup/idn tables on a
                     lattice with four different extents
+  print_params_4x4x4x4.txt  the text the reference's print_params
+                    (lib/start.c:1346-1428) writes for a 4^4 lattice, one
+                    process, one thread, ALIGN 6
 
 The patched build fixes include/su3.h:135-138 and lib/dirac.c:643; the
 shipped build is the reference as distributed. Usage (needs oracle/_ref):
     python tests/golden/make_golden.py
 """
+import ctypes
 import os
 import sys
 
@@ -63,6 +67,16 @@ def main():
     ipt_eo, ipt_lex, iup, idn = P.tables(L)
     np.savez_compressed(os.path.join(HERE, "geom_4x6x8x10.npz"), L=np.array(L), ipt_eo=ipt_eo,
                         ipt_lex=ipt_lex, iup=iup, idn=idn)
+    L = (4, 4, 4, 4)
+    P.setup(L, 1)
+    libc = ctypes.CDLL(None)
+    libc.fopen.restype = ctypes.c_void_p
+    libc.fopen.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    libc.fclose.argtypes = [ctypes.c_void_p]
+    P.lib.print_params.argtypes = [ctypes.c_void_p]
+    fp = libc.fopen(os.path.join(HERE, "print_params_4x4x4x4.txt").encode(), b"w")
+    P.lib.print_params(fp)
+    libc.fclose(fp)
     print("golden fixtures written to", HERE)
 
 

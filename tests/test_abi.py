@@ -210,3 +210,67 @@ def test_device_api_without_gpu_reports_error():
         pass
     with pytest.raises(P.PlqcdError, match="no CUDA device"):
         P.Lattice((4, 4, 4, 4))
+
+
+@pytest.mark.parametrize("n", [0, 1, 12 * 257, 5_000_001])
+def test_split_converters_roundtrip(n):
+    """plqcd_aos_to_split / plqcd_split_to_aos: planes hold exactly the real
+    and imaginary parts, and merging restores the array bit for bit (the
+    largest case runs the multi-threaded path)."""
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    re, im = P.aos_to_split(a)
+    assert np.array_equal(re, a.real) and np.array_equal(im, a.imag)
+    b = np.zeros_like(a)
+    P.split_to_aos(re, im, b)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_split_converters_reject_null():
+    assert P.lib().plqcd_aos_to_split(None, None, None, 4) == P.ERR_ARG
+    assert "bad argument" in P.last_error()
+    x = np.zeros(4)
+    assert P.lib().plqcd_split_to_aos(x.ctypes.data, x.ctypes.data, x.ctypes.data, -1) == P.ERR_ARG
+
+
+def test_packed_field_types_known_answers(tmp_path):
+    """include/su3_256.h and su3_512.h (the reference's two- and four-lane
+    packed types, include/su3_256.h:14-191, su3_512.h:12-216): a C program
+    compiled against the headers checks every lane of every element after
+    packing and that unpacking restores the objects; the headers also
+    compile as C++."""
+    exe = tmp_path / "packed_types"
+    src = os.path.join(ROOT, "tests", "c", "packed_types.c")
+    r = subprocess.run(["gcc", "-std=c11", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), src,
+                        "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout
+    cxx = tmp_path / "t.cpp"
+    cxx.write_text('#include "su3_256.h"\n#include "su3_512.h"\nint main() { return 0; }\n')
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(cxx)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_print_params_matches_reference_golden(tmp_path):
+    """print_params writes byte for byte what the reference's print_params
+    (lib/start.c:1346-1428) wrote for the same 4^4 single-process setup
+    (fixture from tests/golden/make_golden.py)."""
+    P.finalize_plqcd()
+    path = O.write_input_file((4, 4, 4, 4), nthreads=1, align=6)
+    try:
+        assert P.init_plqcd(path) == 0, P.last_error()
+        libc = ctypes.CDLL(None)
+        libc.fopen.restype = ctypes.c_void_p
+        libc.fopen.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        libc.fclose.argtypes = [ctypes.c_void_p]
+        out = tmp_path / "params.txt"
+        fp = libc.fopen(str(out).encode(), b"w")
+        P.lib().print_params(fp)
+        libc.fclose(fp)
+    finally:
+        os.unlink(path)
+        P.finalize_plqcd()
+    want = open(os.path.join(GOLD, "print_params_4x4x4x4.txt"), "rb").read()
+    assert out.read_bytes() == want
