@@ -160,6 +160,15 @@ int plqcd_dslash(plqcd_lattice *lat, const plqcd_gauge *g, void *out, const void
                  int prec, unsigned flags);
 int plqcd_dslash_xpay(plqcd_lattice *lat, const plqcd_gauge *g, void *out, const void *in,
                       int out_parity, int prec, unsigned flags, double a, const void *x, double b);
+/* The same on the output half-sites [h_begin, h_begin + h_count) only (a
+ * t-slab range when it is whole slabs); other sites of out are not written.
+ * For a lattice held in t-slabs by several devices: the local lattice
+ * carries one ghost t-slice on each side, filled from the neighbouring
+ * slabs, and the interior slices are computed with this call. x may be
+ * NULL. No reference counterpart (the reference computes its MPI faces
+ * inside the hop, lib/dirac.c:124-131, 203-228). */
+int plqcd_dslash_sites(plqcd_lattice *lat, const plqcd_gauge *g, void *out, const void *in, int out_parity,
+                       int prec, unsigned flags, double a, const void *x, double b, long h_begin, long h_count);
 /* Full-lattice H in one launch: out_e = H_eo in_o and out_o = H_oe in_e.
  * Each link is used by two sites of the same launch and read from HBM
  * once. */

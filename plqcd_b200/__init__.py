@@ -109,6 +109,8 @@ _SIGS = {
     "plqcd_dslash": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint]),
     "plqcd_dslash_xpay": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint, _d, _vp, _d]),
     "plqcd_dslash_full": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i]),
+    "plqcd_dslash_sites": (_i, [_vp, _vp, _vp, _vp, _i, _i, ctypes.c_uint, ctypes.c_double, _vp, ctypes.c_double,
+                               ctypes.c_long, ctypes.c_long]),
     "plqcd_dslash_mrhs": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, ctypes.c_uint]),
     "plqcd_dslash_mrhs_xpay": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, ctypes.c_uint, _d, _vp, _d]),
     "plqcd_tune_enable": (_i, [_i]),
@@ -310,6 +312,12 @@ class Lattice:
                          b: float, flags: int = 0):
         check(lib().plqcd_dslash_mrhs_xpay(self.handle, gauge.handle, _ptr(out), _ptr(inp), nrhs, out_parity, prec,
                                            flags, a, _ptr(x), b))
+
+    def dslash_sites(self, gauge: "Gauge", out, inp, out_parity: int, prec: int, h_begin: int, h_count: int,
+                     flags: int = 0, a: float = 1.0, x=None, b: float = 0.0):
+        """out[h] = a H in (+ b x) on output half-sites [h_begin, h_begin + h_count)."""
+        check(lib().plqcd_dslash_sites(self.handle, gauge.handle, _ptr(out), _ptr(inp), out_parity, prec, flags,
+                                       a, _ptr(x) if x is not None else None, b, h_begin, h_count))
 
     def dslash_full(self, gauge: "Gauge", out_even, out_odd, in_even, in_odd, prec: int):
         check(lib().plqcd_dslash_full(self.handle, gauge.handle, _ptr(out_even), _ptr(out_odd), _ptr(in_even),

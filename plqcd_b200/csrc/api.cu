@@ -304,6 +304,29 @@ extern "C" int plqcd_dslash_xpay(plqcd_lattice *lat, const plqcd_gauge *g, void 
     return launch_dslash(lat->geom, lat->stream, c);
 }
 
+extern "C" int plqcd_dslash_sites(plqcd_lattice *lat, const plqcd_gauge *g, void *out, const void *in,
+                                  int out_parity, int prec, unsigned flags, double a, const void *x, double b,
+                                  long h_begin, long h_count) {
+    clear_error();
+    DslashCall c;
+    PLQCD_TRY(dslash_common(lat, g, prec, c));
+    if (!out || !in || (out_parity != 0 && out_parity != 1) || h_count < 0)
+        return set_error(PLQCD_ERR_ARG, "dslash_sites: bad argument");
+    if ((flags & PLQCD_DSLASH_COMPAT) && x) return set_error(PLQCD_ERR_ARG, "dslash_sites: compat mode without xpay");
+    if (h_count == 0) return PLQCD_OK;
+    c.out = out;
+    c.in = in;
+    c.out_parity = out_parity;
+    c.flags = flags;
+    c.a_up = a;
+    c.a_low = a;
+    c.x = x;
+    c.b = b;
+    c.h_begin = h_begin;
+    c.h_count = h_count;
+    return launch_dslash(lat->geom, lat->stream, c);
+}
+
 extern "C" int plqcd_dslash_full(plqcd_lattice *lat, const plqcd_gauge *g, void *out_even, void *out_odd,
                                  const void *in_even, const void *in_odd, int prec) {
     clear_error();

@@ -1,0 +1,402 @@
+"""A lattice held in t-slabs by several devices: ghost-slice exchange, the
+hopping matrix and the even/odd CG on top of it.
+
+The reference decomposes the lattice over an MPI process grid and exchanges
+half-spinor faces inside every hop (lib/dirac.c:124-131, 203-228; face
+tables nn_bnde/nn_bndo, include/plqcd_global_params.h:119-132). Here the
+lattice is cut along t only, one slab per rank (one process per GPU):
+
+* rank r of N holds global t in [r*Lt, (r+1)*Lt), Lt = L3 / N, even;
+* its local lattice is (L0, L1, L2, Lt + 2): local slice t' = 0 and
+  t' = Lt + 1 are ghosts holding global slices r*Lt - 1 and (r+1)*Lt
+  (periodic), the interior is t' = 1 .. Lt;
+* local half-site h = xh + L0/2 (y + L1 (z + L2 t')); since t' = t - r*Lt + 1
+  and r*Lt is even, a site's local parity is its global parity plus one, so
+  the field of global parity p is stored as the local field of parity 1 - p;
+* one hop: the input field's first and last interior slices go to the ranks
+  below and above (every SoA plane of a field keeps a t-slice contiguous, so
+  this is one send per plane and neighbour, no packing), the interior slices
+  that do not touch a ghost are computed meanwhile, then the two boundary
+  slices; the kernels are the single-device ones, run on site ranges
+  (plqcd_dslash_sites), with the periodic wrap never reached in t;
+* links: the backward t-link of slice t' = 1 sits in ghost slice 0, filled
+  once per gauge field from the rank below.
+
+Transports move the ghost slices: DistTransport (torch.distributed
+point-to-point, NCCL between GPUs, gloo on the host) and LocalTransport (all
+slabs in one process on one device, for tests and single-GPU runs).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import BF16, F16, F32, F64, Gauge, Lattice, PlqcdError
+
+# bytes of one site in each SoA plane of a one-parity spinor field
+SPINOR_PLANES = {F64: [16] * 12, F32: [16] * 6, F16: [16, 16, 16, 4], BF16: [16, 16, 16, 4]}
+# (elements per link, bytes per element) of the gauge formats; a field is
+# planes[2 parities][4 mu][elements][Vh]
+GAUGE_PLANES = {(F64, 18): (9, 16), (F64, 12): (6, 16), (F32, 18): (9, 8), (F32, 12): (3, 16), (F16, 12): (3, 8),
+                (BF16, 12): (3, 8)}
+
+
+class SlabGeometry:
+    """Index arithmetic of one rank's slab (no device objects)."""
+
+    def __init__(self, L, rank: int, nranks: int):
+        L = tuple(int(v) for v in L)
+        if nranks < 1 or L[3] % nranks or (L[3] // nranks) % 2 or L[3] // nranks < 2:
+            raise PlqcdError(f"t extent {L[3]} does not split into {nranks} even slabs of >= 2 slices")
+        if any(v < 2 or v % 2 for v in L):
+            raise PlqcdError(f"lattice extents must be even and >= 2: {L}")
+        self.L, self.rank, self.nranks = L, rank, nranks
+        self.Lt = L[3] // nranks
+        self.t0 = rank * self.Lt                      # first global t of the slab
+        self.local_dims = (L[0], L[1], L[2], self.Lt + 2)
+        self.L0h = L[0] // 2
+        self.S = self.L0h * L[1] * L[2]               # half-sites of one t-slice
+        self.Vh = self.S * (self.Lt + 2)              # local half volume, ghosts included
+        self.below = (rank - 1) % nranks
+        self.above = (rank + 1) % nranks
+
+    @staticmethod
+    def local_parity(global_parity: int) -> int:
+        return global_parity ^ 1
+
+    def interior(self):
+        """(h_begin, h_count) of the interior slices."""
+        return self.S, self.S * self.Lt
+
+    def slice_range(self, tl: int):
+        return tl * self.S, self.S
+
+    def plane_slices(self, plane_bytes, nsites: int, tl: int):
+        """Byte ranges (offset, length) of local slice tl in every plane of a
+        field whose planes hold nsites sites of plane_bytes[k] bytes each."""
+        out, off = [], 0
+        for eb in plane_bytes:
+            out.append((off + tl * self.S * eb, self.S * eb))
+            off += nsites * eb
+        return out
+
+    def spinor_slices(self, prec: int, tl: int):
+        return self.plane_slices(SPINOR_PLANES[prec], self.Vh, tl)
+
+    def gauge_slices(self, prec: int, recon: int, tl: int):
+        ne, eb = GAUGE_PLANES[(prec, recon)]
+        return self.plane_slices([eb] * (8 * ne), self.Vh, tl)
+
+    # ---- API-layout (host) mapping between global and local arrays --------
+    def local_to_global_sites(self):
+        """For every local even/odd site index (API layout: parity-major),
+        the global even/odd index of the site it holds."""
+        L0, L1, L2, L3 = self.L
+        Lt2 = self.Lt + 2
+        Vl = 2 * self.Vh
+        idx = np.arange(Vl)
+        p_loc, h = idx // self.Vh, idx % self.Vh
+        xh = h % self.L0h
+        row = h // self.L0h
+        y = row % L1
+        z = (row // L1) % L2
+        tl = row // (L1 * L2)
+        assert tl.max() < Lt2
+        x = 2 * xh + ((y + z + tl + p_loc) & 1)
+        t = (self.t0 + tl - 1) % L3
+        p_g = (x + y + z + t) & 1
+        Vh_g = L0 * L1 * L2 * L3 // 2
+        return p_g * Vh_g + x // 2 + self.L0h * (y + L1 * (z + L2 * t))
+
+    def local_links_from_global(self, u_global: np.ndarray, ghosts: bool = True) -> np.ndarray:
+        """Local API-layout link array (4 V_local, 9) from the global one;
+        ghost slices zero unless `ghosts`."""
+        g = self.local_to_global_sites()
+        u = u_global.reshape(-1, 4, 9)[g].copy()
+        if not ghosts:
+            u[self.ghost_mask()] = 0
+        return u.reshape(-1, 9)
+
+    def local_spinor_from_global(self, q_global: np.ndarray, ghosts: bool = True) -> np.ndarray:
+        q = q_global[self.local_to_global_sites()].copy()
+        if not ghosts:
+            q[self.ghost_mask()] = 0
+        return q
+
+    def ghost_mask(self) -> np.ndarray:
+        """True for local API-layout sites in a ghost slice."""
+        h = np.arange(2 * self.Vh) % self.Vh
+        tl = h // self.S
+        return (tl == 0) | (tl == self.Lt + 1)
+
+
+class LocalTransport:
+    """All slabs in one process (one device): ghost slices are copied."""
+
+    def __init__(self, nranks: int):
+        self.nranks = nranks
+        self.pending = {}
+
+    def exchange(self, geos, fields, slices_fn, lower: bool = True, upper: bool = True):
+        """fields[r]: torch uint8 tensor of rank r's field. slices_fn(geo, tl)
+        gives its plane byte ranges of local slice tl."""
+        for r, geo in enumerate(geos):
+            last, first = geo.Lt, 1
+            if lower:  # my last interior slice -> ghost 0 of the rank above
+                dst = fields[geo.above]
+                for (so, n), (do, _) in zip(slices_fn(geo, last), slices_fn(geos[geo.above], 0)):
+                    dst[do:do + n].copy_(fields[r][so:so + n])
+            if upper:  # my first interior slice -> ghost Lt+1 of the rank below
+                dst = fields[geo.below]
+                for (so, n), (do, _) in zip(slices_fn(geo, first), slices_fn(geos[geo.below], geo.Lt + 1)):
+                    dst[do:do + n].copy_(fields[r][so:so + n])
+
+
+class DistTransport:
+    """One slab per process: ghost slices travel by torch.distributed
+    point-to-point operations (NCCL between GPUs, gloo on the host), all of
+    one exchange in one batch."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+
+    def start(self, geo: SlabGeometry, field, slices_fn, lower: bool = True, upper: bool = True):
+        """Post the sends and receives of one exchange; returns the work
+        handles (wait on them before reading the ghosts)."""
+        dist = self.dist
+        if geo.nranks == 1:
+            LocalTransport(1).exchange([geo], [field], slices_fn, lower, upper)
+            return []
+        ops = []
+        grank = lambda r: dist.get_global_rank(self.group, r) if self.group is not None else r
+        if lower:
+            for (so, n) in slices_fn(geo, geo.Lt):
+                ops.append(dist.P2POp(dist.isend, field[so:so + n], grank(geo.above), self.group))
+            for (do, n) in slices_fn(geo, 0):
+                ops.append(dist.P2POp(dist.irecv, field[do:do + n], grank(geo.below), self.group))
+        if upper:
+            for (so, n) in slices_fn(geo, 1):
+                ops.append(dist.P2POp(dist.isend, field[so:so + n], grank(geo.below), self.group))
+            for (do, n) in slices_fn(geo, geo.Lt + 1):
+                ops.append(dist.P2POp(dist.irecv, field[do:do + n], grank(geo.above), self.group))
+        return dist.batch_isend_irecv(ops) if ops else []
+
+    @staticmethod
+    def wait(works):
+        for w in works:
+            w.wait()
+
+
+class ShardedLattice:
+    """One rank's slab on its device: a local Lattice of (L0, L1, L2, Lt+2)
+    plus the geometry. Fields are torch uint8 device tensors of
+    lat.spinor_bytes(prec) bytes in the local parity (global parity ^ 1)."""
+
+    def __init__(self, L, rank: int, nranks: int, device: int = 0, stream: int | None = None):
+        self.geo = SlabGeometry(L, rank, nranks)
+        self.lat = Lattice(self.geo.local_dims, device, stream)
+
+    def field(self, prec: int):
+        import torch
+        return torch.zeros(self.lat.spinor_bytes(prec), dtype=torch.uint8, device=f"cuda:{self.lat.device}")
+
+    def import_global(self, q_global: np.ndarray, global_parity: int, prec: int = F64, ghosts: bool = False):
+        """Device field of one global parity from a global API-layout array."""
+        import torch
+        q = self.geo.local_spinor_from_global(q_global, ghosts)
+        aos = torch.from_numpy(q).to(f"cuda:{self.lat.device}")
+        f = self.field(prec)
+        self.lat.spinor_import(aos, self.geo.local_parity(global_parity), f, prec)
+        return f
+
+    def export_interior(self, f, global_parity: int, prec: int = F64) -> tuple[np.ndarray, np.ndarray]:
+        """(global even/odd indices, API-layout values) of the interior sites
+        of a field of one global parity."""
+        import torch
+        aos = torch.zeros((2 * self.geo.Vh, 12), dtype=torch.complex128, device=f"cuda:{self.lat.device}")
+        p = self.geo.local_parity(global_parity)
+        self.lat.spinor_export(f, prec, p, aos)
+        self.lat.synchronize()
+        h0, n = self.geo.interior()
+        loc = p * self.geo.Vh + np.arange(h0, h0 + n)
+        return self.geo.local_to_global_sites()[loc], aos.cpu().numpy()[loc]
+
+    def gauge_from_global(self, u_global: np.ndarray, prec: int = F64, recon: int = 18) -> Gauge:
+        """Local gauge field (ghost slices zero: fill them with
+        exchange_gauge) from the global API-layout link array."""
+        u = self.geo.local_links_from_global(u_global, ghosts=False)
+        g64 = Gauge(self.lat, F64, 18)
+        g64.load_host(np.ascontiguousarray(u))
+        if (prec, recon) == (F64, 18):
+            return g64
+        g = Gauge(self.lat, prec, recon)
+        g.copy_from(g64)
+        return g
+
+
+def _wrap(ptr: int, nbytes: int, device: int):
+    """uint8 torch tensor over device memory the library owns."""
+    import torch
+
+    class _Arr:
+        pass
+    a = _Arr()
+    a.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False), "version": 3}
+    return torch.as_tensor(a, device=f"cuda:{device}")
+
+
+def exchange_gauge(shards, gauges, transport):
+    """Fill ghost slice 0 of every shard's gauge field (the backward t-link
+    of the first interior slice) from the rank below."""
+    views = [_wrap(g.data, g.lat.gauge_bytes(g.prec, g.recon), g.lat.device) for g in gauges]
+    fn = lambda geo, tl: geo.gauge_slices(gauges[0].prec, gauges[0].recon, tl)
+    if isinstance(transport, LocalTransport):
+        transport.exchange([s.geo for s in shards], views, fn, lower=True, upper=False)
+    else:
+        transport.wait(transport.start(shards[0].geo, views[0], fn, lower=True, upper=False))
+
+
+def dslash(shards, gauges, outs, ins, out_parity: int, prec: int, transport, flags: int = 0, a: float = 1.0,
+           xs=None, b: float = 0.0):
+    """out = a H in (+ b x) on every shard's interior, out_parity global.
+    shards/gauges/outs/ins/xs: one entry per slab this process holds (all N
+    with LocalTransport, one with DistTransport)."""
+    p = SlabGeometry.local_parity(out_parity)
+    fn = lambda geo, tl: geo.spinor_slices(prec, tl)
+    xs = xs if xs is not None else [None] * len(shards)
+    if isinstance(transport, LocalTransport):
+        transport.exchange([s.geo for s in shards], ins, fn)
+        for s, g, o, i, x in zip(shards, gauges, outs, ins, xs):
+            h0, n = s.geo.interior()
+            s.lat.dslash_sites(g, o, i, p, prec, h0, n, flags, a, x, b)
+        return
+    (s,), (g,), (o,), (i,), (x,) = shards, gauges, outs, ins, xs
+    geo = s.geo
+    works = transport.start(geo, i, fn)
+    # slices 2 .. Lt-1 need no ghost: computed while the exchange runs
+    if geo.Lt > 2:
+        s.lat.dslash_sites(g, o, i, p, prec, 2 * geo.S, (geo.Lt - 2) * geo.S, flags, a, x, b)
+    transport.wait(works)
+    for tl in (1, geo.Lt):
+        h0, n = geo.slice_range(tl)
+        s.lat.dslash_sites(g, o, i, p, prec, h0, n, flags, a, x, b)
+
+
+# ---------------------------------------------------------------------------
+# even/odd CG over the slabs (FP64)
+# ---------------------------------------------------------------------------
+
+def _interior_f64(geo: SlabGeometry, f):
+    """float64 view of a field's interior sites: (12 planes, sites, re/im)."""
+    v = f.view(__import__("torch").float64).view(12, geo.Vh, 2)
+    h0, n = geo.interior()
+    return v[:, h0:h0 + n, :]
+
+
+class _Slabs:
+    """The fields of one logical spinor over the slabs this process holds,
+    with reductions summed over all slabs (all ranks)."""
+
+    def __init__(self, shards, transport):
+        self.shards, self.transport = shards, transport
+
+    def new(self):
+        return [s.field(F64) for s in self.shards]
+
+    def norm2(self, fs) -> float:
+        return self.allsum(sum(float((_interior_f64(s.geo, f) ** 2).sum()) for s, f in zip(self.shards, fs)))
+
+    def allsum(self, v: float) -> float:
+        if isinstance(self.transport, LocalTransport):
+            return v
+        import torch
+        dist = self.transport.dist
+        dev = f"cuda:{self.shards[0].lat.device}" if dist.get_backend(self.transport.group) == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, group=self.transport.group)
+        return float(t.item())
+
+    @staticmethod
+    def axpy(a, xs, ys):          # y += a x
+        for x, y in zip(xs, ys):
+            y.view(__import__("torch").float64).add_(x.view(__import__("torch").float64), alpha=a)
+
+    @staticmethod
+    def xpay(xs, b, ys):          # y = x + b y
+        torch = __import__("torch")
+        for x, y in zip(xs, ys):
+            yv = y.view(torch.float64)
+            yv.mul_(b).add_(x.view(torch.float64))
+
+    @staticmethod
+    def copy(src, dst):
+        for s, d in zip(src, dst):
+            d.copy_(s)
+
+
+def cg_solve(shards, g64s, b_even, b_odd, kappa: float, transport, tol: float = 1e-10, max_iter: int = 10000):
+    """Solve D x = b, D = 1 - kappa H, on the slabs: even/odd CG on
+    Mhat^dag Mhat with Mhat = 1 - kappa^2 H_eo H_oe (gamma5-hermitian, so
+    Mhat^dag = g5 Mhat g5, folded into the hopping kernels), convergence on
+    the FP64 Schur residual |b' - Mhat x_e| / |b'| <= tol, then
+    x_o = b_o + kappa H_oe x_e; the same algorithm as plqcd_invert_cg in
+    FP64. b_even/b_odd: lists of per-slab fields of global parity 0 / 1.
+    Returns (x_even, x_odd, iterations, schur_residual). The hops are the
+    library's kernels with one ghost exchange each; the vector updates and
+    interior dot products run as torch operations, the dot products summed
+    over the ranks with one all-reduce each."""
+    from . import DSLASH_G5_IN, DSLASH_G5_OUT, EVEN, ODD
+    S = _Slabs(shards, transport)
+
+    def hop(outs, ins, parity, flags=0, a=1.0, xs=None, b=0.0):
+        dslash(shards, g64s, outs, ins, parity, F64, transport, flags, a, xs, b)
+
+    tmp_o = S.new()
+
+    def mhat(outs, ins, dagger):
+        fin = DSLASH_G5_IN if dagger else 0
+        fout = DSLASH_G5_OUT if dagger else 0
+        hop(tmp_o, ins, ODD, fin)
+        hop(outs, tmp_o, EVEN, fout, -kappa * kappa, ins, 1.0)
+
+    bprime, rhs = S.new(), S.new()
+    hop(bprime, b_odd, EVEN, 0, kappa, b_even, 1.0)
+    bp2 = S.norm2(bprime)
+    x_e, x_o = S.new(), S.new()
+    if not bp2 > 0:
+        hop(x_o, x_e, ODD, 0, kappa, b_odd, 1.0)
+        return x_e, x_o, 0, 0.0
+    mhat(rhs, bprime, True)
+    r, p, t, Ap, r64 = S.new(), S.new(), S.new(), S.new(), S.new()
+    S.copy(rhs, r)
+    S.copy(rhs, p)
+    rr = S.norm2(r)
+    target = tol * tol * rr
+    sr2 = bp2
+    it = 0
+    for it in range(1, max_iter + 1):
+        mhat(t, p, False)
+        pap = S.norm2(t)
+        mhat(Ap, t, True)
+        alpha = rr / pap
+        S.axpy(alpha, p, x_e)
+        S.axpy(-alpha, Ap, r)
+        rr_new = S.norm2(r)
+        if rr_new <= target:
+            # FP64 Schur residual decides convergence
+            mhat(t, x_e, False)
+            for a_, b_, c_ in zip(bprime, t, r64):
+                c_.copy_(a_)
+                c_.view(__import__("torch").float64).sub_(b_.view(__import__("torch").float64))
+            sr2 = S.norm2(r64)
+            if sr2 <= tol * tol * bp2:
+                break
+            mhat(r, r64, True)
+            rr_new = S.norm2(r)
+            if rr_new <= target:
+                target *= 0.25
+        S.xpay(r, rr_new / rr, p)
+        rr = rr_new
+    hop(x_o, x_e, ODD, 0, kappa, b_odd, 1.0)
+    return x_e, x_o, it, (sr2 / bp2) ** 0.5

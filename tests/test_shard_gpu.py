@@ -1,0 +1,117 @@
+"""t-slab decomposition on the GPU (plqcd_b200/shard.py): N slabs held in
+one process on one device (LocalTransport copies the ghost slices), so the
+kernels, the ghost slices and the site ranges of the multi-GPU hop run here;
+the transport between processes is covered by tests/test_shard_cpu.py.
+
+The sharded hop runs the single-device kernels on the same data, so its
+output is bit-identical to the unsharded hop; the sharded CG matches
+plqcd_invert_cg."""
+import numpy as np
+import pytest
+
+import plqcd_b200 as P
+from plqcd_b200 import shard as SH
+from oracle import oracle as O
+from tests.gpu_util import dev_bytes, field_from_host, field_to_host, new_lattice, relmax
+
+pytestmark = pytest.mark.gpu
+
+
+def _global(L, seed):
+    lat = new_lattice(L)
+    g64 = P.Gauge(lat, P.F64, 18)
+    g64.random(seed)
+    u = g64.store_host()
+    q = O.gaussian_spinor(lat.V, np.random.default_rng(seed))
+    return lat, g64, u, q
+
+
+def _shards(L, N, u, prec, recon):
+    import torch
+    stream = torch.cuda.current_stream().cuda_stream
+    shards = [SH.ShardedLattice(L, r, N, 0, stream) for r in range(N)]
+    gauges = [s.gauge_from_global(u, prec, recon) for s in shards]
+    SH.exchange_gauge(shards, gauges, SH.LocalTransport(N))
+    return shards, gauges
+
+
+def _gather(shards, fields, parity, prec, V):
+    out = np.full((V, 12), np.nan + 0j)
+    for s, f in zip(shards, fields):
+        idx, vals = s.export_interior(f, parity, prec)
+        out[idx] = vals
+    return out
+
+
+@pytest.mark.parametrize("N", [1, 2, 4])
+@pytest.mark.parametrize("prec,recon", [(P.F64, 18), (P.F32, 12), (P.F16, 12)])
+def test_sharded_hop_is_bit_identical(cuda, N, prec, recon):
+    L = (8, 8, 4, 16)
+    lat, g64, u, q = _global(L, 31)
+    g = g64 if (prec, recon) == (P.F64, 18) else P.Gauge(lat, prec, recon)
+    if g is not g64:
+        g.copy_from(g64)
+    shards, gauges = _shards(L, N, u, prec, recon)
+    T = SH.LocalTransport(N)
+    flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
+    for p in (P.EVEN, P.ODD):
+        # single device: out = 0.25 g5 H g5-in + (-2) x
+        fin = field_from_host(lat, q, 1 - p, prec)
+        fx = field_from_host(lat, np.conj(q), p, prec)
+        fo = dev_bytes(lat.spinor_bytes(prec))
+        lat.dslash(g, fo, fin, p, prec)
+        fox = dev_bytes(lat.spinor_bytes(prec))
+        lat.dslash_xpay(g, fox, fin, p, prec, 0.25, fx, -2.0, flags)
+        want = field_to_host(lat, fo, prec, p)[p * lat.Vh:(p + 1) * lat.Vh]
+        wantx = field_to_host(lat, fox, prec, p)[p * lat.Vh:(p + 1) * lat.Vh]
+        ins = [s.import_global(q, 1 - p, prec) for s in shards]
+        xs = [s.import_global(np.conj(q), p, prec) for s in shards]
+        outs = [s.field(prec) for s in shards]
+        outx = [s.field(prec) for s in shards]
+        SH.dslash(shards, gauges, outs, ins, p, prec, T)
+        SH.dslash(shards, gauges, outx, ins, p, prec, T, flags, 0.25, xs, -2.0)
+        got = _gather(shards, outs, p, prec, lat.V)[p * lat.Vh:(p + 1) * lat.Vh]
+        gotx = _gather(shards, outx, p, prec, lat.V)[p * lat.Vh:(p + 1) * lat.Vh]
+        assert not np.isnan(got).any()
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+        assert np.array_equal(gotx.view(np.uint64), wantx.view(np.uint64))
+
+
+def test_sharded_hop_matches_oracle(cuda, restatement):
+    L = (4, 4, 4, 12)
+    lat, g64, u, q = _global(L, 32)
+    want = restatement.hop("full", L, q, u)
+    shards, gauges = _shards(L, 3, u, P.F64, 18)
+    T = SH.LocalTransport(3)
+    got = np.full_like(q, np.nan)
+    for p in (P.EVEN, P.ODD):
+        ins = [s.import_global(q, 1 - p) for s in shards]
+        outs = [s.field(P.F64) for s in shards]
+        SH.dslash(shards, gauges, outs, ins, p, P.F64, T)
+        part = _gather(shards, outs, p, P.F64, lat.V)
+        got[p * lat.Vh:(p + 1) * lat.Vh] = part[p * lat.Vh:(p + 1) * lat.Vh]
+    assert relmax(got, want) < 1e-14
+
+
+@pytest.mark.parametrize("N", [2, 4])
+def test_sharded_cg_matches_single_device_cg(cuda, N):
+    L = (8, 8, 4, 16)
+    kappa, tol = 0.12, 1e-10
+    lat, g64, u, q = _global(L, 33)
+    bs = lat.spinor_bytes(P.F64)
+    be, bo = field_from_host(lat, q, 0, P.F64), field_from_host(lat, q, 1, P.F64)
+    xe, xo = dev_bytes(bs), dev_bytes(bs)
+    info = P.invert_cg(lat, g64, None, xe, xo, be, bo, P.cg_param(kappa=kappa, tol=tol))
+    want = field_to_host(lat, xe, P.F64, 0)
+    want[lat.Vh:] = field_to_host(lat, xo, P.F64, 1)[lat.Vh:]
+
+    shards, gauges = _shards(L, N, u, P.F64, 18)
+    T = SH.LocalTransport(N)
+    b_e = [s.import_global(q, 0) for s in shards]
+    b_o = [s.import_global(q, 1) for s in shards]
+    x_e, x_o, iters, res = SH.cg_solve(shards, gauges, b_e, b_o, kappa, T, tol)
+    got = _gather(shards, x_e, 0, P.F64, lat.V)
+    got[lat.Vh:] = _gather(shards, x_o, 1, P.F64, lat.V)[lat.Vh:]
+    assert res <= tol
+    assert abs(iters - info.iterations) <= 2, (iters, info.iterations)
+    assert relmax(got, want) < 1e-8
