@@ -134,7 +134,6 @@ class LocalTransport:
 
     def __init__(self, nranks: int):
         self.nranks = nranks
-        self.pending = {}
 
     def exchange(self, geos, fields, slices_fn, lower: bool = True, upper: bool = True):
         """fields[r]: torch uint8 tensor of rank r's field. slices_fn(geo, tl)
@@ -287,9 +286,15 @@ def dslash(shards, gauges, outs, ins, out_parity: int, prec: int, transport, fla
 # even/odd CG over the slabs (FP64)
 # ---------------------------------------------------------------------------
 
+def _f64(f):
+    """float64 view of a uint8 device field."""
+    import torch
+    return f.view(torch.float64)
+
+
 def _interior_f64(geo: SlabGeometry, f):
     """float64 view of a field's interior sites: (12 planes, sites, re/im)."""
-    v = f.view(__import__("torch").float64).view(12, geo.Vh, 2)
+    v = _f64(f).view(12, geo.Vh, 2)
     h0, n = geo.interior()
     return v[:, h0:h0 + n, :]
 
@@ -320,14 +325,17 @@ class _Slabs:
     @staticmethod
     def axpy(a, xs, ys):          # y += a x
         for x, y in zip(xs, ys):
-            y.view(__import__("torch").float64).add_(x.view(__import__("torch").float64), alpha=a)
+            _f64(y).add_(_f64(x), alpha=a)
 
     @staticmethod
     def xpay(xs, b, ys):          # y = x + b y
-        torch = __import__("torch")
         for x, y in zip(xs, ys):
-            yv = y.view(torch.float64)
-            yv.mul_(b).add_(x.view(torch.float64))
+            _f64(y).mul_(b).add_(_f64(x))
+
+    @staticmethod
+    def sub(xs, ys, zs):          # z = x - y
+        for x, y, z in zip(xs, ys, zs):
+            _f64(z).copy_(_f64(x)).sub_(_f64(y))
 
     @staticmethod
     def copy(src, dst):
@@ -386,9 +394,7 @@ def cg_solve(shards, g64s, b_even, b_odd, kappa: float, transport, tol: float = 
         if rr_new <= target:
             # FP64 Schur residual decides convergence
             mhat(t, x_e, False)
-            for a_, b_, c_ in zip(bprime, t, r64):
-                c_.copy_(a_)
-                c_.view(__import__("torch").float64).sub_(b_.view(__import__("torch").float64))
+            S.sub(bprime, t, r64)
             sr2 = S.norm2(r64)
             if sr2 <= tol * tol * bp2:
                 break
