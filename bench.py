@@ -45,22 +45,22 @@ BYTES_PARITY = {0: 192 + 8 * 144 + 192, 1: 96 + 8 * 72 + 96}        # F64 / F32,
 BYTES_FULL = {0: 192 + 4 * 144 + 192, 1: 96 + 4 * 72 + 96}          # full lattice: each link read once
 BYTES_F32_12 = 96 + 8 * 48 + 96
 BYTES_HALF_12 = 52 + 8 * 24 + 52
-# DRAM bytes (read + write) per site of the full-lattice F64 kernel from one ncu
-# capture on 24^3x48 (profiles/dslash_f64_full_and_eo_24x24x24x48.txt); traffic
-# grows with the sites processed, so a launch moves this times V bytes.
-DRAM_BYTES_PER_SITE_FULL_F64 = 634.8e6 / (24 * 24 * 24 * 48)
-# the same for the TMA-staged kernel, from one capture per configuration on
-# 32^3x24 (profiles/dslash_tma_f64_full_32x32x32x24.txt): variant -> bytes/site
-DRAM_BYTES_PER_SITE_TMA_F64 = {1204: 859.31e6 / (32 * 32 * 32 * 24), 1408: 799.29e6 / (32 * 32 * 32 * 24)}
+# DRAM bytes (read + write) per site of one full-lattice F64 launch at 32^3x64,
+# from single-pass ncu captures of each configuration
+# (profiles/dslash_full_f64_dram_32x32x32x64.txt): variant -> bytes/site.
+# Variant 2 is the cp.async kernel, 1000 + 100*stages + rows the TMA kernel.
+DRAM_BYTES_PER_SITE_F64_FULL = {
+    2: 2252085512 / 2097152, 1204: 2329534320 / 2097152, 1208: 2332055480 / 2097152,
+    1304: 2243929008 / 2097152, 1404: 2666579136 / 2097152, 1408: 2206948256 / 2097152,
+    1604: 2194087920 / 2097152, 1216: 2357703600 / 2097152,
+}
 
 
 def dram_bytes_per_site(cfg) -> float:
-    """ncu DRAM bytes per site of the full-lattice F64 kernel `cfg` runs
-    (TMA configurations without their own capture use the nearest one)."""
-    if cfg is not None and cfg[0] >= 1000:
-        v = cfg[0]
-        return DRAM_BYTES_PER_SITE_TMA_F64.get(v, DRAM_BYTES_PER_SITE_TMA_F64[1204 if v % 100 <= 4 else 1408])
-    return DRAM_BYTES_PER_SITE_FULL_F64
+    """ncu DRAM bytes per site of the full-lattice F64 configuration `cfg`
+    (configurations without their own capture: the largest measured)."""
+    v = 2 if cfg is None else cfg[0]
+    return DRAM_BYTES_PER_SITE_F64_FULL.get(v, max(DRAM_BYTES_PER_SITE_F64_FULL.values()))
 
 
 def measured_peaks():
@@ -422,8 +422,9 @@ def run_ours(args, d: Dist):
                      "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
                      "bytes_per_site": BYTES_FULL[0], "kernel": kernel_name(head_cfg),
                      "traffic": round(dram_bytes_per_site(head_cfg) * V),
-                     "traffic_note": "ncu dram bytes of one launch of this kernel on a smaller lattice "
-                                     "(inputs > L2), scaled by sites"},
+                     "traffic_note": ("ncu dram bytes (read + write) of one launch of this configuration "
+                                      "at 32^3x64, single-pass capture"
+                                      + ("" if tuple(L) == (32, 32, 32, 64) else ", scaled by sites"))},
         "per_parity_f64": parity,
         "f32": fp32,
         "e2e": e2e,

@@ -37,6 +37,8 @@
 #include <cudaTypedefs.h>
 
 #include <atomic>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -52,6 +54,7 @@ struct TmaGeom {
     int L0, L0h, L1, L2, L3;
     int NY;       // rows per tile (divides L1)
     int nty;      // L1 / NY
+    int bz, bt;   // tile order: blocks of bz z-lines x bt t-slices (divide L2, L3)
     int nitems;   // tiles (x 2 parities in full mode)
     int nstage;   // shared-memory buffers in the ring
     int ncw;      // consumer warps = NY * L0h / 32
@@ -86,10 +89,19 @@ __device__ __forceinline__ TileCoord tile_coord(const TmaGeom &g, int item) {
         c.p = g.out_parity;
         tile = item;
     }
-    c.zt = tile / g.nty;
-    c.y0 = (tile - c.zt * g.nty) * g.NY;
-    c.t = c.zt / g.L2;
-    c.z = c.zt - c.t * g.L2;
+    // y-tiles fastest, then z and t inside a (bz x bt) block, then the
+    // blocks (z-blocks inner): a block's z and t neighbours are read while
+    // they are still in L2
+    int k = tile / g.nty;
+    c.y0 = (tile - k * g.nty) * g.NY;
+    const int zin = k % g.bz;
+    k /= g.bz;
+    const int tin = k % g.bt;
+    k /= g.bt;
+    const int nbz = g.L2 / g.bz;
+    c.z = (k % nbz) * g.bz + zin;
+    c.t = (k / nbz) * g.bt + tin;
+    c.zt = c.z + g.L2 * c.t;
     return c;
 }
 
@@ -418,6 +430,18 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     tg.L3 = g.L[3];
     tg.NY = ny;
     tg.nty = g.L[1] / ny;
+    // tile-order block: PLQCD_TMA_ORDER="bz,bt" (each must divide its extent;
+    // 1,1 = plain z-fastest order)
+    // (default: the largest of 8, 4, 2, 1 dividing each extent; at 32^3x64
+    // 8x8 blocks cut the DRAM bytes of a launch from 1140 to 1100 per site)
+    {
+        auto div = [](int L) { return L % 8 == 0 ? 8 : (L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : 1)); };
+        int bz = div(g.L[2]), bt = div(g.L[3]);
+        if (const char *e = getenv("PLQCD_TMA_ORDER"))
+            if (sscanf(e, "%d,%d", &bz, &bt) != 2) bz = bt = 1;
+        tg.bz = (bz > 0 && g.L[2] % bz == 0) ? bz : 1;
+        tg.bt = (bt > 0 && g.L[3] % bt == 0) ? bt : 1;
+    }
     const long ntiles = (long)tg.nty * g.L[2] * g.L[3];
     if (ntiles * (full ? 2 : 1) > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash: lattice too large");
     tg.nitems = (int)(ntiles * (full ? 2 : 1));
