@@ -273,6 +273,9 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
     cudaEventElapsedTime(&ms, e0, e1);
     inf.seconds = ms / 1e3;
     cudaFreeHost(hst);
+    // a hop whose staged loads never arrived leaves a flag, not a CUDA error
+    if (!rc && dslash_tma_status(true))
+        rc = set_error(PLQCD_ERR_TIMEOUT, "plqcd_invert_cg: a TMA stage wait of a hop ran out");
     if (info) *info = inf;
     if (rc) return rc;
     if (!inf.converged)
