@@ -33,6 +33,8 @@
 
 #include "plqcd_global_params.h"
 #include "start.h"
+#include "su3_256.h"
+#include "su3_512.h"
 #include "utils.h"
 
 #ifdef __cplusplus
@@ -83,6 +85,25 @@ double plqcd_hopping_matrix_eo_single_mic_split_nohalfspinor_short(double *qout_
                                                                    double *u_im, double *qin_re, double *qin_im);
 double plqcd_hopping_matrix_oe_single_mic_split_nohalfspinor_short(double *qout_re, double *qout_im, double *u_re,
                                                                    double *u_im, double *qin_re, double *qin_im);
+
+/*
+ * Lane-packed names (reference include/dirac.h:37-38, 46-51): arrays of
+ * spinor_256 / su3_256 (two consecutive even/odd sites per object) or
+ * spinor_512 / su3_512 (four), as built by the copy_*_to_*_256/512
+ * converters (include/su3_256.h, su3_512.h); eo writes the packed objects
+ * of the even half of qout from the odd half of qin, oe the reverse, and
+ * every name computes the same operator as the AoS entry points. The
+ * *_short name reads link rows 0,1 only and rebuilds row 2 as
+ * conj(row0 x row1). Links are cached like the AoS ones.
+ */
+double plqcd_hopping_matrix_eo_intrin_256(spinor_256 *qin, spinor_256 *qout, su3_256 *u);
+double plqcd_hopping_matrix_oe_intrin_256(spinor_256 *qin, spinor_256 *qout, su3_256 *u);
+double plqcd_hopping_matrix_eo_intrin_512(spinor_512 *qin, spinor_512 *qout, su3_512 *u);
+double plqcd_hopping_matrix_oe_intrin_512(spinor_512 *qin, spinor_512 *qout, su3_512 *u);
+double plqcd_hopping_matrix_eo_single_mic(spinor_512 *qin, spinor_512 *qout, su3_512 *u);
+double plqcd_hopping_matrix_oe_single_mic(spinor_512 *qin, spinor_512 *qout, su3_512 *u);
+double plqcd_hopping_matrix_eo_single_mic_short(spinor_512 *qin, spinor_512 *qout, su3_512 *u);
+double plqcd_hopping_matrix_oe_single_mic_short(spinor_512 *qin, spinor_512 *qout, su3_512 *u);
 
 #ifdef __cplusplus
 }

@@ -123,6 +123,8 @@ _SIGS = {
     "plqcd_gauge_update": (_i, [_vp]),
     "plqcd_dropin_last_stats": (_i, [_dp, _dp, _dp]),
     "plqcd_aos_to_split": (_i, [_vp, _vp, _vp, ctypes.c_long]),
+    **{f"plqcd_hopping_matrix_{w}_{v}": (ctypes.c_double, [_vp, _vp, _vp])
+       for w in ("eo", "oe") for v in ("intrin_256", "intrin_512", "single_mic", "single_mic_short")},
     "plqcd_split_to_aos": (_i, [_vp, _vp, _vp, ctypes.c_long]),
 }
 
@@ -197,6 +199,38 @@ def hopping_matrix(which: str, qin: np.ndarray, qout: np.ndarray, u: np.ndarray,
     t = f(qin.ctypes.data, qout.ctypes.data, u.ctypes.data)
     if t < 0:
         raise PlqcdError(f"hopping matrix failed: {last_error()}")
+    return t
+
+
+PACKED_LANES = {"intrin_256": 2, "intrin_512": 4, "single_mic": 4, "single_mic_short": 4}
+
+
+def pack_lanes(a: np.ndarray, lanes: int) -> np.ndarray:
+    """API-layout objects (n, E) -> lane-packed (n/lanes, E, lanes): the
+    layout of arrays of spinor_256/512 (E = 12) or su3_256/512 (E = 9 per
+    link, 36 per site) built by the copy_*_256/512 converters."""
+    n, E = a.shape
+    return np.ascontiguousarray(a.reshape(n // lanes, lanes, E).transpose(0, 2, 1))
+
+
+def unpack_lanes(p: np.ndarray) -> np.ndarray:
+    m, E, lanes = p.shape
+    return np.ascontiguousarray(p.transpose(0, 2, 1).reshape(m * lanes, E))
+
+
+def hopping_matrix_packed(which: str, qin: np.ndarray, qout: np.ndarray, u: np.ndarray, variant: str) -> float:
+    """The lane-packed entry points on API-layout arrays: qin/u are packed
+    for the call, the output objects unpacked back into qout (only the output
+    parity changes)."""
+    lanes = PACKED_LANES[variant]
+    V = qin.shape[0]
+    pq, po = pack_lanes(qin, lanes), pack_lanes(qout, lanes)
+    pu = pack_lanes(u.reshape(V, 36), lanes)
+    f = getattr(lib(), f"plqcd_hopping_matrix_{which}_{variant}")
+    t = f(pq.ctypes.data, po.ctypes.data, pu.ctypes.data)
+    if t < 0:
+        raise PlqcdError(f"hopping matrix failed: {last_error()}")
+    qout[:] = unpack_lanes(po)
     return t
 
 

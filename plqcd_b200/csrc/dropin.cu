@@ -68,6 +68,14 @@ struct DropIn {
     int graph_next = 0;
     GraphKey last_key;
     bool last_valid = false;
+    // lane-packed entry points (spinor_256 / spinor_512 and su3_256 / su3_512)
+    plqcd_gauge *gauge_packed = nullptr, *gauge_packed12 = nullptr;
+    struct {
+        const void *u = nullptr;
+        int lanes = 0;
+        uint64_t fp = 0;
+    } packed18, packed12;
+    bool dirty_packed = true;
 };
 
 std::mutex g_mu;
@@ -78,6 +86,8 @@ void release_locked() {
     if (g_d.gauge) plqcd_gauge_destroy(g_d.gauge);
     if (g_d.gauge_split) plqcd_gauge_destroy(g_d.gauge_split);
     if (g_d.gauge12) plqcd_gauge_destroy(g_d.gauge12);
+    if (g_d.gauge_packed) plqcd_gauge_destroy(g_d.gauge_packed);
+    if (g_d.gauge_packed12) plqcd_gauge_destroy(g_d.gauge_packed12);
     void *bufs[4] = {g_d.aos_in, g_d.aos_out, g_d.f_in, g_d.f_out};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -528,6 +538,151 @@ double hop_call_split(double *qout_re, double *qout_im, double *u_re, double *u_
     return stop_watch(t0);
 }
 
+// ---- lane-packed types (include/su3_256.h, su3_512.h) ----------------------------
+// The reference's intrin_256 / intrin_512 / single_mic kernels
+// (lib/dirac.c:3506, 7122, 7503) take arrays of packed objects that each
+// hold `lanes` (2 or 4) consecutive even/odd sites, one complex element of
+// every site per lane (tests/test_hopping.c:256-275): complex element e of
+// site s sits at ((s / lanes) * E + e) * lanes + s % lanes, E = 12 for a
+// spinor and 36 for the four links of a site. The arrays are moved as they
+// are and unpacked / packed on the device around the same kernels as the
+// AoS entry points; the result is the correct operator for every name.
+
+__global__ void k_lanes_to_sites(double2 *dst, const double2 *src, long nsites, int lanes, int E) {
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= nsites * E) return;
+    const long site = i / E;
+    const int e = (int)(i - site * E);
+    dst[i] = src[((site / lanes) * E + e) * lanes + site % lanes];
+}
+
+__global__ void k_sites_to_lanes(double2 *dst, const double2 *src, long nsites, int lanes, int E) {
+    const long j = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (j >= nsites * E) return;
+    const int lane = (int)(j % lanes);
+    const long rest = j / lanes;
+    const int e = (int)(rest % E);
+    const long site = (rest / E) * lanes + lane;
+    dst[j] = src[site * E + e];
+}
+
+int relayout(cudaStream_t s, void *dst, const void *src, long nsites, int lanes, int E, bool to_sites) {
+    const long n = nsites * E;
+    if (n == 0) return PLQCD_OK;
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (to_sites)
+        k_lanes_to_sites<<<blocks, 256, 0, s>>>(static_cast<double2 *>(dst), static_cast<const double2 *>(src),
+                                                 nsites, lanes, E);
+    else
+        k_sites_to_lanes<<<blocks, 256, 0, s>>>(static_cast<double2 *>(dst), static_cast<const double2 *>(src),
+                                                 nsites, lanes, E);
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+// gauge field from a lane-packed host array, in chunks of sites
+int load_gauge_packed(plqcd_gauge *g, const void *u, int lanes) {
+    const Geom &geo = g->lat->geom;
+    cudaStream_t s = g->lat->stream;
+    const long nsites = 2 * geo.Vh, chunk = 1L << 18;  // sites per chunk (multiple of 4)
+    const long per = nsites < chunk ? nsites : chunk;
+    void *st = nullptr;
+    if (cudaMalloc(&st, 2 * per * 4 * sizeof(su3)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(PLQCD_ERR_NOMEM, "packed gauge upload: staging allocation failed");
+    }
+    char *packed = static_cast<char *>(st), *aos = packed + per * 4 * sizeof(su3);
+    int rc = PLQCD_OK;
+    for (long first = 0; first < nsites && rc == PLQCD_OK; first += per) {
+        const long n = nsites - first < per ? nsites - first : per;
+        cudaError_t e = cudaMemcpyAsync(packed, static_cast<const char *>(u) + first * 4 * sizeof(su3),
+                                        n * 4 * sizeof(su3), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            rc = set_error(PLQCD_ERR_CUDA, "packed gauge upload: %s", cudaGetErrorString(e));
+            break;
+        }
+        rc = relayout(s, aos, packed, n, lanes, 36, true);
+        if (rc == PLQCD_OK)
+            rc = launch_gauge_import(geo, s, aos, 4 * first, 4 * n, g->data, g->prec, g->recon);
+        if (rc == PLQCD_OK && cudaStreamSynchronize(s) != cudaSuccess)
+            rc = set_error(PLQCD_ERR_CUDA, "packed gauge upload failed");
+    }
+    cudaFree(st);
+    return rc;
+}
+
+double hop_call_packed(const void *qin, void *qout, const void *u, int out_parity, int lanes, bool short12) {
+    double t0 = stop_watch(0.0);
+    clear_error();
+    if (!qin || !qout || !u) {
+        set_error(PLQCD_ERR_ARG, "packed hopping matrix: null argument");
+        return -1.0;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (ensure_locked() != PLQCD_OK) return -1.0;
+    plqcd_lattice *lat = g_d.lat;
+    const Geom &geo = lat->geom;
+    const long Vh = geo.Vh;
+    cudaStream_t s = lat->stream;
+    if (Vh % lanes) {
+        set_error(PLQCD_ERR_ARG, "packed hopping matrix: half volume %ld is not a multiple of %d lanes", Vh, lanes);
+        return -1.0;
+    }
+    if (cudaSetDevice(lat->device) != cudaSuccess) {
+        set_error(PLQCD_ERR_CUDA, "packed hopping matrix: cudaSetDevice failed");
+        return -1.0;
+    }
+    g_d.h2d = g_d.d2h = 0;
+    plqcd_gauge *&gf = short12 ? g_d.gauge_packed12 : g_d.gauge_packed;
+    if (!gf && plqcd_gauge_create(lat, PLQCD_F64, short12 ? 12 : 18, &gf) != PLQCD_OK) return -1.0;
+    const uint64_t fp = fingerprint(static_cast<const su3 *>(u), 8 * Vh);
+    auto &pc = short12 ? g_d.packed12 : g_d.packed18;
+    if (!env_flag("PLQCD_GAUGE_CACHE", true) || g_d.dirty_packed || pc.u != u || pc.lanes != lanes || pc.fp != fp) {
+        if (load_gauge_packed(gf, u, lanes) != PLQCD_OK) return -1.0;
+        pc.u = u;
+        pc.lanes = lanes;
+        pc.fp = fp;
+        g_d.h2d += 8.0 * Vh * sizeof(su3);
+    }
+    g_d.dirty_packed = false;
+    const int in_parity = out_parity ^ 1;
+    const size_t half = sizeof(spinor) * Vh;  // one parity, in either layout
+    void *stage = g_d.aos_out, *aos = g_d.aos_in;
+    cudaError_t e = cudaMemcpyAsync(stage, static_cast<const char *>(qin) + in_parity * half, half,
+                                    cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        set_error(PLQCD_ERR_CUDA, "packed hopping matrix: H2D: %s", cudaGetErrorString(e));
+        return -1.0;
+    }
+    if (relayout(s, aos, stage, Vh, lanes, 12, true) != PLQCD_OK) return -1.0;
+    if (launch_spinor_import(geo, s, aos, 0, g_d.f_in, PLQCD_F64, 0, Vh) != PLQCD_OK) return -1.0;
+    DslashCall dc;
+    dc.gauge = gf->data;
+    dc.prec = PLQCD_F64;
+    dc.recon = gf->recon;
+    dc.out = g_d.f_out;
+    dc.in = g_d.f_in;
+    dc.out_parity = out_parity;
+    cudaEventRecord(g_d.ev_k0[0], s);
+    if (launch_dslash(geo, s, dc) != PLQCD_OK) return -1.0;
+    cudaEventRecord(g_d.ev_k1[0], s);
+    if (launch_spinor_export(geo, s, g_d.f_out, PLQCD_F64, 0, aos, 0, Vh) != PLQCD_OK) return -1.0;
+    if (relayout(s, stage, aos, Vh, lanes, 12, false) != PLQCD_OK) return -1.0;
+    e = cudaMemcpyAsync(static_cast<char *>(qout) + out_parity * half, stage, half, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error(PLQCD_ERR_CUDA, "packed hopping matrix: %s", cudaGetErrorString(e));
+        return -1.0;
+    }
+    g_d.h2d += (double)half;
+    g_d.d2h += (double)half;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, g_d.ev_k0[0], g_d.ev_k1[0]);
+    g_d.kernel_ms = ms;
+    lat->last_kernel_ms = ms;
+    return stop_watch(t0);
+}
+
 }  // namespace
 
 namespace plqcd {
@@ -542,6 +697,7 @@ extern "C" int plqcd_gauge_update(const su3 *u) {
     (void)u;
     g_d.dirty = true;
     g_d.dirty_split = true;
+    g_d.dirty_packed = true;
     return PLQCD_OK;
 }
 
@@ -590,4 +746,31 @@ extern "C" double plqcd_hopping_matrix_eo_sse3_intrin_blocking(spinor *qin, spin
 }
 extern "C" double plqcd_hopping_matrix_oe_sse3_intrin_blocking(spinor *qin, spinor *qout, su3 *u) {
     return hop_call(qin, qout, u, 1);
+}
+
+// lane-packed names: include/dirac.h:37-38 (256), 46-51 (512, MIC); the
+// _short form reads link rows 0 and 1 and rebuilds row 2 as conj(row0 x row1)
+extern "C" double plqcd_hopping_matrix_eo_intrin_256(spinor_256 *qin, spinor_256 *qout, su3_256 *u) {
+    return hop_call_packed(qin, qout, u, 0, 2, false);
+}
+extern "C" double plqcd_hopping_matrix_oe_intrin_256(spinor_256 *qin, spinor_256 *qout, su3_256 *u) {
+    return hop_call_packed(qin, qout, u, 1, 2, false);
+}
+extern "C" double plqcd_hopping_matrix_eo_intrin_512(spinor_512 *qin, spinor_512 *qout, su3_512 *u) {
+    return hop_call_packed(qin, qout, u, 0, 4, false);
+}
+extern "C" double plqcd_hopping_matrix_oe_intrin_512(spinor_512 *qin, spinor_512 *qout, su3_512 *u) {
+    return hop_call_packed(qin, qout, u, 1, 4, false);
+}
+extern "C" double plqcd_hopping_matrix_eo_single_mic(spinor_512 *qin, spinor_512 *qout, su3_512 *u) {
+    return hop_call_packed(qin, qout, u, 0, 4, false);
+}
+extern "C" double plqcd_hopping_matrix_oe_single_mic(spinor_512 *qin, spinor_512 *qout, su3_512 *u) {
+    return hop_call_packed(qin, qout, u, 1, 4, false);
+}
+extern "C" double plqcd_hopping_matrix_eo_single_mic_short(spinor_512 *qin, spinor_512 *qout, su3_512 *u) {
+    return hop_call_packed(qin, qout, u, 0, 4, true);
+}
+extern "C" double plqcd_hopping_matrix_oe_single_mic_short(spinor_512 *qin, spinor_512 *qout, su3_512 *u) {
+    return hop_call_packed(qin, qout, u, 1, 4, true);
 }

@@ -274,3 +274,27 @@ def test_print_params_matches_reference_golden(tmp_path):
         P.finalize_plqcd()
     want = open(os.path.join(GOLD, "print_params_4x4x4x4.txt"), "rb").read()
     assert out.read_bytes() == want
+
+
+@pytest.mark.parametrize("lanes", [2, 4])
+def test_python_lane_packing_matches_the_header_converters(tmp_path, lanes):
+    """plqcd_b200.pack_lanes lays out spinors and links exactly as the
+    packed-type converters do when driven like the reference's test driver
+    (pairs / quadruples of consecutive even/odd sites), so the lane-packed
+    entry points are tested on the layout legacy callers build."""
+    so = tmp_path / "pack.so"
+    r = subprocess.run(["gcc", "-std=c11", "-O2", "-shared", "-fPIC", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "c", "pack_arrays.c"), "-o", str(so)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    lib = ctypes.CDLL(str(so))
+    V = 64
+    rng = np.random.default_rng(lanes)
+    q = rng.standard_normal((V, 12)) + 1j * rng.standard_normal((V, 12))
+    u = rng.standard_normal((4 * V, 9)) + 1j * rng.standard_normal((4 * V, 9))
+    pq, pu = np.zeros_like(q), np.zeros_like(u)
+    lib.pack_spinors(lanes, q.ctypes.data_as(ctypes.c_void_p), pq.ctypes.data_as(ctypes.c_void_p), V)
+    lib.pack_links(lanes, u.ctypes.data_as(ctypes.c_void_p), pu.ctypes.data_as(ctypes.c_void_p), V)
+    assert np.array_equal(pq.reshape(-1), P.pack_lanes(q, lanes).reshape(-1))
+    assert np.array_equal(pu.reshape(-1), P.pack_lanes(u.reshape(V, 36), lanes).reshape(-1))
+    assert np.array_equal(P.unpack_lanes(P.pack_lanes(q, lanes)), q)

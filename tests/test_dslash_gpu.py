@@ -574,3 +574,53 @@ def test_tma_kernel_rejects_misfit_tiles(cuda, monkeypatch):
         monkeypatch.setenv("PLQCD_DSLASH_STAGES", v)
         with pytest.raises(P.PlqcdError):
             lat.dslash(g64, o, a, 0, P.F64)
+
+
+def test_tma_kernel_bit_identical_at_benchmark_size(cuda, monkeypatch):
+    """At the benchmark lattice (32^3x64) the TMA configuration the tuner
+    picks there (2 stages x 4 rows, blocked tile order) gives the same bits
+    as the cp.async kernel for the full lattice and for one parity."""
+    L = (32, 32, 32, 64)
+    lat = new_lattice(L)
+    g64 = P.Gauge(lat, P.F64, 18)
+    g64.random(46)
+    bs = lat.spinor_bytes(P.F64)
+    fe, fo = dev_bytes(bs), dev_bytes(bs)
+    lat.spinor_gaussian(fe, P.F64, 0, 11)
+    lat.spinor_gaussian(fo, P.F64, 1, 12)
+    outs = {}
+    for v in ("2", "1204"):
+        monkeypatch.setenv("PLQCD_DSLASH_STAGES", v)
+        monkeypatch.setenv("PLQCD_DSLASH_BLOCK", "64")
+        oe, oo, o1 = dev_bytes(bs), dev_bytes(bs), dev_bytes(bs)
+        lat.dslash_full(g64, oe, oo, fe, fo, P.F64)
+        lat.dslash(g64, o1, fe, P.ODD, P.F64)
+        lat.synchronize()
+        outs[v] = (oe, oo, o1)
+    for a, b in zip(outs["2"], outs["1204"]):
+        assert bool((a == b).all())
+
+
+@pytest.mark.parametrize("variant", ["intrin_256", "intrin_512", "single_mic", "single_mic_short"])
+def test_lane_packed_entry_points(dropin, restatement, variant):
+    """The lane-packed names (spinor_256/512, su3_256/512 arrays) compute the
+    reference's operator on the packed layout; eo writes only the even
+    objects of qout, oe only the odd ones; a changed link array is picked
+    up through plqcd_gauge_update."""
+    L = (8, 4, 6, 4)
+    dropin(L)
+    V = O.volume(L)
+    rng = np.random.default_rng(29)
+    q, u = O.gaussian_spinor(V, rng), O.random_su3(4 * V, rng)
+    want = restatement.hop("full", L, q, u)
+    got = np.full_like(q, np.nan)
+    P.hopping_matrix_packed("eo", q, got, u, variant)
+    assert np.isnan(got[V // 2:]).all() and not np.isnan(got[: V // 2]).any()
+    P.hopping_matrix_packed("oe", q, got, u, variant)
+    tol = 1e-13 if variant.endswith("short") else TOL64
+    assert relmax(got, want) < tol
+    u2 = O.random_su3(4 * V, rng)
+    P.lib().plqcd_gauge_update(None)
+    P.hopping_matrix_packed("eo", q, got, u2, variant)
+    P.hopping_matrix_packed("oe", q, got, u2, variant)
+    assert relmax(got, restatement.hop("full", L, q, u2)) < tol
