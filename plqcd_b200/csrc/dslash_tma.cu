@@ -59,19 +59,150 @@ struct TmaGeom {
     int nstage;   // shared-memory buffers in the ring
     int ncw;      // consumer warps = NY * L0h / 32
     int full, out_parity;
-    // byte offsets inside one stage buffer and the bytes each load brings
-    uint32_t off_sp_row, off_lk_main, off_lk_row, stage_bytes;
-    uint32_t sp_main_bytes, sp_row_bytes, lk_main_bytes, lk_row_bytes;
+    // byte offsets inside one stage buffer and the bytes each load brings;
+    // a spinor format has 1 or 2 plane groups (16-bit formats: values and
+    // the per-site norms), each with its own tensor maps
+    int sp_ng;
+    uint32_t off_sp_main[2], off_sp_row[2], off_lk_main, off_lk_row, stage_bytes;
+    uint32_t sp_main_bytes[2], sp_row_bytes[2], lk_main_bytes, lk_row_bytes;
     double a_up, a_low, b, g5_in;
     void *out0, *out1;  // output of parity 0 / 1 (full); out0 otherwise
     const void *x;      // xpay operand (single parity)
 };
 
 // tensor maps: input spinor field f (full mode: field 0 = even input, read
-// by the odd output; field 1 = odd input), NY-row and one-row boxes
+// by the odd output; field 1 = odd input) and plane group, NY-row and
+// one-row boxes
 struct __align__(64) TmaMaps {
-    CUtensorMap sp_main[2], sp_row[2], lk_main, lk_row;
+    CUtensorMap sp_main[2][2], sp_row[2][2], lk_main, lk_row;
 };
+
+// ---- per-format staged loads ---------------------------------------------------
+// A stage holds each plane group as [plane][row][x] with the format's own
+// element size; element i of plane k is at group base + (i + k * ps) elements.
+// The loaders return exactly what the gather kernels' loads return (16-bit
+// spinors unscaled plus the site norm), so the arithmetic is identical.
+template <class SIO>
+struct TmaSpinor;
+
+template <>
+struct TmaSpinor<SpinorIO<PLQCD_F64>> {
+    __device__ static __forceinline__ void load(const uint8_t *g0, const uint8_t *, int i, int ps, cx<double> s[12],
+                                                double &n) {
+        const double2 *p = reinterpret_cast<const double2 *>(g0) + i;
+#pragma unroll
+        for (int c = 0; c < 12; c++) {
+            const double2 v = p[c * ps];
+            s[c] = {v.x, v.y};
+        }
+        n = 1.0;
+    }
+};
+
+template <>
+struct TmaSpinor<SpinorIO<PLQCD_F32>> {
+    __device__ static __forceinline__ void load(const uint8_t *g0, const uint8_t *, int i, int ps, cx<float> s[12],
+                                                float &n) {
+        const float4 *p = reinterpret_cast<const float4 *>(g0) + i;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const float4 v = p[k * ps];
+            s[2 * k] = {v.x, v.y};
+            s[2 * k + 1] = {v.z, v.w};
+        }
+        n = 1.f;
+    }
+};
+
+template <int PREC>
+struct TmaSpinor16 {
+    __device__ static __forceinline__ void load(const uint8_t *g0, const uint8_t *g1, int i, int ps, cx<float> s[12],
+                                                float &n) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(g0) + i;
+        uint4 v[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = p[k * ps];
+        n = reinterpret_cast<const float *>(g1)[i];
+        SpinorIO16<PREC>::unpack3(v, s);
+    }
+};
+template <>
+struct TmaSpinor<SpinorIO<PLQCD_F16>> : TmaSpinor16<PLQCD_F16> {};
+template <>
+struct TmaSpinor<SpinorIO<PLQCD_BF16>> : TmaSpinor16<PLQCD_BF16> {};
+
+template <class LIO>
+struct TmaLink;
+
+template <>
+struct TmaLink<LinkIO<PLQCD_F64, 18>> {
+    __device__ static __forceinline__ void load(const uint8_t *g, int i, int ps, cx<double> U[9]) {
+        const double2 *p = reinterpret_cast<const double2 *>(g) + i;
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            const double2 v = p[e * ps];
+            U[e] = {v.x, v.y};
+        }
+    }
+};
+
+template <>
+struct TmaLink<LinkIO<PLQCD_F64, 12>> {
+    __device__ static __forceinline__ void load(const uint8_t *g, int i, int ps, cx<double> U[9]) {
+        const double2 *p = reinterpret_cast<const double2 *>(g) + i;
+#pragma unroll
+        for (int e = 0; e < 6; e++) {
+            const double2 v = p[e * ps];
+            U[e] = {v.x, v.y};
+        }
+        reconstruct_row2(U);
+    }
+};
+
+template <>
+struct TmaLink<LinkIO<PLQCD_F32, 18>> {
+    __device__ static __forceinline__ void load(const uint8_t *g, int i, int ps, cx<float> U[9]) {
+        const float2 *p = reinterpret_cast<const float2 *>(g) + i;
+#pragma unroll
+        for (int e = 0; e < 9; e++) {
+            const float2 v = p[e * ps];
+            U[e] = {v.x, v.y};
+        }
+    }
+};
+
+template <>
+struct TmaLink<LinkIO<PLQCD_F32, 12>> {
+    __device__ static __forceinline__ void load(const uint8_t *g, int i, int ps, cx<float> U[9]) {
+        const float4 *p = reinterpret_cast<const float4 *>(g) + i;
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            const float4 v = p[e * ps];
+            U[2 * e] = {v.x, v.y};
+            U[2 * e + 1] = {v.z, v.w};
+        }
+        reconstruct_row2(U);
+    }
+};
+
+template <int PREC>
+struct TmaLink16 {
+    __device__ static __forceinline__ void load(const uint8_t *g, int i, int ps, cx<float> U[9]) {
+        const uint2 *p = reinterpret_cast<const uint2 *>(g) + i;
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            const uint2 v = p[e * ps];
+            const float2 a = Half2<PREC>::unpack(v.x), b = Half2<PREC>::unpack(v.y);
+            U[2 * e] = {a.x, a.y};
+            U[2 * e + 1] = {b.x, b.y};
+        }
+        reconstruct_row2(U);
+    }
+};
+template <>
+struct TmaLink<LinkIO<PLQCD_F16, 12>> : TmaLink16<PLQCD_F16> {};
+template <>
+struct TmaLink<LinkIO<PLQCD_BF16, 12>> : TmaLink16<PLQCD_BF16> {};
 
 __device__ int g_tma_status;  // set to 1 when a stage wait ran out
 
@@ -124,22 +255,21 @@ __device__ __forceinline__ void tma_issue_dir(const TmaMaps &m, const TmaGeom &g
     // forward links sit at the output site, backward ones at the neighbour
     const int lzt = fwd ? c.zt : szt;
     const int lplane = (fwd ? c.p : q) * 4 + mu;
-    uint32_t bytes = g.sp_main_bytes + g.lk_main_bytes;
-    if (d == 1) bytes += g.sp_row_bytes;
-    if (d == 5) bytes += g.sp_row_bytes + g.lk_row_bytes;
+    const bool extra = d == 1 || d == 5;  // y stages: one spinor row across the tile edge
+    uint32_t bytes = g.lk_main_bytes + (d == 5 ? g.lk_row_bytes : 0u);
+    for (int gr = 0; gr < g.sp_ng; gr++) bytes += g.sp_main_bytes[gr] + (extra ? g.sp_row_bytes[gr] : 0u);
     mbar_arrive_expect_tx(bar, bytes);
-    const void *spm = f ? (const void *)&m.sp_main[1] : (const void *)&m.sp_main[0];
-    const void *spr = f ? (const void *)&m.sp_row[1] : (const void *)&m.sp_row[0];
-    tma_load_4d(dst, spm, bar, 0, c.y0, szt, 0);
-    tma_load_5d(dst + g.off_lk_main, &m.lk_main, bar, 0, c.y0, lzt, 0, lplane);
-    if (d == 1) {
-        const int yr = (c.y0 + g.NY == g.L1) ? 0 : c.y0 + g.NY;
-        tma_load_4d(dst + g.off_sp_row, spr, bar, 0, yr, c.zt, 0);
-    } else if (d == 5) {
-        const int yr = (c.y0 == 0) ? g.L1 - 1 : c.y0 - 1;
-        tma_load_4d(dst + g.off_sp_row, spr, bar, 0, yr, c.zt, 0);
-        tma_load_5d(dst + g.off_lk_row, &m.lk_row, bar, 0, yr, c.zt, 0, q * 4 + 1);
+    const int yr = d == 1 ? ((c.y0 + g.NY == g.L1) ? 0 : c.y0 + g.NY) : ((c.y0 == 0) ? g.L1 - 1 : c.y0 - 1);
+    for (int gr = 0; gr < g.sp_ng; gr++) {
+        const void *spm = f ? (const void *)&m.sp_main[1][gr] : (const void *)&m.sp_main[0][gr];
+        tma_load_4d(dst + g.off_sp_main[gr], spm, bar, 0, c.y0, szt, 0);
+        if (extra) {
+            const void *spr = f ? (const void *)&m.sp_row[1][gr] : (const void *)&m.sp_row[0][gr];
+            tma_load_4d(dst + g.off_sp_row[gr], spr, bar, 0, yr, c.zt, 0);
+        }
     }
+    tma_load_5d(dst + g.off_lk_main, &m.lk_main, bar, 0, c.y0, lzt, 0, lplane);
+    if (d == 5) tma_load_5d(dst + g.off_lk_row, &m.lk_row, bar, 0, yr, c.zt, 0, q * 4 + 1);
 }
 
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
@@ -216,7 +346,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
     const int L0h = g.L0h;
     const int j = tid / L0h, xh = tid - j * L0h;
     const int own = j * L0h + xh;
-    const int SM = g.NY * L0h;  // plane stride of an NY-row box, 16-byte units
+    const int SM = g.NY * L0h;  // plane stride of an NY-row box, in elements
     const R sg = (R)g.g5_in;
     const R aup = (R)g.a_up, alow = (R)g.a_low;
     int b = 0;
@@ -238,44 +368,31 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
                 return;
             }
             const uint8_t *st = sbase + (size_t)b * g.stage_bytes;
-            const uint4 *spm = reinterpret_cast<const uint4 *>(st);
-            const uint4 *spr = reinterpret_cast<const uint4 *>(st + g.off_sp_row);
-            const uint4 *lkm = reinterpret_cast<const uint4 *>(st + g.off_lk_main);
-            const uint4 *lkr = reinterpret_cast<const uint4 *>(st + g.off_lk_row);
-            const uint4 *sp, *lk;
-            int sst = SM, lst = SM;
+            // element index and plane stride of the neighbour spinor and the
+            // link, in the NY-row box or in the one-row box of a y stage
+            bool sp_row = false, lk_row = false;
+            int si, li;
             if (d == 0) {
-                sp = spm + (own - xh + xph);
-                lk = lkm + own;
+                si = own - xh + xph;
+                li = own;
             } else if (d == 4) {
-                sp = spm + (own - xh + xmh);
-                lk = lkm + (own - xh + xmh);
+                si = own - xh + xmh;
+                li = si;
             } else if (d == 1) {
-                lk = lkm + own;
-                if (j + 1 < g.NY) {
-                    sp = spm + own + L0h;
-                } else {
-                    sp = spr + xh;
-                    sst = L0h;
-                }
+                li = own;
+                sp_row = j + 1 == g.NY;
+                si = sp_row ? xh : own + L0h;
             } else if (d == 5) {
-                if (j > 0) {
-                    sp = spm + own - L0h;
-                    lk = lkm + own - L0h;
-                } else {
-                    sp = spr + xh;
-                    lk = lkr + xh;
-                    sst = L0h;
-                    lst = L0h;
-                }
+                sp_row = lk_row = j == 0;
+                si = li = sp_row ? xh : own - L0h;
             } else {
-                sp = spm + own;
-                lk = lkm + own;
+                si = li = own;
             }
             cx<R> s[12], U[9];
             R n;
-            SIO::load_staged_raw(sp, sst, s, n);
-            LIO::load_staged(lk, lst, U);
+            TmaSpinor<SIO>::load(st + (sp_row ? g.off_sp_row[0] : g.off_sp_main[0]),
+                                 st + (sp_row ? g.off_sp_row[1] : g.off_sp_main[1]), si, sp_row ? L0h : SM, s, n);
+            TmaLink<LIO>::load(st + (lk_row ? g.off_lk_row : g.off_lk_main), li, lk_row ? L0h : SM, U);
             // the values are in registers: release the buffer to the producer
             __syncwarp();
             if ((tid & 31) == 0) mbar_arrive(empty_bar + 8u * b);
@@ -325,20 +442,53 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// a field of `planes` 16-byte planes over the half lattice, viewed as
-// (2*L0h u64, L1, L2*L3, planes[, 8 parity-mu blocks])
-int encode_map(CUtensorMap *m, const void *base, const Geom &g, int planes, bool links, int rows) {
+// Plane groups of a format: element bytes and planes per group (spinor:
+// one or two groups; links: one group per (parity, mu) block).
+struct TmaFormat {
+    int sp_ng, sp_eb[2], sp_np[2];
+    int lk_eb, lk_np;
+};
+
+bool tma_format(int prec, int recon, TmaFormat *f) {
+    *f = TmaFormat{1, {16, 0}, {12, 0}, 16, 9};
+    if (prec == PLQCD_F64 && recon == 18) return true;
+    if (prec == PLQCD_F64 && recon == 12) {
+        f->lk_np = 6;
+        return true;
+    }
+    if (prec == PLQCD_F32) {
+        f->sp_np[0] = 6;
+        if (recon == 18) {
+            f->lk_eb = 8;
+            f->lk_np = 9;
+        } else {
+            f->lk_np = 3;
+        }
+        return recon == 18 || recon == 12;
+    }
+    if ((prec == PLQCD_F16 || prec == PLQCD_BF16) && recon == 12) {
+        *f = TmaFormat{2, {16, 4}, {3, 1}, 8, 3};
+        return true;
+    }
+    return false;
+}
+
+// `planes` planes of `eb`-byte elements over the half lattice, viewed as
+// (row elements, L1, L2*L3, planes[, 8 parity-mu blocks]); rows of 16- and
+// 8-byte elements are moved as 8-byte words, rows of 4-byte elements as such
+int encode_map(CUtensorMap *m, const void *base, const Geom &g, int eb, int planes, bool links, int rows) {
     auto fn = encode_fn();
     if (!fn) return set_error(PLQCD_ERR_CUDA, "dslash: cuTensorMapEncodeTiled is not available");
-    const cuuint64_t row_b = (cuuint64_t)g.L0h * 16;
-    cuuint64_t dims[5] = {(cuuint64_t)2 * g.L0h, (cuuint64_t)g.L[1], (cuuint64_t)g.L[2] * g.L[3],
-                          (cuuint64_t)planes, 8};
-    cuuint64_t strides[4] = {row_b, row_b * g.L[1], (cuuint64_t)g.Vh * 16, (cuuint64_t)g.Vh * 16 * planes};
-    cuuint32_t box[5] = {(cuuint32_t)(2 * g.L0h), (cuuint32_t)rows, 1, (cuuint32_t)planes, 1};
+    const cuuint64_t row_b = (cuuint64_t)g.L0h * eb;
+    const int word = eb >= 8 ? 8 : 4;
+    const cuuint64_t inner = row_b / word;
+    cuuint64_t dims[5] = {inner, (cuuint64_t)g.L[1], (cuuint64_t)g.L[2] * g.L[3], (cuuint64_t)planes, 8};
+    cuuint64_t strides[4] = {row_b, row_b * g.L[1], (cuuint64_t)g.Vh * eb, (cuuint64_t)g.Vh * eb * planes};
+    cuuint32_t box[5] = {(cuuint32_t)inner, (cuuint32_t)rows, 1, (cuuint32_t)planes, 1};
     cuuint32_t es[5] = {1, 1, 1, 1, 1};
-    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, links ? 5 : 4, const_cast<void *>(base), dims, strides, box,
-                    es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = fn(m, word == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32, links ? 5 : 4,
+                    const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(PLQCD_ERR_CUDA, "dslash: tensor map encoding failed (%d)", (int)r);
     return PLQCD_OK;
 }
@@ -381,28 +531,57 @@ int launch_tma_t(cudaStream_t s, const dev::TmaMaps &m, const dev::TmaGeom &tg, 
 
 }  // namespace
 
-int dslash_tma_plan(const Geom &g, int prec, int recon, int nstage, int ny, int *block, size_t *smem) {
-    int nsp, nlk;
-    if (prec == PLQCD_F64 && recon == 18) {
-        nsp = 12;
-        nlk = 9;
-    } else if (prec == PLQCD_F64 && recon == 12) {
-        nsp = 12;
-        nlk = 6;
-    } else if (prec == PLQCD_F32 && recon == 12) {
-        nsp = 6;
-        nlk = 3;
-    } else {
-        return set_error(PLQCD_ERR_ARG, "dslash: no TMA kernel for precision/reconstruction %d/%d", prec, recon);
+namespace {
+
+// stage layout of a format and tile: offsets (128-byte aligned) and the bytes
+// of each box
+struct StageLayout {
+    uint32_t off_sp_main[2] = {0, 0}, off_sp_row[2] = {0, 0}, off_lk_main = 0, off_lk_row = 0, bytes = 0;
+    uint32_t sp_main_bytes[2] = {0, 0}, sp_row_bytes[2] = {0, 0}, lk_main_bytes = 0, lk_row_bytes = 0;
+};
+
+StageLayout stage_layout(const TmaFormat &f, int L0h, int ny) {
+    StageLayout l;
+    uint32_t off = 0;
+    auto take = [&](uint32_t n) {
+        const uint32_t o = off;
+        off += round128(n);
+        return o;
+    };
+    for (int gr = 0; gr < f.sp_ng; gr++) {
+        l.sp_main_bytes[gr] = (uint32_t)(f.sp_np[gr] * f.sp_eb[gr] * L0h * ny);
+        l.off_sp_main[gr] = take(l.sp_main_bytes[gr]);
+        l.sp_row_bytes[gr] = (uint32_t)(f.sp_np[gr] * f.sp_eb[gr] * L0h);
+        l.off_sp_row[gr] = take(l.sp_row_bytes[gr]);
     }
-    if (nstage < 2 || nstage > 8 || ny < 1 || g.L0h > 128 || g.L[1] % ny || (ny * g.L0h) % 32 ||
-        ny * g.L0h > 256)
+    l.lk_main_bytes = (uint32_t)(f.lk_np * f.lk_eb * L0h * ny);
+    l.off_lk_main = take(l.lk_main_bytes);
+    l.lk_row_bytes = (uint32_t)(f.lk_np * f.lk_eb * L0h);
+    l.off_lk_row = take(l.lk_row_bytes);
+    l.bytes = off;
+    return l;
+}
+
+// a row of eb-byte elements must be a whole number of 16-byte units (tile
+// loads) and at most 256 words
+bool row_ok(int L0h, int eb) {
+    const int word = eb >= 8 ? 8 : 4;
+    return (L0h * eb) % 16 == 0 && L0h * eb / word <= 256;
+}
+
+}  // namespace
+
+int dslash_tma_plan(const Geom &g, int prec, int recon, int nstage, int ny, int *block, size_t *smem) {
+    TmaFormat f;
+    if (!tma_format(prec, recon, &f))
+        return set_error(PLQCD_ERR_ARG, "dslash: no TMA kernel for precision/reconstruction %d/%d", prec, recon);
+    bool rows = row_ok(g.L0h, f.lk_eb);
+    for (int gr = 0; gr < f.sp_ng; gr++) rows = rows && row_ok(g.L0h, f.sp_eb[gr]);
+    if (nstage < 2 || nstage > 8 || ny < 1 || !rows || g.L[1] % ny || (ny * g.L0h) % 32 || ny * g.L0h > 256)
         return set_error(PLQCD_ERR_ARG, "dslash: TMA tile %d rows x %d stages does not fit %dx%dx%dx%d", ny, nstage,
                          g.L[0], g.L[1], g.L[2], g.L[3]);
-    const uint32_t row = (uint32_t)g.L0h * 16;
-    const uint32_t stage = round128(nsp * row * ny) + round128(nsp * row) + round128(nlk * row * ny) +
-                           round128(nlk * row);
-    const size_t bytes = (size_t)nstage * stage + 16u * nstage + 128;
+    const StageLayout l = stage_layout(f, g.L0h, ny);
+    const size_t bytes = (size_t)nstage * l.bytes + 16u * nstage + 128;
     if (bytes > 227u * 1024 - 64) return set_error(PLQCD_ERR_ARG, "dslash: TMA ring of %zu bytes too large", bytes);
     if (block) *block = ny * g.L0h + 32;
     if (smem) *smem = bytes;
@@ -416,9 +595,9 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     PLQCD_TRY(dslash_tma_plan(g, prec, recon, nstage, ny, &block, &smem));
     if (a.nrhs != 1 || a.h_begin != 0 || a.h_end != g.Vh || (full && xpay))
         return set_error(PLQCD_ERR_ARG, "dslash: the TMA kernel takes whole single fields");
-    const int nsp = prec == PLQCD_F64 ? 12 : 6;
-    const int nlk = prec == PLQCD_F64 ? (recon == 18 ? 9 : 6) : 3;
-    const uint32_t row = (uint32_t)g.L0h * 16;
+    TmaFormat fmt;
+    tma_format(prec, recon, &fmt);
+    const StageLayout lay = stage_layout(fmt, g.L0h, ny);
 
     dev::TmaGeom tg;
     memset(&tg, 0, sizeof tg);
@@ -449,14 +628,18 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     tg.ncw = ny * g.L0h / 32;
     tg.full = full ? 1 : 0;
     tg.out_parity = a.out_parity;
-    tg.sp_main_bytes = nsp * row * ny;
-    tg.sp_row_bytes = nsp * row;
-    tg.lk_main_bytes = nlk * row * ny;
-    tg.lk_row_bytes = nlk * row;
-    tg.off_sp_row = round128(tg.sp_main_bytes);
-    tg.off_lk_main = tg.off_sp_row + round128(tg.sp_row_bytes);
-    tg.off_lk_row = tg.off_lk_main + round128(tg.lk_main_bytes);
-    tg.stage_bytes = tg.off_lk_row + round128(tg.lk_row_bytes);
+    tg.sp_ng = fmt.sp_ng;
+    for (int gr = 0; gr < 2; gr++) {
+        tg.sp_main_bytes[gr] = lay.sp_main_bytes[gr];
+        tg.sp_row_bytes[gr] = lay.sp_row_bytes[gr];
+        tg.off_sp_main[gr] = lay.off_sp_main[gr];
+        tg.off_sp_row[gr] = lay.off_sp_row[gr];
+    }
+    tg.lk_main_bytes = lay.lk_main_bytes;
+    tg.lk_row_bytes = lay.lk_row_bytes;
+    tg.off_lk_main = lay.off_lk_main;
+    tg.off_lk_row = lay.off_lk_row;
+    tg.stage_bytes = lay.bytes;
     tg.a_up = a.a_up;
     tg.a_low = a.a_low;
     tg.b = a.b;
@@ -469,25 +652,35 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     memset(&m, 0, sizeof m);
     const int nf = full ? 2 : 1;
     for (int f = 0; f < nf; f++) {
-        PLQCD_TRY(encode_map(&m.sp_main[f], a.in[f], g, nsp, false, ny));
-        PLQCD_TRY(encode_map(&m.sp_row[f], a.in[f], g, nsp, false, 1));
+        size_t goff = 0;  // byte offset of the plane group in the field
+        for (int gr = 0; gr < fmt.sp_ng; gr++) {
+            const void *base = static_cast<const char *>(a.in[f]) + goff;
+            PLQCD_TRY(encode_map(&m.sp_main[f][gr], base, g, fmt.sp_eb[gr], fmt.sp_np[gr], false, ny));
+            PLQCD_TRY(encode_map(&m.sp_row[f][gr], base, g, fmt.sp_eb[gr], fmt.sp_np[gr], false, 1));
+            goff += (size_t)fmt.sp_np[gr] * fmt.sp_eb[gr] * g.Vh;
+        }
     }
-    if (!full) {
-        m.sp_main[1] = m.sp_main[0];
-        m.sp_row[1] = m.sp_row[0];
-    }
-    PLQCD_TRY(encode_map(&m.lk_main, a.gauge, g, nlk, true, ny));
-    PLQCD_TRY(encode_map(&m.lk_row, a.gauge, g, nlk, true, 1));
+    if (!full)
+        for (int gr = 0; gr < 2; gr++) {
+            m.sp_main[1][gr] = m.sp_main[0][gr];
+            m.sp_row[1][gr] = m.sp_row[0][gr];
+        }
+    PLQCD_TRY(encode_map(&m.lk_main, a.gauge, g, fmt.lk_eb, fmt.lk_np, true, ny));
+    PLQCD_TRY(encode_map(&m.lk_row, a.gauge, g, fmt.lk_eb, fmt.lk_np, true, 1));
 
     using namespace dev;
-    if (prec == PLQCD_F64 && recon == 18)
-        return xpay ? launch_tma_t<SpinorIO<PLQCD_F64>, LinkIO<PLQCD_F64, 18>, true>(s, m, tg, block, smem)
-                    : launch_tma_t<SpinorIO<PLQCD_F64>, LinkIO<PLQCD_F64, 18>, false>(s, m, tg, block, smem);
-    if (prec == PLQCD_F64)
-        return xpay ? launch_tma_t<SpinorIO<PLQCD_F64>, LinkIO<PLQCD_F64, 12>, true>(s, m, tg, block, smem)
-                    : launch_tma_t<SpinorIO<PLQCD_F64>, LinkIO<PLQCD_F64, 12>, false>(s, m, tg, block, smem);
-    return xpay ? launch_tma_t<SpinorIO<PLQCD_F32>, LinkIO<PLQCD_F32, 12>, true>(s, m, tg, block, smem)
-                : launch_tma_t<SpinorIO<PLQCD_F32>, LinkIO<PLQCD_F32, 12>, false>(s, m, tg, block, smem);
+#define PLQCD_TMA_CASE(P, RC)                                                                              \
+    if (prec == P && recon == RC)                                                                          \
+        return xpay ? launch_tma_t<SpinorIO<P>, LinkIO<P, RC>, true>(s, m, tg, block, smem)                \
+                    : launch_tma_t<SpinorIO<P>, LinkIO<P, RC>, false>(s, m, tg, block, smem);
+    PLQCD_TMA_CASE(PLQCD_F64, 18)
+    PLQCD_TMA_CASE(PLQCD_F64, 12)
+    PLQCD_TMA_CASE(PLQCD_F32, 18)
+    PLQCD_TMA_CASE(PLQCD_F32, 12)
+    PLQCD_TMA_CASE(PLQCD_F16, 12)
+    PLQCD_TMA_CASE(PLQCD_BF16, 12)
+#undef PLQCD_TMA_CASE
+    return set_error(PLQCD_ERR_ARG, "dslash: no TMA kernel for precision/reconstruction %d/%d", prec, recon);
 }
 
 // Reads (and with `reset`, clears) the timeout flag of the TMA kernel on the

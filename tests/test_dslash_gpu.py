@@ -513,7 +513,8 @@ TMA_CASES = [((16, 8, 4, 6), 1204), ((16, 8, 4, 6), 1308), ((16, 8, 6, 4), 1404)
 
 
 @pytest.mark.parametrize("L,variant", TMA_CASES)
-@pytest.mark.parametrize("prec,recon", [(P.F64, 18), (P.F64, 12), (P.F32, 12)])
+@pytest.mark.parametrize("prec,recon", [(P.F64, 18), (P.F64, 12), (P.F32, 18), (P.F32, 12), (P.F16, 12),
+                                        (P.BF16, 12)])
 def test_tma_kernel_bit_identical(cuda, monkeypatch, L, variant, prec, recon):
     """The TMA-staged kernel (tile loads of whole rows into a shared-memory
     ring, one producer warp) computes exactly what the gather kernel
