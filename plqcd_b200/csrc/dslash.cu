@@ -235,11 +235,7 @@ static int launch_pipe(const Geom &g, cudaStream_t s, const DslashArgs &a, int b
     constexpr int NS = SIO::NSLOT + LIO::NSLOT;
     const size_t smem = (size_t)ST * NS * 16 * block;
     auto k = k_dslash_pipe<SIO, LIO, ST, COMPAT, XPAY, FULL>;
-    static bool attr_set = false;  // per instantiation
-    if (!attr_set) {
-        PLQCD_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        attr_set = true;
-    }
+    PLQCD_TRY(smem_optin((const void *)k, 227 * 1024));
     if (smem > 227 * 1024) return set_error(PLQCD_ERR_ARG, "dslash: %zu bytes of shared memory requested", smem);
     k<<<(unsigned)nblk, block, smem, s>>>(a);
     PLQCD_CUDA_TRY(cudaGetLastError());

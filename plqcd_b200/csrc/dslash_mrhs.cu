@@ -222,11 +222,7 @@ static int launch_nr_pipe(const Geom &g, cudaStream_t s, MrhsArgs a, int block, 
     const size_t smem = (size_t)ST * NS * 16 * block;
     if (smem > 227 * 1024) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: %zu bytes of shared memory", smem);
     auto k = xpay ? k_dslash_mrhs_pipe<SIO, LIO, NR, ST, true> : k_dslash_mrhs_pipe<SIO, LIO, NR, ST, false>;
-    static bool attr_set[2] = {false, false};  // per instantiation and epilogue
-    if (!attr_set[xpay]) {
-        PLQCD_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        attr_set[xpay] = true;
-    }
+    PLQCD_TRY(smem_optin((const void *)k, 227 * 1024));
     k<<<(unsigned)nblk, block, smem, s>>>(a);
     PLQCD_CUDA_TRY(cudaGetLastError());
     return PLQCD_OK;

@@ -513,11 +513,7 @@ inline uint32_t round128(uint32_t v) { return (v + 127u) & ~127u; }
 template <class SIO, class LIO, bool XPAY>
 int launch_tma_t(cudaStream_t s, const dev::TmaMaps &m, const dev::TmaGeom &tg, int block, size_t smem) {
     auto k = dev::k_dslash_tma<SIO, LIO, XPAY>;
-    static size_t attr_bytes = 0;  // per instantiation: the opt-in granted so far
-    if (smem > attr_bytes) {
-        PLQCD_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_bytes = smem;
-    }
+    PLQCD_TRY(smem_optin((const void *)k, smem));
     int occ = 0;
     PLQCD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, block, smem));
     if (occ < 1) return set_error(PLQCD_ERR_ARG, "dslash: TMA tile does not fit on an SM (%zu B)", smem);

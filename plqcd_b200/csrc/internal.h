@@ -132,6 +132,10 @@ int launch_dslash_config(const Geom &g, cudaStream_t s, const DslashCall &c, int
 int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
                        const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b);
 
+// dynamic shared-memory opt-in of kernel `func` on the current device, set
+// once per (kernel, device) to at least `bytes` (utils.cpp)
+int smem_optin(const void *func, size_t bytes);
+
 // device workspace of at least `bytes`, owned by the lattice (cg.cu)
 int lattice_workspace(plqcd_lattice *lat, size_t bytes, void **out);
 

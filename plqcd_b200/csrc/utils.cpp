@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -156,3 +157,27 @@ extern "C" int plqcd_split_to_aos(const double *re, const double *im, double *ao
     });
     return PLQCD_OK;
 }
+
+namespace plqcd {
+
+int smem_optin(const void *func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> granted;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(PLQCD_ERR_CUDA, "smem_optin: no current device");
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &have = granted[{func, dev}];
+    if (bytes <= have) return PLQCD_OK;
+    cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(PLQCD_ERR_CUDA, "shared-memory opt-in of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    have = bytes;
+    return PLQCD_OK;
+}
+
+}  // namespace plqcd
