@@ -71,7 +71,7 @@ def test_reference_arm_runs_on_rank_zero_only():
     code = (f"import sys; sys.path.insert(0, {ROOT!r}); import bench; sys.argv = ['bench.py', '--impl', "
             "'reference', '--gpus', '2', '--steps', '1', '--warmup', '0']; "
             "import unittest.mock as m\n"
-            "with m.patch.object(bench, 'cpu_reference_time', return_value=(0.5, 1, 2, 'reference')), "
+            "with m.patch.object(bench, 'cpu_reference_time', return_value=(0.5, 0.6, 1, 2, 'reference')), "
             "m.patch.object(bench, 'host_fields', return_value=(None, None)):\n"
             "    sys.exit(bench.main())")
     outs = _launch(code)
