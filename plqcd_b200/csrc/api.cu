@@ -351,6 +351,9 @@ extern "C" int plqcd_spinor_norm2(plqcd_lattice *lat, const void *fields, int pr
     PLQCD_TRY(check_prec(prec));
     if (!fields || !norms_dev || nfields < 1 || nfields > 65535)
         return set_error(PLQCD_ERR_ARG, "plqcd_spinor_norm2: bad argument");
+    PLQCD_TRY(check_field_ptr(fields, "plqcd_spinor_norm2"));
+    if (reinterpret_cast<uintptr_t>(norms_dev) & 7u)
+        return set_error(PLQCD_ERR_ARG, "plqcd_spinor_norm2: norms_dev is not 8-byte aligned");
     const int nb = norm2_blocks(lat->geom.Vh);
     const size_t pbytes = sizeof(double) * (size_t)nb * nfields;
     const size_t cbytes = sizeof(unsigned) * (size_t)nfields;

@@ -425,6 +425,13 @@ int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c) {
 }
 
 static int build_args(const Geom &g, const DslashCall &c, dev::DslashArgs &a) {
+    PLQCD_TRY(check_field_ptr(c.out, "dslash"));
+    PLQCD_TRY(check_field_ptr(c.in, "dslash"));
+    if (c.full) {
+        PLQCD_TRY(check_field_ptr(c.out2, "dslash_full"));
+        PLQCD_TRY(check_field_ptr(c.in2, "dslash_full"));
+    }
+    if (c.x) PLQCD_TRY(check_field_ptr(c.x, "dslash_xpay"));
     a.gauge = c.gauge;
     if (c.nrhs < 1 || (c.full && c.nrhs != 1)) return set_error(PLQCD_ERR_ARG, "dslash: nrhs = %d invalid", c.nrhs);
     a.nrhs = c.nrhs;

@@ -283,6 +283,9 @@ static int mrhs_dispatch(const Geom &g, cudaStream_t s, int prec, int recon, con
 int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
                        const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b) {
     if (nrhs < 1) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: nrhs must be >= 1");
+    PLQCD_TRY(check_field_ptr(out, "dslash_mrhs"));
+    PLQCD_TRY(check_field_ptr(in, "dslash_mrhs"));
+    if (x) PLQCD_TRY(check_field_ptr(x, "dslash_mrhs"));
     dev::MrhsArgs m{};
     m.gauge = gauge;
     m.in = static_cast<const char *>(in);

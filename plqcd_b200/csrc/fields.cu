@@ -262,6 +262,8 @@ __global__ void k_gauge_copy(void *dst, const void *src, long Vh) {
 
 int launch_spinor_import(const Geom &g, cudaStream_t s, const void *aos, int parity, void *dst, int prec, long first,
                          long count) {
+    PLQCD_TRY(check_field_ptr(aos, "spinor import (API layout)"));
+    PLQCD_TRY(check_field_ptr(dst, "spinor import"));
     if (count < 0) count = g.Vh - first;
 #define F(P) dev::k_spinor_import<P><<<dev::nblocks(count), dev::kBlock, 0, s>>>((const double2 *)aos, g.Vh, parity, dst, first, count)
     PLQCD_SPINOR_SWITCH(prec, F)
@@ -272,6 +274,8 @@ int launch_spinor_import(const Geom &g, cudaStream_t s, const void *aos, int par
 
 int launch_spinor_export(const Geom &g, cudaStream_t s, const void *src, int prec, int parity, void *aos, long first,
                          long count) {
+    PLQCD_TRY(check_field_ptr(src, "spinor export"));
+    PLQCD_TRY(check_field_ptr(aos, "spinor export (API layout)"));
     if (count < 0) count = g.Vh - first;
 #define F(P) dev::k_spinor_export<P><<<dev::nblocks(count), dev::kBlock, 0, s>>>(src, g.Vh, parity, (double2 *)aos, first, count)
     PLQCD_SPINOR_SWITCH(prec, F)
@@ -307,6 +311,8 @@ int launch_gauge_import_split(const Geom &g, cudaStream_t s, const double *re, c
 }
 
 int launch_spinor_convert(const Geom &g, cudaStream_t s, void *dst, int dprec, const void *src, int sprec) {
+    PLQCD_TRY(check_field_ptr(dst, "spinor convert"));
+    PLQCD_TRY(check_field_ptr(src, "spinor convert"));
 #define G(DP, SP) dev::k_spinor_convert<DP, SP><<<dev::nblocks(g.Vh), dev::kBlock, 0, s>>>(dst, src, g.Vh)
 #define F(DP)                                                  \
     switch (sprec) {                                           \
@@ -324,6 +330,7 @@ int launch_spinor_convert(const Geom &g, cudaStream_t s, void *dst, int dprec, c
 }
 
 int launch_spinor_gaussian(const Geom &g, cudaStream_t s, void *dst, int prec, int parity, uint64_t seed) {
+    PLQCD_TRY(check_field_ptr(dst, "spinor gaussian"));
 #define F(P) dev::k_spinor_gaussian<P><<<dev::nblocks(g.Vh), dev::kBlock, 0, s>>>(dst, g.Vh, parity, seed)
     PLQCD_SPINOR_SWITCH(prec, F)
 #undef F
@@ -333,6 +340,7 @@ int launch_spinor_gaussian(const Geom &g, cudaStream_t s, void *dst, int prec, i
 
 int launch_gauge_import(const Geom &g, cudaStream_t s, const void *aos, long first, long n, void *dst, int prec,
                         int recon) {
+    PLQCD_TRY(check_field_ptr(aos, "gauge import (API layout)"));
 #define F(P, R) dev::k_gauge_import<P, R><<<dev::nblocks(n), dev::kBlock, 0, s>>>((const double2 *)aos, first, n, g.Vh, dst)
     PLQCD_GAUGE_SWITCH(prec, recon, F)
 #undef F

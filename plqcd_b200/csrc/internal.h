@@ -28,6 +28,15 @@ void clear_error();
         if (_s != PLQCD_OK) return _s; \
     } while (0)
 
+// Device fields are read and written with 16-byte vector and tile loads: a
+// pointer that is not 16-byte aligned is refused before any launch.
+inline int check_field_ptr(const void *p, const char *what) {
+    if (!p) return set_error(PLQCD_ERR_ARG, "%s: null field pointer", what);
+    if (reinterpret_cast<uintptr_t>(p) & 15u)
+        return set_error(PLQCD_ERR_ARG, "%s: field pointer %p is not 16-byte aligned", what, p);
+    return PLQCD_OK;
+}
+
 // ---- geometry --------------------------------------------------------------
 struct Geom {
     int L[4];

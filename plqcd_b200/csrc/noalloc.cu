@@ -64,6 +64,9 @@ extern "C" int plqcd_spinor_norm2_noalloc(plqcd_lattice *lat, const void *fields
         return set_error(PLQCD_ERR_ARG,
                          "plqcd_spinor_norm2_noalloc: nfields = %d outside 1..%d (the size of its static scratch)",
                          nfields, kNoallocMaxFields);
+    PLQCD_TRY(check_field_ptr(fields, "plqcd_spinor_norm2_noalloc"));
+    if (reinterpret_cast<uintptr_t>(norms_dev) & 7u)
+        return set_error(PLQCD_ERR_ARG, "plqcd_spinor_norm2_noalloc: norms_dev is not 8-byte aligned");
     PLQCD_CUDA_TRY(cudaSetDevice(lat->device));
     void *base = nullptr;
     PLQCD_TRY(scratch_address(lat->device, &base));

@@ -625,3 +625,24 @@ def test_lane_packed_entry_points(dropin, restatement, variant):
     P.hopping_matrix_packed("eo", q, got, u2, variant)
     P.hopping_matrix_packed("oe", q, got, u2, variant)
     assert relmax(got, restatement.hop("full", L, q, u2)) < tol
+
+
+def test_misaligned_fields_are_refused(cuda):
+    """Field pointers that are not 16-byte aligned are refused with an
+    argument error before any launch (the kernels use 16-byte vector and
+    tile loads); nothing runs on the device with them."""
+    L = (4, 4, 4, 4)
+    lat, g64, u = _device_setup(L, 47)
+    bs = lat.spinor_bytes(P.F64)
+    buf = dev_bytes(bs + 64)
+    ok = buf.data_ptr()
+    bad = ok + 8
+    for call in (lambda: lat.dslash(g64, bad, ok + 16, 0, P.F64),
+                 lambda: lat.dslash(g64, ok, bad, 0, P.F64),
+                 lambda: lat.dslash_xpay(g64, ok, ok + 16, 0, P.F64, 1.0, bad, 1.0),
+                 lambda: lat.dslash_full(g64, ok, ok + 16, bad, ok + 32, P.F64),
+                 lambda: lat.spinor_gaussian(bad, P.F64, 0, 1),
+                 lambda: lat.spinor_convert(bad, P.F32, ok, P.F64)):
+        with pytest.raises(P.PlqcdError, match="aligned"):
+            call()
+    lat.synchronize()
