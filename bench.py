@@ -324,6 +324,11 @@ def run_ours(args, d: Dist):
     lat.spinor_gaussian(fo, P.F64, 1, 77 + d.rank)
 
     K, W = args.steps, args.warmup
+    if args.only == "sharded":  # the t-slab decomposition held on one device
+        res = run_sharded(torch, P, lat, g64, fe, fo, args)
+        if d.rank == 0:
+            print(json.dumps({"only": "sharded", "sharded": res}))
+        return 0
     if args.only == "cg":  # profiling runs of the solver section alone
         cg = run_cg(torch, P, lat, g64, buf, args)
         if d.rank == 0:
@@ -494,6 +499,53 @@ def run_e2e(torch, P, lat, g64, fe, fo, d: Dist, args):
     lib.afree(pout)
     lib.afree(pu)
     return res
+
+
+def run_sharded(torch, P, lat, g64, fe, fo, args):
+    """The t-slab decomposition (plqcd_b200/shard.py) with all `--shards`
+    slabs held by this process on one GPU, ghost slices copied in place: the
+    eo+oe pair over the slabs against the unsharded pair on the same fields.
+    The difference is the decomposition's own cost (ghost copies, separate
+    interior and boundary launches on site ranges); between GPUs the copies
+    become NCCL transfers overlapped with the interior slices."""
+    from plqcd_b200 import shard as SH
+    L, N = lat.dims, args.shards
+    stream = torch.cuda.current_stream().cuda_stream
+    u = g64.store_host()
+    aos = torch.zeros((lat.V, 12), dtype=torch.complex128, device="cuda")
+    lat.spinor_export(fe, P.F64, 0, aos)
+    lat.spinor_export(fo, P.F64, 1, aos)
+    lat.synchronize()
+    q = aos.cpu().numpy()
+    del aos
+    shards = [SH.ShardedLattice(L, r, N, lat.device, stream) for r in range(N)]
+    T = SH.LocalTransport(N)
+    gauges = [s.gauge_from_global(u) for s in shards]
+    del u
+    SH.exchange_gauge(shards, gauges, T)
+    ins = {p: [s.import_global(q, 1 - p) for s in shards] for p in (0, 1)}
+    outs = {p: [s.field(P.F64) for s in shards] for p in (0, 1)}
+
+    def sharded():
+        for p in (0, 1):
+            SH.dslash(shards, gauges, outs[p], ins[p], p, P.F64, T)
+
+    oe_, oo_ = (torch.empty(lat.spinor_bytes(P.F64), dtype=torch.uint8, device="cuda") for _ in range(2))
+
+    def single():
+        lat.dslash(g64, oe_, fo, P.EVEN, P.F64)
+        lat.dslash(g64, oo_, fe, P.ODD, P.F64)
+
+    K, W = max(10, args.steps // 10), max(3, args.warmup)
+    t_sh = time_kernel(torch, sharded, K, W) / 1e3 / K
+    t_1 = time_kernel(torch, single, K, W) / 1e3 / K
+    ghost = sum(2 * sum(n for _, n in s.geo.spinor_slices(P.F64, 1)) for s in shards)
+    return {"lattice": list(L), "slabs": N, "slab_t": shards[0].geo.Lt,
+            "sharded_gflops": round(lat.V * FLOP_PER_SITE / t_sh / 1e9, 1),
+            "single_pair_gflops": round(lat.V * FLOP_PER_SITE / t_1 / 1e9, 1),
+            "overhead": round(t_sh / t_1 - 1, 4),
+            "ghost_bytes_per_hop": ghost,
+            "note": "all slabs on one GPU; ghost slices copied on the device"}
 
 
 def run_cg(torch, P, lat, g64, buf, args):
@@ -699,8 +751,10 @@ def main():
     ap.add_argument("--delta", type=float, default=0.01, help="reliable-update threshold of the mixed solvers")
     ap.add_argument("--lattice", default=",".join(map(str, L_BENCH)),
                     help="L0,L1,L2,L3 of the hopping-matrix workload (default 32,32,32,64)")
-    ap.add_argument("--only", choices=["all", "dslash", "cg"], default="all",
-                    help="dslash / cg: only that section (profiling runs)")
+    ap.add_argument("--only", choices=["all", "dslash", "cg", "sharded"], default="all",
+                    help="dslash / cg: only that section (profiling runs); sharded: the t-slab "
+                         "decomposition with --shards slabs held on one GPU")
+    ap.add_argument("--shards", type=int, default=4, help="slabs of --only sharded")
     args = ap.parse_args()
     args.lattice = tuple(int(x) for x in args.lattice.split(","))
     d = Dist()

@@ -483,8 +483,9 @@ static int tune_dslash(const Geom &g, cudaStream_t s, const DslashCall &c, const
         }
     }
     // TMA-staged rows: ring depth x rows per tile, where the tile fits
-    const bool tma_ok = !(c.flags & PLQCD_DSLASH_COMPAT) && c.nrhs == 1 && a.h_begin == 0 && a.h_end == g.Vh &&
-                        getenv("PLQCD_NO_TMA") == nullptr;
+    const long slab = (long)g.L0h * g.L[1] * g.L[2];  // TMA tiles cover whole t-slices
+    const bool tma_ok = !(c.flags & PLQCD_DSLASH_COMPAT) && c.nrhs == 1 && a.h_begin % slab == 0 &&
+                        (a.h_end - a.h_begin) % slab == 0 && getenv("PLQCD_NO_TMA") == nullptr;
     if (tma_ok)
         for (int ny : {4, 8, 16, 2})
             for (int ns : {2, 3, 4, 6}) {

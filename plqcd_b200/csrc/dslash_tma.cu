@@ -54,7 +54,8 @@ struct TmaGeom {
     int L0, L0h, L1, L2, L3;
     int NY;       // rows per tile (divides L1)
     int nty;      // L1 / NY
-    int bz, bt;   // tile order: blocks of bz z-lines x bt t-slices (divide L2, L3)
+    int bz, bt;   // tile order: blocks of bz z-lines x bt t-slices (divide L2 and tc)
+    int t0, tc;   // the t-slices computed: [t0, t0 + tc) (all of them for whole fields)
     int nitems;   // tiles (x 2 parities in full mode)
     int nstage;   // shared-memory buffers in the ring
     int ncw;      // consumer warps = NY * L0h / 32
@@ -231,7 +232,7 @@ __device__ __forceinline__ TileCoord tile_coord(const TmaGeom &g, int item) {
     k /= g.bt;
     const int nbz = g.L2 / g.bz;
     c.z = (k % nbz) * g.bz + zin;
-    c.t = (k / nbz) * g.bt + tin;
+    c.t = g.t0 + (k / nbz) * g.bt + tin;
     c.zt = c.z + g.L2 * c.t;
     return c;
 }
@@ -589,8 +590,11 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     int block = 0;
     size_t smem = 0;
     PLQCD_TRY(dslash_tma_plan(g, prec, recon, nstage, ny, &block, &smem));
-    if (a.nrhs != 1 || a.h_begin != 0 || a.h_end != g.Vh || (full && xpay))
-        return set_error(PLQCD_ERR_ARG, "dslash: the TMA kernel takes whole single fields");
+    // whole t-slices of one field (all of them for the full lattice)
+    const long S = (long)g.L0h * g.L[1] * g.L[2];
+    if (a.nrhs != 1 || (full && xpay) || a.h_begin % S || (a.h_end - a.h_begin) % S ||
+        (full && (a.h_begin != 0 || a.h_end != g.Vh)))
+        return set_error(PLQCD_ERR_ARG, "dslash: the TMA kernel takes whole t-slices of single fields");
     TmaFormat fmt;
     tma_format(prec, recon, &fmt);
     const StageLayout lay = stage_layout(fmt, g.L0h, ny);
@@ -611,13 +615,16 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     // 8x8 blocks cut the DRAM bytes of a launch from 1140 to 1100 per site)
     {
         auto div = [](int L) { return L % 8 == 0 ? 8 : (L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : 1)); };
-        int bz = div(g.L[2]), bt = div(g.L[3]);
+        const int tc = (int)((a.h_end - a.h_begin) / S);
+        tg.t0 = (int)(a.h_begin / S);
+        tg.tc = tc;
+        int bz = div(g.L[2]), bt = div(tc);
         if (const char *e = getenv("PLQCD_TMA_ORDER"))
             if (sscanf(e, "%d,%d", &bz, &bt) != 2) bz = bt = 1;
         tg.bz = (bz > 0 && g.L[2] % bz == 0) ? bz : 1;
-        tg.bt = (bt > 0 && g.L[3] % bt == 0) ? bt : 1;
+        tg.bt = (bt > 0 && tc % bt == 0) ? bt : 1;
     }
-    const long ntiles = (long)tg.nty * g.L[2] * g.L[3];
+    const long ntiles = (long)tg.nty * g.L[2] * tg.tc;
     if (ntiles * (full ? 2 : 1) > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash: lattice too large");
     tg.nitems = (int)(ntiles * (full ? 2 : 1));
     tg.nstage = nstage;

@@ -14,10 +14,11 @@ lattice is cut along t only, one slab per rank (one process per GPU):
   and r*Lt is even, a site's local parity is its global parity plus one, so
   the field of global parity p is stored as the local field of parity 1 - p;
 * one hop: the input field's first and last interior slices go to the ranks
-  below and above (every SoA plane of a field keeps a t-slice contiguous, so
-  this is one send per plane and neighbour, no packing), the interior slices
-  that do not touch a ghost are computed meanwhile, then the two boundary
-  slices; the kernels are the single-device ones, run on site ranges
+  below and above. A t-slice is contiguous in every SoA plane, so the slice
+  of a group of planes is one strided (planes x slice-bytes) view: packed
+  with one copy, sent with one send, unpacked with one copy. The interior
+  slices that do not touch a ghost are computed meanwhile, then the two
+  boundary slices; the kernels are the single-device ones, run on site ranges
   (plqcd_dslash_sites), with the periodic wrap never reached in t;
 * links: the backward t-link of slice t' = 1 sits in ghost slice 0, filled
   once per gauge field from the rank below.
@@ -86,6 +87,19 @@ class SlabGeometry:
         ne, eb = GAUGE_PLANES[(prec, recon)]
         return self.plane_slices([eb] * (8 * ne), self.Vh, tl)
 
+    def spinor_groups(self, prec: int):
+        """Plane groups (byte offset, planes, element bytes) of a one-parity
+        field: planes of equal element size that follow each other."""
+        return _groups(SPINOR_PLANES[prec], self.Vh)
+
+    def gauge_groups(self, prec: int, recon: int):
+        ne, eb = GAUGE_PLANES[(prec, recon)]
+        return _groups([eb] * (8 * ne), self.Vh)
+
+    def cols(self, tl: int, eb: int):
+        """Byte columns of local slice tl in a plane of eb-byte elements."""
+        return slice(tl * self.S * eb, (tl + 1) * self.S * eb)
+
     # ---- API-layout (host) mapping between global and local arrays --------
     def local_to_global_sites(self):
         """For every local even/odd site index (API layout: parity-major),
@@ -129,62 +143,98 @@ class SlabGeometry:
         return (tl == 0) | (tl == self.Lt + 1)
 
 
+def _groups(plane_bytes, nsites):
+    out, off, i = [], 0, 0
+    while i < len(plane_bytes):
+        eb, n = plane_bytes[i], 0
+        while i < len(plane_bytes) and plane_bytes[i] == eb:
+            n, i = n + 1, i + 1
+        out.append((off, n, eb))
+        off += n * nsites * eb
+    return out
+
+
+def _view(field, geo: SlabGeometry, group):
+    """(planes, Vh * eb) byte view of one plane group of a field."""
+    off, n, eb = group
+    return field[off:off + n * geo.Vh * eb].view(n, geo.Vh * eb)
+
+
 class LocalTransport:
     """All slabs in one process (one device): ghost slices are copied."""
 
     def __init__(self, nranks: int):
         self.nranks = nranks
 
-    def exchange(self, geos, fields, slices_fn, lower: bool = True, upper: bool = True):
-        """fields[r]: torch uint8 tensor of rank r's field. slices_fn(geo, tl)
-        gives its plane byte ranges of local slice tl."""
+    def exchange(self, geos, fields, groups, lower: bool = True, upper: bool = True):
+        """fields[r]: torch uint8 tensor of rank r's field; groups: its plane
+        groups (SlabGeometry.spinor_groups / gauge_groups). One strided copy
+        per plane group and direction."""
         for r, geo in enumerate(geos):
-            last, first = geo.Lt, 1
-            if lower:  # my last interior slice -> ghost 0 of the rank above
-                dst = fields[geo.above]
-                for (so, n), (do, _) in zip(slices_fn(geo, last), slices_fn(geos[geo.above], 0)):
-                    dst[do:do + n].copy_(fields[r][so:so + n])
-            if upper:  # my first interior slice -> ghost Lt+1 of the rank below
-                dst = fields[geo.below]
-                for (so, n), (do, _) in zip(slices_fn(geo, first), slices_fn(geos[geo.below], geo.Lt + 1)):
-                    dst[do:do + n].copy_(fields[r][so:so + n])
+            for gr in groups:
+                src = _view(fields[r], geo, gr)
+                eb = gr[2]
+                if lower:  # my last interior slice -> ghost 0 of the rank above
+                    up = geos[geo.above]
+                    _view(fields[geo.above], up, gr)[:, up.cols(0, eb)].copy_(src[:, geo.cols(geo.Lt, eb)])
+                if upper:  # my first interior slice -> ghost Lt+1 of the rank below
+                    dn = geos[geo.below]
+                    _view(fields[geo.below], dn, gr)[:, dn.cols(dn.Lt + 1, eb)].copy_(src[:, geo.cols(1, eb)])
+
+
+class _Exchange:
+    """Sends and receives of one exchange in flight: wait() completes them
+    and copies the received slices into the ghost slices."""
+
+    def __init__(self, works, unpack):
+        self.works, self.unpack = works, unpack
+
+    def wait(self):
+        for w in self.works:
+            w.wait()
+        for dst, buf in self.unpack:
+            dst.copy_(buf)
 
 
 class DistTransport:
     """One slab per process: ghost slices travel by torch.distributed
-    point-to-point operations (NCCL between GPUs, gloo on the host), all of
-    one exchange in one batch."""
+    point-to-point operations (NCCL between GPUs, gloo on the host). Per plane
+    group and direction the boundary slice is packed into one contiguous
+    buffer (one strided copy), sent with one send, received into one buffer
+    and unpacked into the ghost slice; all sends and receives of an exchange
+    go in one batch."""
 
     def __init__(self, group=None):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
 
-    def start(self, geo: SlabGeometry, field, slices_fn, lower: bool = True, upper: bool = True):
-        """Post the sends and receives of one exchange; returns the work
-        handles (wait on them before reading the ghosts)."""
+    def start(self, geo: SlabGeometry, field, groups, lower: bool = True, upper: bool = True) -> _Exchange:
+        """Post the sends and receives of one exchange; call .wait() on the
+        result before reading the ghost slices."""
+        import torch
         dist = self.dist
         if geo.nranks == 1:
-            LocalTransport(1).exchange([geo], [field], slices_fn, lower, upper)
-            return []
-        ops = []
+            LocalTransport(1).exchange([geo], [field], groups, lower, upper)
+            return _Exchange([], [])
         grank = lambda r: dist.get_global_rank(self.group, r) if self.group is not None else r
-        if lower:
-            for (so, n) in slices_fn(geo, geo.Lt):
-                ops.append(dist.P2POp(dist.isend, field[so:so + n], grank(geo.above), self.group))
-            for (do, n) in slices_fn(geo, 0):
-                ops.append(dist.P2POp(dist.irecv, field[do:do + n], grank(geo.below), self.group))
-        if upper:
-            for (so, n) in slices_fn(geo, 1):
-                ops.append(dist.P2POp(dist.isend, field[so:so + n], grank(geo.below), self.group))
-            for (do, n) in slices_fn(geo, geo.Lt + 1):
-                ops.append(dist.P2POp(dist.irecv, field[do:do + n], grank(geo.above), self.group))
-        return dist.batch_isend_irecv(ops) if ops else []
+        ops, unpack = [], []
+        for gr in groups:
+            v, eb = _view(field, geo, gr), gr[2]
+            for on, src_tl, ghost_tl, to, frm in ((lower, geo.Lt, 0, geo.above, geo.below),
+                                                 (upper, 1, geo.Lt + 1, geo.below, geo.above)):
+                if not on:
+                    continue
+                send = v[:, geo.cols(src_tl, eb)].contiguous()
+                recv = torch.empty_like(send)
+                ops.append(dist.P2POp(dist.isend, send, grank(to), self.group))
+                ops.append(dist.P2POp(dist.irecv, recv, grank(frm), self.group))
+                unpack.append((v[:, geo.cols(ghost_tl, eb)], recv))
+        return _Exchange(dist.batch_isend_irecv(ops) if ops else [], unpack)
 
     @staticmethod
-    def wait(works):
-        for w in works:
-            w.wait()
+    def wait(ex: _Exchange):
+        ex.wait()
 
 
 class ShardedLattice:
@@ -249,11 +299,11 @@ def exchange_gauge(shards, gauges, transport):
     """Fill ghost slice 0 of every shard's gauge field (the backward t-link
     of the first interior slice) from the rank below."""
     views = [_wrap(g.data, g.lat.gauge_bytes(g.prec, g.recon), g.lat.device) for g in gauges]
-    fn = lambda geo, tl: geo.gauge_slices(gauges[0].prec, gauges[0].recon, tl)
+    groups = shards[0].geo.gauge_groups(gauges[0].prec, gauges[0].recon)
     if isinstance(transport, LocalTransport):
-        transport.exchange([s.geo for s in shards], views, fn, lower=True, upper=False)
+        transport.exchange([s.geo for s in shards], views, groups, lower=True, upper=False)
     else:
-        transport.wait(transport.start(shards[0].geo, views[0], fn, lower=True, upper=False))
+        transport.start(shards[0].geo, views[0], groups, lower=True, upper=False).wait()
 
 
 def dslash(shards, gauges, outs, ins, out_parity: int, prec: int, transport, flags: int = 0, a: float = 1.0,
@@ -262,21 +312,21 @@ def dslash(shards, gauges, outs, ins, out_parity: int, prec: int, transport, fla
     shards/gauges/outs/ins/xs: one entry per slab this process holds (all N
     with LocalTransport, one with DistTransport)."""
     p = SlabGeometry.local_parity(out_parity)
-    fn = lambda geo, tl: geo.spinor_slices(prec, tl)
+    groups = shards[0].geo.spinor_groups(prec)
     xs = xs if xs is not None else [None] * len(shards)
     if isinstance(transport, LocalTransport):
-        transport.exchange([s.geo for s in shards], ins, fn)
+        transport.exchange([s.geo for s in shards], ins, groups)
         for s, g, o, i, x in zip(shards, gauges, outs, ins, xs):
             h0, n = s.geo.interior()
             s.lat.dslash_sites(g, o, i, p, prec, h0, n, flags, a, x, b)
         return
     (s,), (g,), (o,), (i,), (x,) = shards, gauges, outs, ins, xs
     geo = s.geo
-    works = transport.start(geo, i, fn)
+    ex = transport.start(geo, i, groups)
     # slices 2 .. Lt-1 need no ghost: computed while the exchange runs
     if geo.Lt > 2:
         s.lat.dslash_sites(g, o, i, p, prec, 2 * geo.S, (geo.Lt - 2) * geo.S, flags, a, x, b)
-    transport.wait(works)
+    ex.wait()
     for tl in (1, geo.Lt):
         h0, n = geo.slice_range(tl)
         s.lat.dslash_sites(g, o, i, p, prec, h0, n, flags, a, x, b)

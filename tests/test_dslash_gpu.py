@@ -646,3 +646,32 @@ def test_misaligned_fields_are_refused(cuda):
         with pytest.raises(P.PlqcdError, match="aligned"):
             call()
     lat.synchronize()
+
+
+@pytest.mark.parametrize("variant", ["1204", "1308"])
+def test_tma_kernel_on_whole_slice_ranges(cuda, monkeypatch, variant):
+    """On a site range of whole t-slices (a slab interior, a pipeline chunk)
+    the TMA kernel writes the same bits as the gather kernel on that range
+    and leaves the other sites of the output untouched."""
+    L = (16, 8, 4, 6)
+    lat, g64, u = _device_setup(L, 48)
+    S = (L[0] // 2) * L[1] * L[2]
+    bs = lat.spinor_bytes(P.F64)
+    fin, x = dev_bytes(bs), dev_bytes(bs)
+    lat.spinor_gaussian(fin, P.F64, 1, 3)
+    lat.spinor_gaussian(x, P.F64, 0, 4)
+    outs = {}
+    for v in ("2", variant):
+        monkeypatch.setenv("PLQCD_DSLASH_STAGES", v)
+        monkeypatch.setenv("PLQCD_DSLASH_BLOCK", "64")
+        o = dev_bytes(bs)
+        o.fill_(7)
+        lat.dslash_sites(g64, o, fin, 0, P.F64, S, 4 * S, P.DSLASH_G5_IN, 0.5, x, -1.0)
+        lat.synchronize()
+        outs[v] = o
+    assert bool((outs["2"] == outs[variant]).all())
+    import torch
+    plane = outs[variant].view(12, -1)      # 12 planes of Vh * 16 bytes
+    assert bool((plane[:, :S * 16] == 7).all()) and bool((plane[:, 5 * S * 16:] == 7).all())
+    assert not bool((plane[:, S * 16:5 * S * 16] == 7).all())
+    del torch

@@ -106,7 +106,7 @@ ok = True
 for prec in (P.F64, P.F16):
     planes = SPINOR_PLANES[prec]
     f = fill(planes, geo.Vh)
-    T.wait(T.start(geo, f, lambda g, tl: g.plane_slices(planes, g.Vh, tl)))
+    T.start(geo, f, geo.spinor_groups(prec)).wait()
     for tl, gt in ((0, (geo.t0 - 1) % L[3]), (geo.Lt + 1, (geo.t0 + geo.Lt) % L[3])):
         for k, (o, n) in enumerate(geo.plane_slices(planes, geo.Vh, tl)):
             ok &= bool((f[o:o + n] == (7 * k + 3 * gt + 1) % 251).all())
@@ -119,7 +119,7 @@ for prec in (P.F64, P.F16):
 ne, eb = GAUGE_PLANES[(P.F64, 18)]
 planes = [eb] * (8 * ne)
 f = fill(planes, geo.Vh)
-T.wait(T.start(geo, f, lambda g, tl: g.plane_slices(planes, g.Vh, tl), lower=True, upper=False))
+T.start(geo, f, geo.gauge_groups(P.F64, 18), lower=True, upper=False).wait()
 for k, (o, n) in enumerate(geo.plane_slices(planes, geo.Vh, 0)):
     ok &= bool((f[o:o + n] == (7 * k + 3 * ((geo.t0 - 1) % L[3]) + 1) % 251).all())
 for (o, n) in geo.plane_slices(planes, geo.Vh, geo.Lt + 1):
