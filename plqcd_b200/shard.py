@@ -83,10 +83,6 @@ class SlabGeometry:
     def spinor_slices(self, prec: int, tl: int):
         return self.plane_slices(SPINOR_PLANES[prec], self.Vh, tl)
 
-    def gauge_slices(self, prec: int, recon: int, tl: int):
-        ne, eb = GAUGE_PLANES[(prec, recon)]
-        return self.plane_slices([eb] * (8 * ne), self.Vh, tl)
-
     def spinor_groups(self, prec: int):
         """Plane groups (byte offset, planes, element bytes) of a one-parity
         field: planes of equal element size that follow each other."""
