@@ -48,7 +48,8 @@ BYTES_HALF_12 = 52 + 8 * 24 + 52
 # DRAM bytes (read + write) per site of one full-lattice F64 launch at 32^3x64,
 # from single-pass ncu captures of each configuration
 # (profiles/dslash_full_f64_dram_32x32x32x64.txt): variant -> bytes/site.
-# Variant 2 is the cp.async kernel, 1000 + 100*stages + rows the TMA kernel.
+# Variant 2 is the cp.async kernel, 1000*kind + 100*stages + rows a TMA kernel
+# (kind 1: a stage per direction; 2-5: own-line rows staged once per tile).
 DRAM_BYTES_PER_SITE_F64_FULL = {
     2: 2252085512 / 2097152, 1204: 2329534320 / 2097152, 1208: 2332055480 / 2097152,
     1304: 2243929008 / 2097152, 1404: 2666579136 / 2097152, 1408: 2206948256 / 2097152,
@@ -279,6 +280,12 @@ def kernel_name(cfg) -> str:
     if cfg is None:
         return "k_dslash_pipe<F64,18,full>"
     v, b = cfg
+    if v >= 2000:
+        kind = v // 1000
+        own = kind - 1 if kind <= 3 else kind - 3
+        form = ", one box per stage" if kind >= 4 else ""
+        return (f"k_dslash_tma_xy<F64,18> ({own} own-line + {(v // 100) % 10} ring buffers{form}, "
+                f"{v % 100} rows per tile, full lattice)")
     if v >= 1000:
         return f"k_dslash_tma<F64,18> ({(v // 100) % 10} stages, {v % 100} rows per tile, full lattice)"
     if v in (2, 3):

@@ -376,7 +376,7 @@ static int launch_pr(const Geom &g, cudaStream_t s, const DslashArgs &a, int var
 }  // namespace dev
 
 int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, int prec, int recon, bool full,
-                      bool xpay, int nstage, int ny);
+                      bool xpay, int kind, int nstage, int ny);
 
 static int env_int(const char *name, int dflt) {
     const char *e = getenv(name);
@@ -487,18 +487,22 @@ static int tune_dslash(const Geom &g, cudaStream_t s, const DslashCall &c, const
     const bool tma_ok = !(c.flags & PLQCD_DSLASH_COMPAT) && c.nrhs == 1 && a.h_begin % slab == 0 &&
                         (a.h_end - a.h_begin) % slab == 0 && getenv("PLQCD_NO_TMA") == nullptr;
     if (tma_ok)
-        for (int ny : {4, 8, 16, 2})
-            for (int ns : {2, 3, 4, 6}) {
-                int blk = 0;
-                if (dslash_tma_plan(g, c.prec, c.recon, ns, ny, &blk, nullptr) != PLQCD_OK) {
-                    clear_error();
-                    continue;
+        // (kinds 3 and 5, two own-line buffers, lost to 2 and 4 at every
+        // measured point and are not tried)
+        for (int kind : {1, 2, 4})
+            for (int ny : {4, 8, 16, 2})
+                for (int ns : {1, 2, 3, 4, 6}) {
+                    if (kind == 2 ? ns == 6 : ns == 1) continue;
+                    int blk = 0;
+                    if (dslash_tma_plan(g, c.prec, c.recon, kind, ns, ny, &blk, nullptr) != PLQCD_OK) {
+                        clear_error();
+                        continue;
+                    }
+                    TuneResult r;
+                    r.variant = 1000 * kind + 100 * ns + ny;
+                    r.block = blk;
+                    cands.push_back(r);
                 }
-                TuneResult r;
-                r.variant = 1000 + 100 * ns + ny;
-                r.block = blk;
-                cands.push_back(r);
-            }
     // trial launches write into scratch outputs: an xpay whose output aliases
     // its x operand must not be applied more than once
     void *scratch[2] = {nullptr, nullptr};
@@ -548,7 +552,8 @@ static int dispatch(const Geom &g, cudaStream_t s, const DslashCall &c, const de
     const bool xpay = c.x != nullptr;
     if (variant >= 1000) {  // TMA-staged rows; the block follows from the tile
         if (compat) return set_error(PLQCD_ERR_ARG, "dslash: no bug-compatible TMA kernel");
-        return launch_dslash_tma(g, s, a, c.prec, c.recon, c.full, xpay, (variant / 100) % 10, variant % 100);
+        return launch_dslash_tma(g, s, a, c.prec, c.recon, c.full, xpay, variant / 1000, (variant / 100) % 10,
+                                 variant % 100);
     }
     if (block % 32 || block < 32 || block > 256) return set_error(PLQCD_ERR_ARG, "dslash: block size %d invalid", block);
     switch (c.prec * 100 + c.recon) {

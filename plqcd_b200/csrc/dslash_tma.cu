@@ -66,6 +66,12 @@ struct TmaGeom {
     int sp_ng;
     uint32_t off_sp_main[2], off_sp_row[2], off_lk_main, off_lk_row, stage_bytes;
     uint32_t sp_main_bytes[2], sp_row_bytes[2], lk_main_bytes, lk_row_bytes;
+    // shared own-line kernel (k_dslash_tma_xy): a second ring of nstage_a
+    // buffers of a_bytes for the own-line rows (NY rows plus the rows on
+    // either side of the tile), and a second link box in a stage buffer;
+    // split: one tile-load box per stage
+    int nstage_a, split;
+    uint32_t a_bytes, off_a_main[2], off_a_lo[2], off_a_hi[2], off_lk2;
     double a_up, a_low, b, g5_in;
     void *out0, *out1;  // output of parity 0 / 1 (full); out0 otherwise
     const void *x;      // xpay operand (single parity)
@@ -276,6 +282,167 @@ __device__ __forceinline__ void tma_issue_dir(const TmaMaps &m, const TmaGeom &g
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 constexpr uint64_t kDrainLimitNs = 200000000ull;  // 0.2 s
 
+// ---- shared own-line variant ----------------------------------------------------
+// The x+-, y+- neighbours of a tile all sit in the own (z, t) line: rows
+// y0-1 .. y0+NY of the input. k_dslash_tma_xy stages them once per tile, in
+// a ring of their own, and keeps them while the four x / y directions are
+// computed; the link ring carries six stages per tile:
+//   0: U_0, U_1 forward (own parity, own rows)     -> directions 0, 1
+//   1: spinor line z+1 + U_2 forward               -> 2
+//   2: spinor line t+1 + U_3 forward               -> 3
+//   3: U_0, U_1 backward (opposite parity; U_1 also the row y0-1) -> 4, 5
+//   4: spinor line z-1 + U_2 at line z-1           -> 6
+//   5: spinor line t-1 + U_3 at line t-1           -> 7
+// The split form carries one box per stage (12 stages per tile, buffers
+// about half the size, so more tiles fit on an SM):
+//   0: U_0 fwd  1: U_1 fwd  2: spinor z+1  3: U_2 fwd  4: spinor t+1
+//   5: U_3 fwd  6: U_0 bwd  7: U_1 bwd (+ row y0-1)  8: spinor z-1
+//   9: U_2 at z-1  10: spinor t-1  11: U_3 at t-1
+// and a spinor stage is kept until the link stage after it has arrived.
+// Directions are accumulated in the same order 0..7 as in the other kernels,
+// so the results are the same bits. Per tile it stages NY+2 own-line rows
+// instead of 4 NY + 2.
+
+// own-line rows of the input (y0-1 and y0+NY wrapped) into an A buffer
+__device__ __forceinline__ void tma_issue_xy_a(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, uint32_t dst,
+                                               uint32_t bar) {
+    const int f = g.full ? (c.p == 0 ? 1 : 0) : 0;
+    uint32_t bytes = 0;
+    for (int gr = 0; gr < g.sp_ng; gr++) bytes += g.sp_main_bytes[gr] + 2u * g.sp_row_bytes[gr];
+    mbar_arrive_expect_tx(bar, bytes);
+    const int ylo = c.y0 == 0 ? g.L1 - 1 : c.y0 - 1;
+    const int yhi = c.y0 + g.NY == g.L1 ? 0 : c.y0 + g.NY;
+    for (int gr = 0; gr < g.sp_ng; gr++) {
+        const void *spm = f ? (const void *)&m.sp_main[1][gr] : (const void *)&m.sp_main[0][gr];
+        const void *spr = f ? (const void *)&m.sp_row[1][gr] : (const void *)&m.sp_row[0][gr];
+        tma_load_4d(dst + g.off_a_main[gr], spm, bar, 0, c.y0, c.zt, 0);
+        tma_load_4d(dst + g.off_a_lo[gr], spr, bar, 0, ylo, c.zt, 0);
+        tma_load_4d(dst + g.off_a_hi[gr], spr, bar, 0, yhi, c.zt, 0);
+    }
+}
+
+// (z, t) line of the neighbour rows of direction d (0..3 forward mu, 4..7 backward)
+__device__ __forceinline__ int neighbour_line(const TmaGeom &g, const TileCoord &c, int d) {
+    const int mu = d & 3;
+    const bool fwd = d < 4;
+    if (mu == 2) {
+        const int z2 = fwd ? (c.z + 1 == g.L2 ? 0 : c.z + 1) : (c.z == 0 ? g.L2 - 1 : c.z - 1);
+        return z2 + g.L2 * c.t;
+    }
+    if (mu == 3) {
+        const int t2 = fwd ? (c.t + 1 == g.L3 ? 0 : c.t + 1) : (c.t == 0 ? g.L3 - 1 : c.t - 1);
+        return c.z + g.L2 * t2;
+    }
+    return c.zt;
+}
+
+// the NY spinor rows of the neighbour line of direction d (2, 3, 6, 7)
+__device__ __forceinline__ uint32_t tma_issue_line_spinor(const TmaMaps &m, const TmaGeom &g, const TileCoord &c,
+                                                          int d, uint32_t dst, uint32_t bar) {
+    const int f = g.full ? (c.p == 0 ? 1 : 0) : 0;
+    const int szt = neighbour_line(g, c, d);
+    uint32_t bytes = 0;
+    for (int gr = 0; gr < g.sp_ng; gr++) {
+        const void *spm = f ? (const void *)&m.sp_main[1][gr] : (const void *)&m.sp_main[0][gr];
+        tma_load_4d(dst + g.off_sp_main[gr], spm, bar, 0, c.y0, szt, 0);
+        bytes += g.sp_main_bytes[gr];
+    }
+    return bytes;
+}
+
+// the NY link rows of direction d: forward links at the tile's own rows and
+// parity, backward ones at the neighbour's rows and the opposite parity
+__device__ __forceinline__ void tma_issue_link(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, int d,
+                                               uint32_t dst, uint32_t bar) {
+    const int mu = d & 3;
+    const bool fwd = d < 4;
+    const int lzt = fwd ? c.zt : neighbour_line(g, c, d);
+    tma_load_5d(dst, &m.lk_main, bar, 0, c.y0, lzt, 0, (fwd ? c.p : (c.p ^ 1)) * 4 + mu);
+}
+
+// the link row y0-1 of U_1 at the opposite parity (the y- term of the tile's row 0)
+__device__ __forceinline__ void tma_issue_link_row(const TmaMaps &m, const TmaGeom &g, const TileCoord &c,
+                                                   uint32_t dst, uint32_t bar) {
+    const int ylo = c.y0 == 0 ? g.L1 - 1 : c.y0 - 1;
+    tma_load_5d(dst, &m.lk_row, bar, 0, ylo, c.zt, 0, (c.p ^ 1) * 4 + 1);
+}
+
+// link-ring stage s (0..5 of the six-stage table) into a B buffer. The
+// expected byte count is set before the loads are issued.
+__device__ __forceinline__ void tma_issue_xy_b(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, int s,
+                                               uint32_t dst, uint32_t bar) {
+    if (s == 0 || s == 3) {
+        const int d0 = s == 0 ? 0 : 4;
+        mbar_arrive_expect_tx(bar, 2u * g.lk_main_bytes + (s == 3 ? g.lk_row_bytes : 0u));
+        tma_issue_link(m, g, c, d0, dst + g.off_lk_main, bar);
+        tma_issue_link(m, g, c, d0 + 1, dst + g.off_lk2, bar);
+        if (s == 3) tma_issue_link_row(m, g, c, dst + g.off_lk_row, bar);
+        return;
+    }
+    const int d = s < 3 ? s + 1 : s + 2;  // 2, 3, 6, 7
+    uint32_t bytes = g.lk_main_bytes;
+    for (int gr = 0; gr < g.sp_ng; gr++) bytes += g.sp_main_bytes[gr];
+    mbar_arrive_expect_tx(bar, bytes);
+    tma_issue_line_spinor(m, g, c, d, dst, bar);
+    tma_issue_link(m, g, c, d, dst + g.off_lk_main, bar);
+}
+
+// direction served by split stage s (a spinor stage: that of the link stage after it)
+__host__ __device__ constexpr int split_dir(int s) {
+    return s < 2 ? s : (s < 6 ? (s >> 1) + 1 : (s < 8 ? s - 2 : (s >> 1) + 2));
+}
+__host__ __device__ constexpr bool split_is_spinor(int s) { return s == 2 || s == 4 || s == 8 || s == 10; }
+
+// split stage s (0..11) into a B buffer
+__device__ __forceinline__ void tma_issue_xy_split(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, int s,
+                                                   uint32_t dst, uint32_t bar) {
+    const int d = split_dir(s);
+    if (split_is_spinor(s)) {
+        uint32_t bytes = 0;
+        for (int gr = 0; gr < g.sp_ng; gr++) bytes += g.sp_main_bytes[gr];
+        mbar_arrive_expect_tx(bar, bytes);
+        tma_issue_line_spinor(m, g, c, d, dst, bar);
+        return;
+    }
+    mbar_arrive_expect_tx(bar, g.lk_main_bytes + (d == 5 ? g.lk_row_bytes : 0u));
+    tma_issue_link(m, g, c, d, dst + g.off_lk_main, bar);
+    if (d == 5) tma_issue_link_row(m, g, c, dst + g.off_lk_row, bar);
+}
+
+// waits for the full barriers of the last min(issued, n) stages of a ring
+__device__ __forceinline__ void tma_drain(uint32_t full_bar, long issued, int n) {
+    const long first = issued > n ? issued - n : 0;
+    for (long s = first; s < issued; s++) {
+        const int bb = (int)(s % n);
+        const uint32_t par = (uint32_t)(s / n) & 1;
+        if (!mbar_wait(full_bar + 8u * bb, par, kDrainLimitNs, nullptr)) atomicExch(&g_tma_status, 1);
+    }
+}
+
+// the xpay / scale epilogue and the store of one output site
+template <class SIO, bool XPAY, class R>
+__device__ __forceinline__ void tma_epilogue(const TmaGeom &g, const TileCoord &c, int xh, int y, cx<R> acc[12]) {
+    const R aup = (R)g.a_up, alow = (R)g.a_low;
+    const long h = xh + (long)g.L0h * (y + (long)g.L1 * c.zt);
+    void *out = (g.full && c.p == 1) ? g.out1 : g.out0;
+    if (XPAY) {
+        cx<R> xv[12];
+        SIO::load(g.x, g.Vh, h, xv);
+        const R bb = (R)g.b;
+#pragma unroll
+        for (int e = 0; e < 12; e++) {
+            const R ak = e < 6 ? aup : alow;
+            acc[e] = {fma(ak, acc[e].re, bb * xv[e].re), fma(ak, acc[e].im, bb * xv[e].im)};
+        }
+    } else {
+#pragma unroll
+        for (int e = 6; e < 12; e++) acc[e] = {alow * acc[e].re, alow * acc[e].im};
+#pragma unroll
+        for (int e = 0; e < 6; e++) acc[e] = {aup * acc[e].re, aup * acc[e].im};
+    }
+    SIO::store(out, g.Vh, h, acc);
+}
+
 template <class SIO, class LIO, bool XPAY>
 __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ TmaMaps m,
                                                         const __grid_constant__ TmaGeom g) {
@@ -349,7 +516,6 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
     const int own = j * L0h + xh;
     const int SM = g.NY * L0h;  // plane stride of an NY-row box, in elements
     const R sg = (R)g.g5_in;
-    const R aup = (R)g.a_up, alow = (R)g.a_low;
     int b = 0;
     uint32_t k = 0;
     for (int it = 0; it < nmine; it++) {
@@ -403,24 +569,199 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
                 k++;
             }
         }
-        const long h = xh + (long)L0h * (y + (long)g.L1 * c.zt);
-        void *out = (g.full && c.p == 1) ? g.out1 : g.out0;
-        if (XPAY) {
-            cx<R> xv[12];
-            SIO::load(g.x, g.Vh, h, xv);
-            const R bb = (R)g.b;
-#pragma unroll
-            for (int e = 0; e < 12; e++) {
-                const R ak = e < 6 ? aup : alow;
-                acc[e] = {fma(ak, acc[e].re, bb * xv[e].re), fma(ak, acc[e].im, bb * xv[e].im)};
-            }
-        } else {
-#pragma unroll
-            for (int e = 6; e < 12; e++) acc[e] = {alow * acc[e].re, alow * acc[e].im};
-#pragma unroll
-            for (int e = 0; e < 6; e++) acc[e] = {aup * acc[e].re, aup * acc[e].im};
+        tma_epilogue<SIO, XPAY, R>(g, c, xh, y, acc);
+    }
+}
+
+
+// Shared own-line kernel (stage tables above tma_issue_xy_a; SPLIT: one box
+// per stage). Shared memory: [nstage_a A buffers][nstage B buffers][A full |
+// A empty | B full | B empty barriers]. Bounded waits and the drain as in
+// k_dslash_tma. A consumer warp releases the A buffer after its last read
+// of the own-line rows (direction 5), a B buffer after its last read of it.
+template <class SIO, class LIO, bool XPAY, bool SPLIT>
+__global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant__ TmaMaps m,
+                                                           const __grid_constant__ TmaGeom g) {
+    using R = typename SIO::real;
+    constexpr int kStages = SPLIT ? 12 : 6;  // B stages per tile
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ int s_abort;
+    const uint32_t raw = smem_addr(smem_raw);
+    const uint32_t pad = ((raw + 127u) & ~127u) - raw;
+    const uint8_t *sbase = smem_raw + pad;
+    const uint32_t base = raw + pad;
+    const int nA = g.nstage_a, nB = g.nstage;
+    const uint32_t b_base = base + (uint32_t)nA * g.a_bytes;
+    const uint32_t fullA = b_base + (uint32_t)nB * g.stage_bytes;
+    const uint32_t emptyA = fullA + 8u * nA;
+    const uint32_t fullB = emptyA + 8u * nA;
+    const uint32_t emptyB = fullB + 8u * nB;
+    const int bid = blockIdx.x;
+    const int nmine = bid < g.nitems ? (g.nitems - 1 - bid) / (int)gridDim.x + 1 : 0;
+    const int nthr_c = g.ncw * 32;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_abort = 0;
+        for (int b = 0; b < nA; b++) {
+            mbar_init(fullA + 8u * b, 1);
+            mbar_init(emptyA + 8u * b, (uint32_t)g.ncw);
         }
-        SIO::store(out, g.Vh, h, acc);
+        for (int b = 0; b < nB; b++) {
+            mbar_init(fullB + 8u * b, 1);
+            mbar_init(emptyB + 8u * b, (uint32_t)g.ncw);
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (nmine == 0) return;
+    volatile int *abort = &s_abort;
+
+    if (tid >= nthr_c) {
+        // producer warp, lane 0: per tile the A stage, then the B stages
+        if (tid != nthr_c) return;
+        tma_prefetch_map(&m.lk_main);
+        int a = 0, b = 0;
+        uint32_t ka = 0, kb = 0;
+        long na = 0, nb = 0;
+        bool ok = true;
+        for (int it = 0; it < nmine && ok; it++) {
+            const TileCoord c = tile_coord(g, bid + it * (int)gridDim.x);
+            if (!mbar_wait(emptyA + 8u * a, (ka + 1) & 1, kWaitLimitNs, abort)) {
+                ok = false;
+                break;
+            }
+            tma_issue_xy_a(m, g, c, base + (uint32_t)a * g.a_bytes, fullA + 8u * a);
+            na++;
+            if (++a == nA) {
+                a = 0;
+                ka++;
+            }
+#pragma unroll 1
+            for (int s = 0; s < kStages; s++) {
+                if (!mbar_wait(emptyB + 8u * b, (kb + 1) & 1, kWaitLimitNs, abort)) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t dst = b_base + (uint32_t)b * g.stage_bytes;
+                if (SPLIT)
+                    tma_issue_xy_split(m, g, c, s, dst, fullB + 8u * b);
+                else
+                    tma_issue_xy_b(m, g, c, s, dst, fullB + 8u * b);
+                nb++;
+                if (++b == nB) {
+                    b = 0;
+                    kb++;
+                }
+            }
+        }
+        if (!ok) {
+            *abort = 1;
+            atomicExch(&g_tma_status, 1);
+        }
+        // never leave with copies in flight
+        tma_drain(fullA, na, nA);
+        tma_drain(fullB, nb, nB);
+        return;
+    }
+
+    // consumers: thread (row j, half-x xh) of the tile
+    const int L0h = g.L0h;
+    const int j = tid / L0h, xh = tid - j * L0h;
+    const int own = j * L0h + xh;
+    const int SM = g.NY * L0h;  // plane stride of an NY-row box, in elements
+    const R sg = (R)g.g5_in;
+    const bool top = j + 1 == g.NY, bottom = j == 0;
+    int a = 0, b = 0;
+    uint32_t ka = 0, kb = 0;
+    for (int it = 0; it < nmine; it++) {
+        const TileCoord c = tile_coord(g, bid + it * (int)gridDim.x);
+        const int y = c.y0 + j;
+        const int x = 2 * xh + ((y + c.z + c.t + c.p) & 1);
+        const int xph = ((x + 1 == g.L0) ? 0 : x + 1) >> 1;
+        const int xmh = ((x == 0) ? g.L0 - 1 : x - 1) >> 1;
+        cx<R> acc[12];
+#pragma unroll
+        for (int e = 0; e < 12; e++) acc[e] = {R(0), R(0)};
+        if (!mbar_wait(fullA + 8u * a, ka & 1, kWaitLimitNs, abort)) {
+            *abort = 1;
+            atomicExch(&g_tma_status, 1);
+            return;
+        }
+        const uint8_t *sa = sbase + (size_t)a * g.a_bytes;
+        const uint8_t *sps = nullptr;  // split: the spinor stage waiting for its link stage
+        int bsp = 0;
+#pragma unroll
+        for (int s = 0; s < kStages; s++) {
+            if (!mbar_wait(fullB + 8u * b, kb & 1, kWaitLimitNs, abort)) {
+                *abort = 1;
+                atomicExch(&g_tma_status, 1);
+                return;
+            }
+            const uint8_t *st = sbase + (size_t)nA * g.a_bytes + (size_t)b * g.stage_bytes;
+            // directions of this stage: d0 (and d0 + 1 for a two-link stage)
+            const bool pair = !SPLIT && (s == 0 || s == 3);
+            const int d0 = SPLIT ? split_dir(s) : (s == 0 ? 0 : (s == 3 ? 4 : (s < 3 ? s + 1 : s + 2)));
+            if (SPLIT && split_is_spinor(s)) {
+                sps = st;
+                bsp = b;
+            } else {
+#pragma unroll
+                for (int k = 0; k < (pair ? 2 : 1); k++) {
+                    const int d = d0 + k;
+                    cx<R> sv[12], U[9];
+                    R n;
+                    // the link of a pair's second direction is the second box
+                    const uint8_t *lk = st + (pair && k == 1 ? g.off_lk2 : g.off_lk_main);
+                    int rel2 = -1;  // split: the spinor stage's buffer, released with this one
+                    if (d == 0 || d == 4) {
+                        // x: neighbour in the same row; the backward link sits there too
+                        const int si = own - xh + (d == 0 ? xph : xmh);
+                        TmaSpinor<SIO>::load(sa + g.off_a_main[0], sa + g.off_a_main[1], si, SM, sv, n);
+                        TmaLink<LIO>::load(lk, d == 0 ? own : si, SM, U);
+                    } else if (d == 1 || d == 5) {
+                        // y: the row above / below, across the tile edge from the
+                        // extra rows; the backward link of row 0 is the link row
+                        const bool fwd = d == 1;
+                        const bool edge = fwd ? top : bottom;
+                        const uint32_t so0 = edge ? (fwd ? g.off_a_hi[0] : g.off_a_lo[0]) : g.off_a_main[0];
+                        const uint32_t so1 = edge ? (fwd ? g.off_a_hi[1] : g.off_a_lo[1]) : g.off_a_main[1];
+                        const int syi = edge ? xh : (fwd ? own + L0h : own - L0h);
+                        TmaSpinor<SIO>::load(sa + so0, sa + so1, syi, edge ? L0h : SM, sv, n);
+                        if (fwd)
+                            TmaLink<LIO>::load(lk, own, SM, U);
+                        else if (edge)
+                            TmaLink<LIO>::load(st + g.off_lk_row, xh, L0h, U);
+                        else
+                            TmaLink<LIO>::load(lk, own - L0h, SM, U);
+                    } else {
+                        // z / t: the neighbour line's rows
+                        const uint8_t *sp = SPLIT ? sps : st;
+                        TmaSpinor<SIO>::load(sp + g.off_sp_main[0], sp + g.off_sp_main[1], own, SM, sv, n);
+                        TmaLink<LIO>::load(lk, own, SM, U);
+                        if (SPLIT) rel2 = bsp;
+                    }
+                    if (!pair || k == 1) {
+                        // the values are in registers: release the buffers
+                        __syncwarp();
+                        if ((tid & 31) == 0) {
+                            mbar_arrive(emptyB + 8u * b);
+                            if (rel2 >= 0) mbar_arrive(emptyB + 8u * rel2);
+                            if (d == 5) mbar_arrive(emptyA + 8u * a);  // last use of the own-line rows
+                        }
+                    }
+                    compute_dir_n<false, SIO::kScaled, R>(d, acc, sv, U, sg, n);
+                }
+            }
+            if (++b == nB) {
+                b = 0;
+                kb++;
+            }
+        }
+        if (++a == nA) {
+            a = 0;
+            ka++;
+        }
+        tma_epilogue<SIO, XPAY, R>(g, c, xh, y, acc);
     }
 }
 
@@ -513,7 +854,9 @@ inline uint32_t round128(uint32_t v) { return (v + 127u) & ~127u; }
 
 template <class SIO, class LIO, bool XPAY>
 int launch_tma_t(cudaStream_t s, const dev::TmaMaps &m, const dev::TmaGeom &tg, int block, size_t smem) {
-    auto k = dev::k_dslash_tma<SIO, LIO, XPAY>;
+    auto k = !tg.nstage_a ? dev::k_dslash_tma<SIO, LIO, XPAY>
+             : tg.split   ? dev::k_dslash_tma_xy<SIO, LIO, XPAY, true>
+                          : dev::k_dslash_tma_xy<SIO, LIO, XPAY, false>;
     PLQCD_TRY(smem_optin((const void *)k, smem));
     int occ = 0;
     PLQCD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, block, smem));
@@ -559,6 +902,49 @@ StageLayout stage_layout(const TmaFormat &f, int L0h, int ny) {
     return l;
 }
 
+// layout of the shared own-line kernel: the A buffer holds the NY own-line
+// rows and the rows below and above the tile. A B buffer holds a link box
+// and either the neighbour spinor rows (z, t stages) or a second link box
+// and the link row (x / y stages) in the same place; split: the spinor rows,
+// or one link box and the link row.
+struct XyLayout {
+    uint32_t off_a_main[2] = {0, 0}, off_a_lo[2] = {0, 0}, off_a_hi[2] = {0, 0}, a_bytes = 0;
+    uint32_t off_sp_main[2] = {0, 0}, off_lk_main = 0, off_lk2 = 0, off_lk_row = 0, b_bytes = 0;
+};
+
+XyLayout xy_layout(const TmaFormat &f, const StageLayout &l, bool split) {
+    XyLayout x;
+    uint32_t off = 0;
+    auto take = [&](uint32_t n) {
+        const uint32_t o = off;
+        off += round128(n);
+        return o;
+    };
+    for (int gr = 0; gr < f.sp_ng; gr++) {
+        x.off_a_main[gr] = take(l.sp_main_bytes[gr]);
+        x.off_a_lo[gr] = take(l.sp_row_bytes[gr]);
+        x.off_a_hi[gr] = take(l.sp_row_bytes[gr]);
+    }
+    x.a_bytes = off;
+    off = 0;
+    if (!split) x.off_lk_main = take(l.lk_main_bytes);
+    const uint32_t second = off;
+    for (int gr = 0; gr < f.sp_ng; gr++) x.off_sp_main[gr] = take(l.sp_main_bytes[gr]);
+    const uint32_t end_sp = off;
+    off = second;
+    if (split)
+        x.off_lk_main = take(l.lk_main_bytes);
+    else
+        x.off_lk2 = take(l.lk_main_bytes);
+    x.off_lk_row = take(l.lk_row_bytes);
+    x.b_bytes = end_sp > off ? end_sp : off;
+    return x;
+}
+
+// kind of a TMA variant -> A buffers (0: the per-direction kernel) and form
+inline int kind_a_buffers(int kind) { return kind <= 1 ? 0 : (kind <= 3 ? kind - 1 : kind - 3); }
+inline bool kind_split(int kind) { return kind >= 4; }
+
 // a row of eb-byte elements must be a whole number of 16-byte units (tile
 // loads) and at most 256 words
 bool row_ok(int L0h, int eb) {
@@ -568,17 +954,27 @@ bool row_ok(int L0h, int eb) {
 
 }  // namespace
 
-int dslash_tma_plan(const Geom &g, int prec, int recon, int nstage, int ny, int *block, size_t *smem) {
+int dslash_tma_plan(const Geom &g, int prec, int recon, int kind, int nstage, int ny, int *block, size_t *smem) {
     TmaFormat f;
     if (!tma_format(prec, recon, &f))
         return set_error(PLQCD_ERR_ARG, "dslash: no TMA kernel for precision/reconstruction %d/%d", prec, recon);
     bool rows = row_ok(g.L0h, f.lk_eb);
     for (int gr = 0; gr < f.sp_ng; gr++) rows = rows && row_ok(g.L0h, f.sp_eb[gr]);
-    if (nstage < 2 || nstage > 8 || ny < 1 || !rows || g.L[1] % ny || (ny * g.L0h) % 32 || ny * g.L0h > 256)
-        return set_error(PLQCD_ERR_ARG, "dslash: TMA tile %d rows x %d stages does not fit %dx%dx%dx%d", ny, nstage,
-                         g.L[0], g.L[1], g.L[2], g.L[3]);
+    // kind 1: one stage per direction (a ring of at least 2); 2, 3: own-line
+    // rows in 1 or 2 buffers of their own; 4, 5: the same with one box per
+    // stage (a spinor stage waits for the link stage after it: 2 at least)
+    const int min_stage = kind == 2 || kind == 3 ? 1 : 2;
+    if (kind < 1 || kind > 5 || nstage < min_stage || nstage > 8 || ny < 1 || !rows || g.L[1] % ny ||
+        (ny * g.L0h) % 32 || ny * g.L0h > 256)
+        return set_error(PLQCD_ERR_ARG, "dslash: TMA tile %d rows x %d stages (kind %d) does not fit %dx%dx%dx%d", ny,
+                         nstage, kind, g.L[0], g.L[1], g.L[2], g.L[3]);
     const StageLayout l = stage_layout(f, g.L0h, ny);
-    const size_t bytes = (size_t)nstage * l.bytes + 16u * nstage + 128;
+    size_t bytes = (size_t)nstage * l.bytes + 16u * nstage + 128;
+    if (kind > 1) {
+        const XyLayout x = xy_layout(f, l, kind_split(kind));
+        const int na = kind_a_buffers(kind);
+        bytes = (size_t)na * x.a_bytes + (size_t)nstage * x.b_bytes + 16u * (na + nstage) + 128;
+    }
     if (bytes > 227u * 1024 - 64) return set_error(PLQCD_ERR_ARG, "dslash: TMA ring of %zu bytes too large", bytes);
     if (block) *block = ny * g.L0h + 32;
     if (smem) *smem = bytes;
@@ -586,10 +982,10 @@ int dslash_tma_plan(const Geom &g, int prec, int recon, int nstage, int ny, int 
 }
 
 int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, int prec, int recon, bool full,
-                      bool xpay, int nstage, int ny) {
+                      bool xpay, int kind, int nstage, int ny) {
     int block = 0;
     size_t smem = 0;
-    PLQCD_TRY(dslash_tma_plan(g, prec, recon, nstage, ny, &block, &smem));
+    PLQCD_TRY(dslash_tma_plan(g, prec, recon, kind, nstage, ny, &block, &smem));
     // whole t-slices of one field (all of them for the full lattice)
     const long S = (long)g.L0h * g.L[1] * g.L[2];
     if (a.nrhs != 1 || (full && xpay) || a.h_begin % S || (a.h_end - a.h_begin) % S ||
@@ -643,6 +1039,22 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     tg.off_lk_main = lay.off_lk_main;
     tg.off_lk_row = lay.off_lk_row;
     tg.stage_bytes = lay.bytes;
+    if (kind > 1) {
+        const XyLayout xl = xy_layout(fmt, lay, kind_split(kind));
+        tg.nstage_a = kind_a_buffers(kind);
+        tg.split = kind_split(kind) ? 1 : 0;
+        tg.a_bytes = xl.a_bytes;
+        for (int gr = 0; gr < 2; gr++) {
+            tg.off_a_main[gr] = xl.off_a_main[gr];
+            tg.off_a_lo[gr] = xl.off_a_lo[gr];
+            tg.off_a_hi[gr] = xl.off_a_hi[gr];
+            tg.off_sp_main[gr] = xl.off_sp_main[gr];
+        }
+        tg.off_lk_main = xl.off_lk_main;
+        tg.off_lk2 = xl.off_lk2;
+        tg.off_lk_row = xl.off_lk_row;
+        tg.stage_bytes = xl.b_bytes;
+    }
     tg.a_up = a.a_up;
     tg.a_low = a.a_low;
     tg.b = a.b;

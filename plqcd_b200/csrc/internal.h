@@ -129,10 +129,13 @@ struct DslashCall {
     int nrhs = 1;
 };
 int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c);
-// TMA-staged hop (dslash_tma.cu): variant 1000 + 100 * nstage + ny selects
-// nstage shared-memory buffers and ny rows per tile. `plan` checks that the
-// configuration exists for this lattice and format and gives block / bytes.
-int dslash_tma_plan(const Geom &g, int prec, int recon, int nstage, int ny, int *block, size_t *smem);
+// TMA-staged hop (dslash_tma.cu): variant 1000 * kind + 100 * nstage + ny
+// selects the kernel (kind 1: one stage per direction; 2, 3: own-line rows
+// staged once per tile, in 1 or 2 buffers of their own; 4, 5: the same with
+// one tile-load box per ring stage), nstage ring buffers and ny rows per
+// tile. `plan` checks that the configuration exists for this lattice and
+// format and gives block / bytes.
+int dslash_tma_plan(const Geom &g, int prec, int recon, int kind, int nstage, int ny, int *block, size_t *smem);
 // the device flag a TMA stage wait sets when it runs out (reset: clear it)
 int dslash_tma_status(bool reset);
 // variant 0: direct loads, 2/3: cp.async pipeline depth; no tuning

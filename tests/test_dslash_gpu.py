@@ -507,9 +507,16 @@ def test_dslash_every_load_strategy(cuda, monkeypatch, variant, block, prec, rec
     assert relmax(got, want) <= tol
 
 
-# TMA-staged kernel: variant 1000 + 100 * ring depth + rows per tile
+# TMA-staged kernels: variant 1000 * kind + 100 * ring depth + rows per tile;
+# kind 1 stages every direction on its own, kinds 2-5 stage the own-line rows
+# once per tile (2, 3: in 1 or 2 buffers of their own; 4, 5: the same with
+# one tile-load box per ring stage)
 TMA_CASES = [((16, 8, 4, 6), 1204), ((16, 8, 4, 6), 1308), ((16, 8, 6, 4), 1404), ((32, 8, 4, 4), 1602),
-             ((8, 8, 4, 4), 1208), ((32, 16, 4, 2), 1216)]
+             ((8, 8, 4, 4), 1208), ((32, 16, 4, 2), 1216),
+             ((16, 8, 4, 6), 2104), ((16, 8, 4, 6), 2208), ((16, 8, 6, 4), 3204), ((32, 8, 4, 4), 2302),
+             ((8, 8, 4, 4), 3108), ((32, 16, 4, 2), 2116), ((16, 4, 4, 4), 2404),
+             ((16, 8, 4, 6), 4204), ((16, 8, 4, 6), 4308), ((16, 8, 6, 4), 5204), ((32, 8, 4, 4), 4602),
+             ((8, 8, 4, 4), 5308), ((16, 4, 4, 4), 4404)]
 
 
 @pytest.mark.parametrize("L,variant", TMA_CASES)
@@ -571,16 +578,16 @@ def test_tma_kernel_rejects_misfit_tiles(cuda, monkeypatch):
     lat, g64, u = _device_setup((6, 4, 6, 10), 45)
     bs = lat.spinor_bytes(P.F64)
     a, o = dev_bytes(bs), dev_bytes(bs)
-    for v in ("1408", "1203"):
+    for v in ("1408", "1203", "2203", "3008", "4104", "6204"):
         monkeypatch.setenv("PLQCD_DSLASH_STAGES", v)
         with pytest.raises(P.PlqcdError):
             lat.dslash(g64, o, a, 0, P.F64)
 
 
 def test_tma_kernel_bit_identical_at_benchmark_size(cuda, monkeypatch):
-    """At the benchmark lattice (32^3x64) the TMA configuration the tuner
-    picks there (2 stages x 4 rows, blocked tile order) gives the same bits
-    as the cp.async kernel for the full lattice and for one parity."""
+    """At the benchmark lattice (32^3x64) the TMA configurations the tuner
+    picks among there (blocked tile order) give the same bits as the
+    cp.async kernel for the full lattice and for one parity."""
     L = (32, 32, 32, 64)
     lat = new_lattice(L)
     g64 = P.Gauge(lat, P.F64, 18)
@@ -590,7 +597,8 @@ def test_tma_kernel_bit_identical_at_benchmark_size(cuda, monkeypatch):
     lat.spinor_gaussian(fe, P.F64, 0, 11)
     lat.spinor_gaussian(fo, P.F64, 1, 12)
     outs = {}
-    for v in ("2", "1204"):
+    variants = ("1204", "2204", "4304")
+    for v in ("2",) + variants:
         monkeypatch.setenv("PLQCD_DSLASH_STAGES", v)
         monkeypatch.setenv("PLQCD_DSLASH_BLOCK", "64")
         oe, oo, o1 = dev_bytes(bs), dev_bytes(bs), dev_bytes(bs)
@@ -598,8 +606,9 @@ def test_tma_kernel_bit_identical_at_benchmark_size(cuda, monkeypatch):
         lat.dslash(g64, o1, fe, P.ODD, P.F64)
         lat.synchronize()
         outs[v] = (oe, oo, o1)
-    for a, b in zip(outs["2"], outs["1204"]):
-        assert bool((a == b).all())
+    for v in variants:
+        for a, b in zip(outs["2"], outs[v]):
+            assert bool((a == b).all()), v
 
 
 @pytest.mark.parametrize("variant", ["intrin_256", "intrin_512", "single_mic", "single_mic_short"])
@@ -648,7 +657,7 @@ def test_misaligned_fields_are_refused(cuda):
     lat.synchronize()
 
 
-@pytest.mark.parametrize("variant", ["1204", "1308"])
+@pytest.mark.parametrize("variant", ["1204", "1308", "2204", "3104", "4304"])
 def test_tma_kernel_on_whole_slice_ranges(cuda, monkeypatch, variant):
     """On a site range of whole t-slices (a slab interior, a pipeline chunk)
     the TMA kernel writes the same bits as the gather kernel on that range
