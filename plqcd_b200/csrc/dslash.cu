@@ -246,8 +246,10 @@ static int launch_pipe(const Geom &g, cudaStream_t s, const DslashArgs &a, int b
 // direct loads, the direction loops of both sites interleaved: twice the
 // independent loads in flight per thread and shared index arithmetic, for
 // the 32- and 16-bit formats whose kernels are latency / issue bound.
+// PACK: the two sites are the two lanes of packed FP32 instructions (f2),
+// which halves the arithmetic instructions and gives the same bits.
 // Single parity only (RHS blocks allowed), no bug-compatible mode.
-template <class SIO, class LIO, bool XPAY>
+template <class SIO, class LIO, bool XPAY, bool PACK>
 __global__ void __launch_bounds__(256) k_dslash_spt2(const DslashArgs a) {
     using R = typename SIO::real;
     constexpr int S = 2;
@@ -283,24 +285,55 @@ __global__ void __launch_bounds__(256) k_dslash_spt2(const DslashArgs a) {
     if (!ok[0]) return;
     const R sg = (R)a.g5_in;
     cx<R> acc[S][12];
+    if constexpr (PACK) {
+        static_assert(S == 2, "one site per lane");
+        cx<f2> acc2[12];
 #pragma unroll
-    for (int j = 0; j < S; j++)
+        for (int k = 0; k < 12; k++) acc2[k] = {f2(0.f), f2(0.f)};
+        const f2 sg2(sg);
 #pragma unroll
-        for (int k = 0; k < 12; k++) acc[j][k] = {R(0), R(0)};
+        for (int d = 0; d < 8; d++) {
+            cx<R> s[S][12], U[S][9];
+            R n[S];
 #pragma unroll
-    for (int d = 0; d < 8; d++) {
-        cx<R> s[S][12], U[S][9];
-        R n[S];
+            for (int j = 0; j < S; j++) {
+                SIO::load_raw(in, Vh, nb[j][d], s[j], n[j]);
+                if (d < 4)
+                    LIO::load(a.gauge, Vh, par, d, hs[j], U[j]);
+                else
+                    LIO::load(a.gauge, Vh, opp, d - 4, nb[j][d], U[j]);
+            }
+            cx<f2> s2[12], U2[9];
 #pragma unroll
-        for (int j = 0; j < S; j++) {
-            SIO::load_raw(in, Vh, nb[j][d], s[j], n[j]);
-            if (d < 4)
-                LIO::load(a.gauge, Vh, par, d, hs[j], U[j]);
-            else
-                LIO::load(a.gauge, Vh, opp, d - 4, nb[j][d], U[j]);
+            for (int k = 0; k < 12; k++) s2[k] = zip(s[0][k], s[1][k]);
+#pragma unroll
+            for (int k = 0; k < 9; k++) U2[k] = zip(U[0][k], U[1][k]);
+            compute_dir_n<false, SIO::kScaled, f2>(d, acc2, s2, U2, sg2, f2(n[0], n[1]));
         }
 #pragma unroll
-        for (int j = 0; j < S; j++) compute_dir_n<false, SIO::kScaled, R>(d, acc[j], s[j], U[j], sg, n[j]);
+        for (int j = 0; j < S; j++)
+#pragma unroll
+            for (int k = 0; k < 12; k++) acc[j][k] = lane(acc2[k], j);
+    } else {
+#pragma unroll
+        for (int j = 0; j < S; j++)
+#pragma unroll
+            for (int k = 0; k < 12; k++) acc[j][k] = {R(0), R(0)};
+#pragma unroll
+        for (int d = 0; d < 8; d++) {
+            cx<R> s[S][12], U[S][9];
+            R n[S];
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                SIO::load_raw(in, Vh, nb[j][d], s[j], n[j]);
+                if (d < 4)
+                    LIO::load(a.gauge, Vh, par, d, hs[j], U[j]);
+                else
+                    LIO::load(a.gauge, Vh, opp, d - 4, nb[j][d], U[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < S; j++) compute_dir_n<false, SIO::kScaled, R>(d, acc[j], s[j], U[j], sg, n[j]);
+        }
     }
     const R aup = (R)a.a_up, alow = (R)a.a_low;
 #pragma unroll
@@ -330,23 +363,27 @@ template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
 static int launch_direct(const Geom &g, cudaStream_t s, const DslashArgs &a, int block);
 
 template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
-static int launch_spt2(const Geom &g, cudaStream_t s, const DslashArgs &a, int block) {
+static int launch_spt2(const Geom &g, cudaStream_t s, const DslashArgs &a, int block, bool pack) {
     if constexpr (COMPAT || FULL || std::is_same<typename SIO::real, double>::value) {
         return set_error(PLQCD_ERR_ARG, "dslash: two sites per thread exists for 32/16-bit single-parity calls");
     } else {
         const long nblk = (a.h_end - a.h_begin + 2L * block - 1) / (2L * block) * a.nrhs;
-        k_dslash_spt2<SIO, LIO, XPAY><<<(unsigned)nblk, block, 0, s>>>(a);
+        if (pack)
+            k_dslash_spt2<SIO, LIO, XPAY, true><<<(unsigned)nblk, block, 0, s>>>(a);
+        else
+            k_dslash_spt2<SIO, LIO, XPAY, false><<<(unsigned)nblk, block, 0, s>>>(a);
         PLQCD_CUDA_TRY(cudaGetLastError());
         return PLQCD_OK;
     }
 }
 
-// variant 0: direct loads; 2, 3: cp.async pipeline of that depth
+// variant 0: direct loads; 2, 3: cp.async pipeline of that depth; 12: two
+// sites per thread; 13: the same on packed FP32 lanes
 template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
 static int launch_t(const Geom &g, cudaStream_t s, const DslashArgs &a, int variant, int block) {
     if (variant == 2) return launch_pipe<SIO, LIO, 2, COMPAT, XPAY, FULL>(g, s, a, block);
     if (variant == 3) return launch_pipe<SIO, LIO, 3, COMPAT, XPAY, FULL>(g, s, a, block);
-    if (variant == 12) return launch_spt2<SIO, LIO, COMPAT, XPAY, FULL>(g, s, a, block);
+    if (variant == 12 || variant == 13) return launch_spt2<SIO, LIO, COMPAT, XPAY, FULL>(g, s, a, block, variant == 13);
     return launch_direct<SIO, LIO, COMPAT, XPAY, FULL>(g, s, a, block);
 }
 
@@ -473,8 +510,8 @@ static int tune_dslash(const Geom &g, cudaStream_t s, const DslashCall &c, const
     // thread) x block size
     std::vector<TuneResult> cands;
     const bool spt_ok = c.prec != PLQCD_F64 && !c.full && !(c.flags & PLQCD_DSLASH_COMPAT);
-    for (int v : {2, 0, 3, 12}) {
-        if (v == 12 && !spt_ok) continue;
+    for (int v : {2, 0, 3, 12, 13}) {
+        if (v >= 12 && !spt_ok) continue;
         for (int b : {64, 128, 256}) {
             TuneResult r;
             r.variant = v;

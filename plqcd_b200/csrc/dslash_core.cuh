@@ -29,6 +29,36 @@ struct DslashArgs {
     long fbytes;
 };
 
+// Two FP32 lanes in one register pair, each operation one packed sm_100
+// instruction (FFMA2 / FMUL2 / FADD2). Every lane is rounded exactly as the
+// scalar operation, so the arithmetic below computes, lane by lane, the
+// same bits as with R = float: two sites per thread, one per lane, take half
+// the FP32 instructions of two scalar threads.
+// (the operations are hidden friends: found for f2 arguments only, so they
+// do not hide the scalar fma of the other types)
+struct f2 {
+    float2 v;
+    f2() = default;
+    __device__ __forceinline__ explicit f2(float s) : v(make_float2(s, s)) {}
+    __device__ __forceinline__ f2(float a, float b) : v(make_float2(a, b)) {}
+    __device__ __forceinline__ explicit f2(float2 w) : v(w) {}
+    __device__ friend __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return f2(__ffma2_rn(a.v, b.v, c.v)); }
+    __device__ friend __forceinline__ f2 operator*(f2 a, f2 b) { return f2(__fmul2_rn(a.v, b.v)); }
+    __device__ friend __forceinline__ f2 operator+(f2 a, f2 b) { return f2(__fadd2_rn(a.v, b.v)); }
+    __device__ friend __forceinline__ f2 operator-(f2 a) { return f2(-a.v.x, -a.v.y); }
+    __device__ friend __forceinline__ f2 operator-(f2 a, f2 b) { return a + (-b); }
+    // sign factors (+-1, exact)
+    __device__ friend __forceinline__ f2 operator*(int s, f2 a) {
+        return s == 1 ? a : (s == -1 ? -a : f2((float)s) * a);
+    }
+};
+
+// lane pairing of per-site values
+__device__ __forceinline__ cx<f2> zip(cx<float> a, cx<float> b) { return {f2(a.re, b.re), f2(a.im, b.im)}; }
+__device__ __forceinline__ cx<float> lane(cx<f2> a, int j) {
+    return j == 0 ? cx<float>{a.re.v.x, a.im.v.x} : cx<float>{a.re.v.y, a.im.v.y};
+}
+
 // projection of the neighbour spinor onto the two upper spin components.
 // FWD: (1 - g_mu) psi(x+mu); backward: (1 + g_mu) psi(x-mu). `sg` is the
 // sign on the lower spins (backward and gamma5-on-input flip it).

@@ -474,16 +474,18 @@ def test_shipped_selftest(cuda):
     assert P.lib().plqcd_selftest(0, 1) == 0, P.last_error()
 
 
-@pytest.mark.parametrize("variant,block", [(0, 64), (2, 64), (2, 128), (3, 64), (12, 64), (12, 128)])
+@pytest.mark.parametrize("variant,block", [(0, 64), (2, 64), (2, 128), (3, 64), (12, 64), (12, 128), (13, 64),
+                                           (13, 128)])
 @pytest.mark.parametrize("prec,recon,tol", [(P.F64, 18, 1e-14), (P.F32, 12, 1e-6), (P.F16, 12, 1e-3),
                                             (P.BF16, 12, 1e-2)])
 def test_dslash_every_load_strategy(cuda, monkeypatch, variant, block, prec, recon, tol):
     """Each load strategy of the single-RHS kernel, forced past the tuner
-    (direct, cp.async pipeline depth 2/3, two sites per thread), matches the
+    (direct, cp.async pipeline depth 2/3, two sites per thread, also on
+    packed FP32 lanes), matches the
     FP64 oracle-checked kernel within the precision's tolerance, with the
     xpay and gamma5 epilogue and on a lattice whose half volume is not a
     multiple of the block."""
-    if variant == 12 and prec == P.F64:
+    if variant >= 12 and prec == P.F64:
         pytest.skip("two sites per thread is built for 32/16-bit formats")
     L = (6, 4, 6, 10)
     lat, g64, u = _device_setup(L, 41)
@@ -505,6 +507,35 @@ def test_dslash_every_load_strategy(cuda, monkeypatch, variant, block, prec, rec
     want = field_to_host(lat, ref, prec, 1)[lat.V // 2:]
     got = field_to_host(lat, o, prec, 1)[lat.V // 2:]
     assert relmax(got, want) <= tol
+
+
+@pytest.mark.parametrize("prec,recon", [(P.F32, 18), (P.F32, 12), (P.F16, 12), (P.BF16, 12)])
+def test_packed_lanes_bit_identical(cuda, monkeypatch, prec, recon):
+    """Two sites per thread on packed FP32 lanes (FFMA2, variant 13) round
+    every lane as the scalar arithmetic does: the outputs are the same
+    bits as the one-site cp.async kernel, for a plain hop and for the xpay /
+    gamma5 epilogue, on a lattice whose half volume leaves a ragged last tile."""
+    L = (6, 4, 6, 10)
+    lat, g64, u = _device_setup(L, 49)
+    g = P.Gauge(lat, prec, recon)
+    g.copy_from(g64)
+    bs = lat.spinor_bytes(prec)
+    a, x = dev_bytes(bs), dev_bytes(bs)
+    lat.spinor_gaussian(a, prec, 0, 15)
+    lat.spinor_gaussian(x, prec, 1, 16)
+    flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
+    outs = {}
+    for v, blk in (("2", "64"), ("12", "64"), ("13", "64"), ("13", "128"), ("13", "32")):
+        monkeypatch.setenv("PLQCD_DSLASH_STAGES", v)
+        monkeypatch.setenv("PLQCD_DSLASH_BLOCK", blk)
+        o1, o2 = dev_bytes(bs), dev_bytes(bs)
+        lat.dslash(g, o1, a, 1, prec)
+        lat.dslash_xpay(g, o2, a, 1, prec, 0.25, x, -2.0, flags)
+        lat.synchronize()
+        outs[v + "/" + blk] = (o1, o2)
+    ref = outs["2/64"]
+    for k, (o1, o2) in outs.items():
+        assert bool((o1 == ref[0]).all()) and bool((o2 == ref[1]).all()), k
 
 
 # TMA-staged kernels: variant 1000 * kind + 100 * ring depth + rows per tile;
