@@ -104,13 +104,14 @@ __global__ void __launch_bounds__(256) k_dslash(const DslashArgs a) {
 #pragma unroll
     for (int k = 0; k < 12; k++) acc[k] = {R(0), R(0)};
 
+    // the order of dir_at: x+, x-, y+, y-, z+, z-, t+, t-
     hop_dir<SIO, LIO, 0, true, COMPAT>(acc, in, a.gauge, Vh, h_xp, fpar, h, sg);
-    hop_dir<SIO, LIO, 1, true, COMPAT>(acc, in, a.gauge, Vh, h_yp, fpar, h, sg);
-    hop_dir<SIO, LIO, 2, true, COMPAT>(acc, in, a.gauge, Vh, h_zp, fpar, h, sg);
-    hop_dir<SIO, LIO, 3, true, COMPAT>(acc, in, a.gauge, Vh, h_tp, fpar, h, sg);
     hop_dir<SIO, LIO, 0, false, COMPAT>(acc, in, a.gauge, Vh, h_xm, opp, h_xm, sg);
+    hop_dir<SIO, LIO, 1, true, COMPAT>(acc, in, a.gauge, Vh, h_yp, fpar, h, sg);
     hop_dir<SIO, LIO, 1, false, COMPAT>(acc, in, a.gauge, Vh, h_ym, opp, h_ym, sg);
+    hop_dir<SIO, LIO, 2, true, COMPAT>(acc, in, a.gauge, Vh, h_zp, fpar, h, sg);
     hop_dir<SIO, LIO, 2, false, COMPAT>(acc, in, a.gauge, Vh, h_zm, opp, h_zm, sg);
+    hop_dir<SIO, LIO, 3, true, COMPAT>(acc, in, a.gauge, Vh, h_tp, fpar, h, sg);
     hop_dir<SIO, LIO, 3, false, COMPAT>(acc, in, a.gauge, Vh, h_tm, opp, h_tm, sg);
 
     const R aup = (R)a.a_up, alow = (R)a.a_low;
@@ -178,8 +179,10 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
 
     const int stride = B * 16;  // bytes between consecutive slots of one thread
     const uint32_t s_thread = smem_addr(smem) + threadIdx.x * 16;
-    auto issue = [&](int d) {
-        const uint32_t s0 = s_thread + (uint32_t)((d % ST) * NS) * stride;
+    // k-th direction of dir_at into slot k % ST
+    auto issue = [&](int k) {
+        const int d = dir_at(k);
+        const uint32_t s0 = s_thread + (uint32_t)((k % ST) * NS) * stride;
         SIO::issue(in, Vh, nb[d], s0, stride);
         if (d < 4)
             LIO::issue(a.gauge, Vh, fpar, d, h, s0 + SIO::NSLOT * stride, stride);
@@ -187,8 +190,8 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
             LIO::issue(a.gauge, Vh, opp, d - 4, nb[d], s0 + SIO::NSLOT * stride, stride);
     };
 #pragma unroll
-    for (int d = 0; d < ST; d++) {
-        issue(d);
+    for (int k = 0; k < ST; k++) {
+        issue(k);
         cp_async_commit();
     }
     cx<R> acc[12];
@@ -196,16 +199,16 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
     for (int k = 0; k < 12; k++) acc[k] = {R(0), R(0)};
     const R sg = (R)a.g5_in;
 #pragma unroll
-    for (int d = 0; d < 8; d++) {
+    for (int k = 0; k < 8; k++) {
         cp_async_wait<ST - 1>();
-        const uint4 *s0 = smem + threadIdx.x + (d % ST) * NS * B;
+        const uint4 *s0 = smem + threadIdx.x + (k % ST) * NS * B;
         cx<R> s[12], U[9];
         R n;
         SIO::load_staged_raw(s0, B, s, n);
         LIO::load_staged(s0 + SIO::NSLOT * B, B, U);
-        compute_dir_n<COMPAT, SIO::kScaled, R>(d, acc, s, U, sg, n);
+        compute_dir_n<COMPAT, SIO::kScaled, R>(dir_at(k), acc, s, U, sg, n);
         // the slot just consumed is refilled only after its values were used
-        if (d + ST < 8) issue(d + ST);
+        if (k + ST < 8) issue(k + ST);
         cp_async_commit();
     }
 
@@ -292,7 +295,8 @@ __global__ void __launch_bounds__(256) k_dslash_spt2(const DslashArgs a) {
         for (int k = 0; k < 12; k++) acc2[k] = {f2(0.f), f2(0.f)};
         const f2 sg2(sg);
 #pragma unroll
-        for (int d = 0; d < 8; d++) {
+        for (int k = 0; k < 8; k++) {
+            const int d = dir_at(k);
             cx<R> s[S][12], U[S][9];
             R n[S];
 #pragma unroll
@@ -320,7 +324,8 @@ __global__ void __launch_bounds__(256) k_dslash_spt2(const DslashArgs a) {
 #pragma unroll
             for (int k = 0; k < 12; k++) acc[j][k] = {R(0), R(0)};
 #pragma unroll
-        for (int d = 0; d < 8; d++) {
+        for (int k = 0; k < 8; k++) {
+            const int d = dir_at(k);
             cx<R> s[S][12], U[S][9];
             R n[S];
 #pragma unroll

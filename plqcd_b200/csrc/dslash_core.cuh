@@ -194,6 +194,13 @@ __device__ __forceinline__ void compute_dir(cx<R> acc[12], const cx<R> s[12], co
     accumulate<MU, FWD ? 1 : -1, !(COMPAT && FWD), SC, R>(acc, c0, c1, n);
 }
 
+// Accumulation order of the eight directions in every kernel: x+, x-, y+,
+// y-, z+, z-, t+, t- (d = 0..3 forward mu, 4..7 backward mu). Forward and
+// backward terms of one axis read the same rows and links of the other
+// parity, so the row-staging kernels consume them back to back; all
+// kernels add in this order and give the same bits.
+__host__ __device__ constexpr int dir_at(int k) { return (k & 1) ? 4 + (k >> 1) : (k >> 1); }
+
 template <bool COMPAT, bool SC, typename R>
 __device__ __forceinline__ void compute_dir_n(int d, cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg,
                                               R n) {

@@ -71,7 +71,8 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs(const MrhsArgs a) {
         for (int k = 0; k < 12; k++) acc[r][k] = {R(0), R(0)};
 
 #pragma unroll
-    for (int d = 0; d < 8; d++) {
+    for (int k = 0; k < 8; k++) {
+        const int d = dir_at(k);
         cx<R> U[9];
         if (d < 4)
             LIO::load(a.gauge, Vh, par, d, h, U);
@@ -148,8 +149,10 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
 
     const int stride = B * 16;
     const uint32_t s_thread = smem_addr(smem) + threadIdx.x * 16;
-    auto issue = [&](int d) {
-        const uint32_t s0 = s_thread + (uint32_t)((d % ST) * NS) * stride;
+    // k-th direction of dir_at into slot k % ST
+    auto issue = [&](int k) {
+        const int d = dir_at(k);
+        const uint32_t s0 = s_thread + (uint32_t)((k % ST) * NS) * stride;
         if (d < 4)
             LIO::issue(a.gauge, Vh, par, d, h, s0, stride);
         else
@@ -161,8 +164,8 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
                            s0 + (uint32_t)(LIO::NSLOT + r * SIO::NSLOT) * stride, stride);
     };
 #pragma unroll
-    for (int d = 0; d < ST; d++) {
-        issue(d);
+    for (int k = 0; k < ST; k++) {
+        issue(k);
         cp_async_commit();
     }
     cx<R> acc[NR][12];
@@ -171,9 +174,10 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
 #pragma unroll
         for (int k = 0; k < 12; k++) acc[r][k] = {R(0), R(0)};
 #pragma unroll
-    for (int d = 0; d < 8; d++) {
+    for (int k = 0; k < 8; k++) {
+        const int d = dir_at(k);
         cp_async_wait<ST - 1>();
-        const uint4 *s0 = smem + threadIdx.x + (d % ST) * NS * B;
+        const uint4 *s0 = smem + threadIdx.x + (k % ST) * NS * B;
         cx<R> U[9];
         LIO::load_staged(s0, B, U);
 #pragma unroll
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
             }
         }
         // the slot just consumed is refilled only after its values were used
-        if (d + ST < 8) issue(d + ST);
+        if (k + ST < 8) issue(k + ST);
         cp_async_commit();
     }
 

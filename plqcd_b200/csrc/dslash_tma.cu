@@ -18,8 +18,9 @@
 // are processed at the same time and a link read from HBM for one parity's
 // forward term serves the other's backward term from L2.
 //
-// Per tile the producer fills 8 stages, one per direction, in a ring of
-// `nstage` shared-memory buffers (full / empty mbarrier pairs):
+// Per tile the producer fills 8 stages, one per direction in the order of
+// dir_at (x+, x-, y+, ...), in a ring of `nstage` shared-memory buffers
+// (full / empty mbarrier pairs):
 //   x+, x-:  the tile's own rows of the input (the x neighbours sit in the
 //            same rows) and the mu=0 links (own parity / opposite parity);
 //   y+, y-:  own rows plus one extra row across the tile edge (y0+NY or
@@ -285,23 +286,25 @@ constexpr uint64_t kDrainLimitNs = 200000000ull;  // 0.2 s
 // ---- shared own-line variant ----------------------------------------------------
 // The x+-, y+- neighbours of a tile all sit in the own (z, t) line: rows
 // y0-1 .. y0+NY of the input. k_dslash_tma_xy stages them once per tile, in
-// a ring of their own, and keeps them while the four x / y directions are
-// computed; the link ring carries six stages per tile:
-//   0: U_0, U_1 forward (own parity, own rows)     -> directions 0, 1
-//   1: spinor line z+1 + U_2 forward               -> 2
-//   2: spinor line t+1 + U_3 forward               -> 3
-//   3: U_0, U_1 backward (opposite parity; U_1 also the row y0-1) -> 4, 5
-//   4: spinor line z-1 + U_2 at line z-1           -> 6
-//   5: spinor line t-1 + U_3 at line t-1           -> 7
+// a ring of their own, and keeps them while the four x / y directions (the
+// first four of the dir_at order) are computed; the link ring carries six
+// stages per tile:
+//   0: U_0 forward (own parity) + U_0 backward (opposite parity), own rows
+//                                                  -> x+, x-
+//   1: U_1 forward + U_1 backward (and its row y0-1) -> y+, y-
+//   2: spinor line z+1 + U_2 forward               -> z+
+//   3: spinor line z-1 + U_2 at line z-1           -> z-
+//   4: spinor line t+1 + U_3 forward               -> t+
+//   5: spinor line t-1 + U_3 at line t-1           -> t-
 // The split form carries one box per stage (12 stages per tile, buffers
 // about half the size, so more tiles fit on an SM):
-//   0: U_0 fwd  1: U_1 fwd  2: spinor z+1  3: U_2 fwd  4: spinor t+1
-//   5: U_3 fwd  6: U_0 bwd  7: U_1 bwd (+ row y0-1)  8: spinor z-1
-//   9: U_2 at z-1  10: spinor t-1  11: U_3 at t-1
+//   0: U_0 fwd  1: U_0 bwd  2: U_1 fwd  3: U_1 bwd (+ row y0-1)
+//   4: spinor z+1  5: U_2 fwd  6: spinor z-1  7: U_2 at z-1
+//   8: spinor t+1  9: U_3 fwd  10: spinor t-1  11: U_3 at t-1
 // and a spinor stage is kept until the link stage after it has arrived.
-// Directions are accumulated in the same order 0..7 as in the other kernels,
-// so the results are the same bits. Per tile it stages NY+2 own-line rows
-// instead of 4 NY + 2.
+// Directions are accumulated in the order of the other kernels, so the
+// results are the same bits. Per tile it stages NY+2 own-line rows instead
+// of 4 NY + 2.
 
 // own-line rows of the input (y0-1 and y0+NY wrapped) into an A buffer
 __device__ __forceinline__ void tma_issue_xy_a(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, uint32_t dst,
@@ -371,15 +374,14 @@ __device__ __forceinline__ void tma_issue_link_row(const TmaMaps &m, const TmaGe
 // expected byte count is set before the loads are issued.
 __device__ __forceinline__ void tma_issue_xy_b(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, int s,
                                                uint32_t dst, uint32_t bar) {
-    if (s == 0 || s == 3) {
-        const int d0 = s == 0 ? 0 : 4;
-        mbar_arrive_expect_tx(bar, 2u * g.lk_main_bytes + (s == 3 ? g.lk_row_bytes : 0u));
-        tma_issue_link(m, g, c, d0, dst + g.off_lk_main, bar);
-        tma_issue_link(m, g, c, d0 + 1, dst + g.off_lk2, bar);
-        if (s == 3) tma_issue_link_row(m, g, c, dst + g.off_lk_row, bar);
+    if (s < 2) {  // forward and backward links of mu = s
+        mbar_arrive_expect_tx(bar, 2u * g.lk_main_bytes + (s == 1 ? g.lk_row_bytes : 0u));
+        tma_issue_link(m, g, c, s, dst + g.off_lk_main, bar);
+        tma_issue_link(m, g, c, s + 4, dst + g.off_lk2, bar);
+        if (s == 1) tma_issue_link_row(m, g, c, dst + g.off_lk_row, bar);
         return;
     }
-    const int d = s < 3 ? s + 1 : s + 2;  // 2, 3, 6, 7
+    const int d = dir_at(s + 2);  // z+, z-, t+, t-
     uint32_t bytes = g.lk_main_bytes;
     for (int gr = 0; gr < g.sp_ng; gr++) bytes += g.sp_main_bytes[gr];
     mbar_arrive_expect_tx(bar, bytes);
@@ -388,10 +390,15 @@ __device__ __forceinline__ void tma_issue_xy_b(const TmaMaps &m, const TmaGeom &
 }
 
 // direction served by split stage s (a spinor stage: that of the link stage after it)
-__host__ __device__ constexpr int split_dir(int s) {
-    return s < 2 ? s : (s < 6 ? (s >> 1) + 1 : (s < 8 ? s - 2 : (s >> 1) + 2));
-}
-__host__ __device__ constexpr bool split_is_spinor(int s) { return s == 2 || s == 4 || s == 8 || s == 10; }
+__host__ __device__ constexpr int split_dir(int s) { return s < 4 ? dir_at(s) : dir_at(4 + (s - 4) / 2); }
+__host__ __device__ constexpr bool split_is_spinor(int s) { return s >= 4 && !(s & 1); }
+static_assert(split_dir(0) == 0 && split_dir(1) == 4 && split_dir(2) == 1 && split_dir(3) == 5 &&
+                  split_dir(4) == 2 && split_dir(5) == 2 && split_dir(6) == 6 && split_dir(7) == 6 &&
+                  split_dir(8) == 3 && split_dir(9) == 3 && split_dir(10) == 7 && split_dir(11) == 7,
+              "split stage table");
+static_assert(dir_at(0) == 0 && dir_at(1) == 4 && dir_at(2) == 1 && dir_at(3) == 5 && dir_at(4) == 2 &&
+                  dir_at(5) == 6 && dir_at(6) == 3 && dir_at(7) == 7,
+              "accumulation order x+, x-, y+, y-, z+, z-, t+, t-");
 
 // split stage s (0..11) into a B buffer
 __device__ __forceinline__ void tma_issue_xy_split(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, int s,
@@ -482,13 +489,13 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
         for (int it = 0; it < nmine && ok; it++) {
             const TileCoord c = tile_coord(g, bid + it * (int)gridDim.x);
 #pragma unroll 1
-            for (int d = 0; d < 8; d++) {
+            for (int kd = 0; kd < 8; kd++) {
                 // the consumers released this buffer's previous use
                 if (!mbar_wait(empty_bar + 8u * b, (k + 1) & 1, kWaitLimitNs, abort)) {
                     ok = false;
                     break;
                 }
-                tma_issue_dir(m, g, c, d, base + (uint32_t)b * g.stage_bytes, full_bar + 8u * b);
+                tma_issue_dir(m, g, c, dir_at(kd), base + (uint32_t)b * g.stage_bytes, full_bar + 8u * b);
                 issued++;
                 if (++b == g.nstage) {
                     b = 0;
@@ -528,7 +535,8 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
 #pragma unroll
         for (int e = 0; e < 12; e++) acc[e] = {R(0), R(0)};
 #pragma unroll
-        for (int d = 0; d < 8; d++) {
+        for (int kd = 0; kd < 8; kd++) {
+            const int d = dir_at(kd);
             if (!mbar_wait(full_bar + 8u * b, k & 1, kWaitLimitNs, abort)) {
                 *abort = 1;
                 atomicExch(&g_tma_status, 1);
@@ -698,16 +706,16 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
                 return;
             }
             const uint8_t *st = sbase + (size_t)nA * g.a_bytes + (size_t)b * g.stage_bytes;
-            // directions of this stage: d0 (and d0 + 1 for a two-link stage)
-            const bool pair = !SPLIT && (s == 0 || s == 3);
-            const int d0 = SPLIT ? split_dir(s) : (s == 0 ? 0 : (s == 3 ? 4 : (s < 3 ? s + 1 : s + 2)));
+            // directions of this stage: one, or the forward and backward
+            // terms of x or y for a two-link stage
+            const bool pair = !SPLIT && s < 2;
             if (SPLIT && split_is_spinor(s)) {
                 sps = st;
                 bsp = b;
             } else {
 #pragma unroll
                 for (int k = 0; k < (pair ? 2 : 1); k++) {
-                    const int d = d0 + k;
+                    const int d = SPLIT ? split_dir(s) : (pair ? s + 4 * k : dir_at(s + 2));
                     cx<R> sv[12], U[9];
                     R n;
                     // the link of a pair's second direction is the second box
@@ -764,6 +772,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
         tma_epilogue<SIO, XPAY, R>(g, c, xh, y, acc);
     }
 }
+
 
 }  // namespace dev
 
@@ -943,7 +952,7 @@ XyLayout xy_layout(const TmaFormat &f, const StageLayout &l, bool split) {
 
 // kind of a TMA variant -> A buffers (0: the per-direction kernel) and form
 inline int kind_a_buffers(int kind) { return kind <= 1 ? 0 : (kind <= 3 ? kind - 1 : kind - 3); }
-inline bool kind_split(int kind) { return kind >= 4; }
+inline bool kind_split(int kind) { return kind == 4 || kind == 5; }
 
 // a row of eb-byte elements must be a whole number of 16-byte units (tile
 // loads) and at most 256 words
@@ -964,8 +973,9 @@ int dslash_tma_plan(const Geom &g, int prec, int recon, int kind, int nstage, in
     // rows in 1 or 2 buffers of their own; 4, 5: the same with one box per
     // stage (a spinor stage waits for the link stage after it: 2 at least)
     const int min_stage = kind == 2 || kind == 3 ? 1 : 2;
+    const int nsites = ny * g.L0h;  // consumer threads
     if (kind < 1 || kind > 5 || nstage < min_stage || nstage > 8 || ny < 1 || !rows || g.L[1] % ny ||
-        (ny * g.L0h) % 32 || ny * g.L0h > 256)
+        (ny * g.L0h) % 32 || nsites > 256)
         return set_error(PLQCD_ERR_ARG, "dslash: TMA tile %d rows x %d stages (kind %d) does not fit %dx%dx%dx%d", ny,
                          nstage, kind, g.L[0], g.L[1], g.L[2], g.L[3]);
     const StageLayout l = stage_layout(f, g.L0h, ny);
@@ -976,7 +986,7 @@ int dslash_tma_plan(const Geom &g, int prec, int recon, int kind, int nstage, in
         bytes = (size_t)na * x.a_bytes + (size_t)nstage * x.b_bytes + 16u * (na + nstage) + 128;
     }
     if (bytes > 227u * 1024 - 64) return set_error(PLQCD_ERR_ARG, "dslash: TMA ring of %zu bytes too large", bytes);
-    if (block) *block = ny * g.L0h + 32;
+    if (block) *block = nsites + 32;
     if (smem) *smem = bytes;
     return PLQCD_OK;
 }

@@ -554,8 +554,8 @@ TMA_CASES = [((16, 8, 4, 6), 1204), ((16, 8, 4, 6), 1308), ((16, 8, 6, 4), 1404)
 @pytest.mark.parametrize("prec,recon", [(P.F64, 18), (P.F64, 12), (P.F32, 18), (P.F32, 12), (P.F16, 12),
                                         (P.BF16, 12)])
 def test_tma_kernel_bit_identical(cuda, monkeypatch, L, variant, prec, recon):
-    """The TMA-staged kernel (tile loads of whole rows into a shared-memory
-    ring, one producer warp) computes exactly what the gather kernel
+    """The TMA-staged kernels (tile loads of whole rows into a shared-memory
+    ring, one producer warp) compute exactly what the gather kernel
     computes: bit-identical outputs for the full lattice, for one parity with
     the xpay and gamma5 epilogue, and no stage wait runs out."""
     lat, g64, u = _device_setup(L, 43)
@@ -604,8 +604,9 @@ def test_tma_kernel_matches_oracle(cuda, restatement):
 
 def test_tma_kernel_rejects_misfit_tiles(cuda, monkeypatch):
     """A tile that does not divide the lattice (rows per tile not dividing L1,
-    or not a whole number of warps) is refused on the host with an argument
-    error; nothing is launched."""
+    or not a whole number of warps), an unknown kernel kind or a ring too
+    short for its kernel is refused on the host with an argument error;
+    nothing is launched."""
     lat, g64, u = _device_setup((6, 4, 6, 10), 45)
     bs = lat.spinor_bytes(P.F64)
     a, o = dev_bytes(bs), dev_bytes(bs)
