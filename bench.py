@@ -51,9 +51,8 @@ BYTES_HALF_12 = 52 + 8 * 24 + 52
 # Variant 2 is the cp.async kernel, 1000*kind + 100*stages + rows a TMA kernel
 # (kind 1: a stage per direction; 2-5: own-line rows staged once per tile).
 DRAM_BYTES_PER_SITE_F64_FULL = {
-    2: 2252085512 / 2097152, 1204: 2329534320 / 2097152, 1208: 2332055480 / 2097152,
-    1304: 2243929008 / 2097152, 1404: 2666579136 / 2097152, 1408: 2206948256 / 2097152,
-    1604: 2194087920 / 2097152, 1216: 2357703600 / 2097152,
+    2: 2127234136 / 2097152, 1204: 2191090112 / 2097152, 2204: 2253279192 / 2097152,
+    4304: 2204120856 / 2097152, 1304: 2527646688 / 2097152, 1408: 2198568976 / 2097152,
 }
 
 

@@ -166,7 +166,9 @@ int tune_launch(const std::string &key, cudaStream_t s, const std::vector<TuneRe
             if (ok && ms < t) t = ms;
         }
         if (!ok) continue;
-        if (t < best) {
+        // a later candidate must win by more than 1%: near-ties (timing
+        // noise) keep the earlier, simpler configuration on every GPU
+        if (t < best * 0.99) {
             best = t;
             bestc = c;
             bestc.ms = t;
