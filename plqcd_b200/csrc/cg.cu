@@ -154,10 +154,11 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
     bool end_recorded = false;  // device time covers the solve, not the verification
 
     do {
+        const bool mixed = ps != PLQCD_F64;
         // b' = b_e + kappa H_eo b_o ; rhs = Mhat^dag b'
         if ((rc = op.hop(g64, bprime, b_odd, PLQCD_EVEN, 0, b_even, prm->kappa, 1.0))) break;
         if ((rc = blas_norm2(g, s, bprime, PLQCD_F64, red, RED_AUX))) break;
-        if ((rc = op.mhat(g64, rhs, bprime, tmp64, true))) break;
+        if (!mixed && (rc = op.mhat(g64, rhs, bprime, tmp64, true))) break;
         if ((rc = read_state())) break;
         bp2 = hst->aux;
         if (!(bp2 > 0)) {  // zero source: zero solution
@@ -166,18 +167,31 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
             inf.converged = 1;
             break;
         }
-        // x = 0, r = rhs
+        // x = 0, r = p = rhs
         cudaMemsetAsync(x_even, 0, b64, s);
         cudaMemsetAsync(xs, 0, bx, s);
-        if ((rc = blas_norm2(g, s, rhs, PLQCD_F64, red, RED_RR_INIT))) break;
-        if ((rc = launch_spinor_convert(g, s, rs, ps, rhs, PLQCD_F64))) break;
-        if ((rc = launch_spinor_convert(g, s, p, ps, rhs, PLQCD_F64))) break;
+        if (mixed) {
+            // the sloppy recursion starts from rhs in sloppy precision, so
+            // the sloppy operator computes it; convergence is decided on the
+            // FP64 Schur residual of b', which does not use rhs
+            if ((rc = launch_spinor_convert(g, s, t, ps, bprime, PLQCD_F64))) break;
+            if ((rc = op.mhat(gs, rs, t, tmps, true))) break;
+            if ((rc = blas_norm2(g, s, rs, ps, red, RED_RR_INIT))) break;
+            if (cudaMemcpyAsync(p, rs, bs, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+                rc = set_error(PLQCD_ERR_CUDA, "plqcd_invert_cg: device copy failed");
+                break;
+            }
+            inf.sloppy_hops += 2;
+        } else {
+            if ((rc = blas_norm2(g, s, rhs, PLQCD_F64, red, RED_RR_INIT))) break;
+            if ((rc = launch_spinor_convert(g, s, rs, ps, rhs, PLQCD_F64))) break;
+            if ((rc = launch_spinor_convert(g, s, p, ps, rhs, PLQCD_F64))) break;
+        }
         if ((rc = read_state())) break;
         const double rhs2 = hst->rr;
         double maxrr = hst->rr;
         double target = prm->tol * prm->tol * rhs2;  // normal-equation trigger for convergence checks
         const double delta2 = prm->delta * prm->delta;
-        const bool mixed = ps != PLQCD_F64;
         // a sloppy recursion that stops reducing its residual (16-bit storage
         // with a tiny delta) would never trigger an update: force one after
         // this many iterations without
