@@ -41,21 +41,11 @@ __device__ __forceinline__ void hop_dir(cx<typename SIO::real> acc[12], const vo
     cx<R> s[12];
     R n;
     SIO::load_raw(in, Vh, h_nbr, s, n);
-    cx<R> h0[3], h1[3];
-    project<MU, R>(s, FWD ? sg_in : -sg_in, h0, h1);
     cx<R> U[9];
     LIO::load(gauge, Vh, link_par, MU, h_link, U);
-    cx<R> c0[3], c1[3];
-    if (FWD) {
-        su3_mul(U, h0, c0);
-        su3_mul(U, h1, c1);
-    } else {
-        su3_dag_mul(U, h0, c0);
-        su3_dag_mul(U, h1, c1);
-    }
-    // The reference as shipped drops every forward contribution to spins
-    // 2,3 (its backward mu=0 step overwrites them, include/su3.h:135-138).
-    accumulate<MU, FWD ? 1 : -1, !(COMPAT && FWD), SIO::kScaled, R>(acc, c0, c1, n);
+    // projection, SU(3) product and rebuild (with COMPAT, the reference's
+    // as-shipped loss of the forward terms of spins 2, 3)
+    compute_dir_n<COMPAT, SIO::kScaled, R>(FWD ? MU : MU + 4, acc, s, U, sg_in, n);
 }
 
 template <class SIO, class LIO, bool COMPAT, bool XPAY, bool FULL>
@@ -206,7 +196,7 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
         R n;
         SIO::load_staged_raw(s0, B, s, n);
         LIO::load_staged(s0 + SIO::NSLOT * B, B, U);
-        compute_dir_n<COMPAT, SIO::kScaled, R>(dir_at(k), acc, s, U, sg, n);
+        compute_dir_n<COMPAT, SIO::kScaled, R, true>(dir_at(k), acc, s, U, sg, n);
         // the slot just consumed is refilled only after its values were used
         if (k + ST < 8) issue(k + ST);
         cp_async_commit();

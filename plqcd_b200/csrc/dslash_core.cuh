@@ -7,6 +7,8 @@
 //   backward: chi' = U_mu(x-mu)^dag h', h' = upper((1 + g_mu) psi(x-mu))
 #pragma once
 
+#include <type_traits>
+
 #include "device_fields.cuh"
 
 namespace plqcd {
@@ -201,10 +203,131 @@ __device__ __forceinline__ void compute_dir(cx<R> acc[12], const cx<R> s[12], co
 // kernels add in this order and give the same bits.
 __host__ __device__ constexpr int dir_at(int k) { return (k & 1) ? 4 + (k >> 1) : (k >> 1); }
 
-template <bool COMPAT, bool SC, typename R>
+// FP32 form of compute_dir on packed lanes within one site: lane 0 carries
+// spin 0 (upper) / spin 2 (lower), lane 1 spin 1 / spin 3, so one packed
+// instruction does the work of the two half-spinor vectors. Every lane runs
+// exactly the scalar sequence of project / su3_mul / accumulate (a sign
+// +-1 enters through an FMA, which rounds as the scalar add or subtract),
+// so the results are the same bits as with R = float.
+__device__ __forceinline__ f2 lanes(float a, float b) { return f2(a, b); }
+
+template <int MU, bool FWD, bool COMPAT, bool SC>
+__device__ __forceinline__ void compute_dir_pk(cx<float> acc[12], const cx<float> s[12], const cx<float> U[9],
+                                               float sg_in, float n) {
+    const float sg = FWD ? sg_in : -sg_in;
+    // projection: H[c] = (h0[c], h1[c])
+    cx<f2> H[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const cx<float> s0 = s[c], s1 = s[3 + c], s2 = s[6 + c], s3 = s[9 + c];
+        const f2 lo_re = lanes(s0.re, s1.re), lo_im = lanes(s0.im, s1.im);
+        if (MU == 0) {
+            H[c] = {fma(f2(sg), lanes(s2.re, s3.re), lo_re), fma(f2(sg), lanes(s2.im, s3.im), lo_im)};
+        } else if (MU == 1) {
+            H[c] = {fma(f2(-sg), lanes(s3.im, s2.im), lo_re), fma(f2(sg), lanes(s3.re, s2.re), lo_im)};
+        } else if (MU == 2) {
+            H[c] = {fma(lanes(sg, -sg), lanes(s3.re, s2.re), lo_re), fma(lanes(sg, -sg), lanes(s3.im, s2.im), lo_im)};
+        } else {
+            H[c] = {fma(lanes(-sg, sg), lanes(s2.im, s3.im), lo_re), fma(lanes(sg, -sg), lanes(s2.re, s3.re), lo_im)};
+        }
+    }
+    // SU(3) product of both vectors: C[a] = (c0[a], c1[a])
+    cx<f2> C[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const cx<float> u0 = FWD ? U[3 * a] : U[a];
+        const float ui0 = FWD ? u0.im : -u0.im;  // U^dag: conjugate
+        f2 re = f2(u0.re) * H[0].re;
+        f2 im = f2(u0.re) * H[0].im;
+        re = fma(f2(-ui0), H[0].im, re);
+        im = fma(f2(ui0), H[0].re, im);
+#pragma unroll
+        for (int b = 1; b < 3; b++) {
+            const cx<float> ub = FWD ? U[3 * a + b] : U[3 * b + a];
+            const float uib = FWD ? ub.im : -ub.im;
+            re = fma(f2(ub.re), H[b].re, re);
+            re = fma(f2(-uib), H[b].im, re);
+            im = fma(f2(ub.re), H[b].im, im);
+            im = fma(f2(uib), H[b].re, im);
+        }
+        C[a] = {re, im};
+    }
+    // rebuild: upper spins (0, 1) += chi; lower spins (2, 3) by the sign / i
+    // pattern of the direction (LS = +1 forward, -1 backward)
+    constexpr float LS = FWD ? 1.f : -1.f;
+    constexpr bool LOWER = !(COMPAT && FWD);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        f2 u_re = lanes(acc[c].re, acc[3 + c].re), u_im = lanes(acc[c].im, acc[3 + c].im);
+        f2 l_re = lanes(acc[6 + c].re, acc[9 + c].re), l_im = lanes(acc[6 + c].im, acc[9 + c].im);
+        const f2 cre = C[c].re, cim = C[c].im;
+        const f2 sre = lanes(cre.v.y, cre.v.x), sim = lanes(cim.v.y, cim.v.x);  // lanes swapped
+        if (SC) {
+            const float p = LS * n, q = -LS * n;
+            u_re = fma(f2(n), cre, u_re);
+            u_im = fma(f2(n), cim, u_im);
+            if (LOWER) {
+                if (MU == 0) {
+                    l_re = fma(f2(p), cre, l_re);
+                    l_im = fma(f2(p), cim, l_im);
+                } else if (MU == 1) {
+                    l_re = fma(f2(p), sim, l_re);
+                    l_im = fma(f2(q), sre, l_im);
+                } else if (MU == 2) {
+                    l_re = fma(lanes(q, p), sre, l_re);
+                    l_im = fma(lanes(q, p), sim, l_im);
+                } else {
+                    l_re = fma(lanes(p, q), cim, l_re);
+                    l_im = fma(lanes(q, p), cre, l_im);
+                }
+            }
+        } else {
+            u_re = u_re + cre;
+            u_im = u_im + cim;
+            if (LOWER) {
+                if (MU == 0) {
+                    l_re = fma(f2(LS), cre, l_re);
+                    l_im = fma(f2(LS), cim, l_im);
+                } else if (MU == 1) {
+                    l_re = fma(f2(LS), sim, l_re);
+                    l_im = fma(f2(-LS), sre, l_im);
+                } else if (MU == 2) {
+                    l_re = fma(lanes(-LS, LS), sre, l_re);
+                    l_im = fma(lanes(-LS, LS), sim, l_im);
+                } else {
+                    l_re = fma(lanes(LS, -LS), cim, l_re);
+                    l_im = fma(lanes(-LS, LS), cre, l_im);
+                }
+            }
+        }
+        acc[c] = {u_re.v.x, u_im.v.x};
+        acc[3 + c] = {u_re.v.y, u_im.v.y};
+        acc[6 + c] = {l_re.v.x, l_im.v.x};
+        acc[9 + c] = {l_re.v.y, l_im.v.y};
+    }
+}
+
+// PK: FP32 on packed lanes within the site (compute_dir_pk). It pays in
+// the single-RHS cp.async pipeline kernel (32^3x64: F16 xpay hop -12%, BF16
+// -9%, F32 -1..-4% as tuned) and loses in the direct-load, multi-RHS and TMA
+// kernels, which keep the scalar form; both give the same bits.
+template <bool COMPAT, bool SC, typename R, bool PK = false>
 __device__ __forceinline__ void compute_dir_n(int d, cx<R> acc[12], const cx<R> s[12], const cx<R> U[9], R sg,
                                               R n) {
     // d is a compile-time constant after unrolling, so this switch folds
+    if constexpr (PK && std::is_same<R, float>::value) {
+        switch (d) {
+            case 0: compute_dir_pk<0, true, COMPAT, SC>(acc, s, U, sg, n); break;
+            case 1: compute_dir_pk<1, true, COMPAT, SC>(acc, s, U, sg, n); break;
+            case 2: compute_dir_pk<2, true, COMPAT, SC>(acc, s, U, sg, n); break;
+            case 3: compute_dir_pk<3, true, COMPAT, SC>(acc, s, U, sg, n); break;
+            case 4: compute_dir_pk<0, false, COMPAT, SC>(acc, s, U, sg, n); break;
+            case 5: compute_dir_pk<1, false, COMPAT, SC>(acc, s, U, sg, n); break;
+            case 6: compute_dir_pk<2, false, COMPAT, SC>(acc, s, U, sg, n); break;
+            default: compute_dir_pk<3, false, COMPAT, SC>(acc, s, U, sg, n); break;
+        }
+        return;
+    }
     switch (d) {
         case 0: compute_dir<0, true, COMPAT, SC>(acc, s, U, sg, n); break;
         case 1: compute_dir<1, true, COMPAT, SC>(acc, s, U, sg, n); break;

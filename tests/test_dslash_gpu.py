@@ -511,10 +511,12 @@ def test_dslash_every_load_strategy(cuda, monkeypatch, variant, block, prec, rec
 
 @pytest.mark.parametrize("prec,recon", [(P.F32, 18), (P.F32, 12), (P.F16, 12), (P.BF16, 12)])
 def test_packed_lanes_bit_identical(cuda, monkeypatch, prec, recon):
-    """Two sites per thread on packed FP32 lanes (FFMA2, variant 13) round
-    every lane as the scalar arithmetic does: the outputs are the same
-    bits as the one-site cp.async kernel, for a plain hop and for the xpay /
-    gamma5 epilogue, on a lattice whose half volume leaves a ragged last tile."""
+    """Packed FP32 lanes (FFMA2) round every lane as the scalar arithmetic
+    does: the one-site cp.async kernel (variant 2, spin pairs of one site on
+    the two lanes), two sites per thread with scalar arithmetic (variant 12)
+    and on packed lanes (variant 13) give the same bits, for a plain hop and
+    for the xpay / gamma5 epilogue, on a lattice whose half volume leaves a
+    ragged last tile."""
     L = (6, 4, 6, 10)
     lat, g64, u = _device_setup(L, 49)
     g = P.Gauge(lat, prec, recon)
