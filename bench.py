@@ -56,11 +56,25 @@ DRAM_BYTES_PER_SITE_F64_FULL = {
 }
 
 
-def dram_bytes_per_site(cfg) -> float:
-    """ncu DRAM bytes per site of the full-lattice F64 configuration `cfg`
-    (configurations without their own capture: the largest measured)."""
+def dram_bytes_per_site(cfg):
+    """ncu DRAM bytes per site of the full-lattice F64 configuration `cfg`,
+    or None when that configuration has no capture."""
     v = 2 if cfg is None else cfg[0]
-    return DRAM_BYTES_PER_SITE_F64_FULL.get(v, max(DRAM_BYTES_PER_SITE_F64_FULL.values()))
+    return DRAM_BYTES_PER_SITE_F64_FULL.get(v)
+
+
+def traffic_bytes(cfg, V):
+    b = dram_bytes_per_site(cfg)
+    return None if b is None else round(b * V)
+
+
+def traffic_note(cfg, L) -> str:
+    """Where roofline.traffic comes from: not measured in this run."""
+    if dram_bytes_per_site(cfg) is None:
+        return "no ncu capture of this configuration (see profiles/ for the captured ones)"
+    return ("ncu dram bytes (read + write) of one launch of this configuration at 32^3x64, taken from the "
+            "single-pass capture in profiles/dslash_full_f64_dram_32x32x32x64.txt, not measured in this run"
+            + ("" if tuple(L) == (32, 32, 32, 64) else "; scaled by sites"))
 
 
 def measured_peaks():
@@ -354,6 +368,7 @@ def run_ours(args, d: Dist):
         head_cfg = (int(os.environ["PLQCD_DSLASH_FULL_STAGES"]), 0)
     value = d.world * V * FLOP_PER_SITE / t_step / 1e9
     achieved = V * BYTES_FULL[0] / t_step / 1e9
+    sustained = run_sustained(torch, full, t_step, V, hbm, d, args) if args.sustained_s > 0 else None
 
     # ---- per-parity kernels (the drop-in and solver building block) ---------
     Kp = K if args.only == "dslash" else max(10, K // 2)
@@ -389,7 +404,8 @@ def run_ours(args, d: Dist):
         if d.rank == 0:
             print(json.dumps({"metric": "Dslash GFLOP/s", "value": round(value, 1), "unit": "GFLOP/s",
                               "lattice": list(L), "only": "dslash", "kernel": kernel_name(head_cfg),
-                              "frac": round(achieved / hbm, 4), "clocks": clocks, "per_parity_f64": parity,
+                              "frac": round(achieved / hbm, 4), "clocks": clocks, "sustained": sustained,
+                              "per_parity_f64": parity,
                               "f32": fp32}))
         return 0
 
@@ -432,10 +448,9 @@ def run_ours(args, d: Dist):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "peak_kind": peak_kind,
                      "bytes_per_site": BYTES_FULL[0], "kernel": kernel_name(head_cfg),
-                     "traffic": round(dram_bytes_per_site(head_cfg) * V),
-                     "traffic_note": ("ncu dram bytes (read + write) of one launch of this configuration "
-                                      "at 32^3x64, single-pass capture"
-                                      + ("" if tuple(L) == (32, 32, 32, 64) else ", scaled by sites"))},
+                     "traffic": traffic_bytes(head_cfg, V),
+                     "traffic_note": traffic_note(head_cfg, L)},
+        "sustained": sustained,
         "per_parity_f64": parity,
         "f32": fp32,
         "e2e": e2e,
@@ -453,14 +468,43 @@ def run_ours(args, d: Dist):
     return 0
 
 
+def write_input_file(L) -> str:
+    """Key-value input file for init_plqcd (lib/start.c:84-107): one
+    process, one host thread."""
+    fd, path = tempfile.mkstemp(suffix=".input")
+    with os.fdopen(fd, "w") as f:
+        f.write("".join(f"L{k} {int(L[k])}\n" for k in range(4)))
+        f.write("".join(f"NPROC{k} 1\n" for k in range(4)))
+        f.write("NTHREAD 1\nALIGN 6\n")
+    return path
+
+
+def run_sustained(torch, full, t_step, V, hbm, d: Dist, args):
+    """The headline launch back to back for about --sustained-s seconds, with
+    its own clock samples: the rate once the power cap has settled the SM
+    clock, beside the short --steps window of `value`."""
+    n = max(10, int(args.sustained_s / max(t_step, 1e-6)))
+    clk = ClockSampler(d.local)
+    clk.start()
+    ms = d.max(time_kernel(torch, full, n, 3, d))
+    clocks = clk.stop()
+    t = ms / 1e3 / n
+    return {"launches": n, "seconds": round(ms / 1e3, 3), "ms_per_launch": round(t * 1e3, 4),
+            "gflops": round(d.world * V * FLOP_PER_SITE / t / 1e9, 1),
+            "achieved_gbs": round(V * BYTES_FULL[0] / t / 1e9, 1), "frac": round(V * BYTES_FULL[0] / t / 1e9 / hbm, 4),
+            "clocks": clocks}
+
+
 def run_e2e(torch, P, lat, g64, fe, fo, d: Dist, args):
     """eo+oe through plqcd_hopping_matrix_*_sse3_assymbly on pinned host
-    arrays, copies included, wall clock (the calls are synchronous)."""
-    from oracle import oracle as O
+    arrays, copies included, wall clock (the calls are synchronous). The
+    link array is registered once with plqcd_gauge_update, as a caller that
+    keeps its links fixed over many hops does; every call moves its spinor
+    parity up and its output parity down."""
     L = lat.dims
     V = lat.V
     os.environ["PLQCD_DEVICE"] = str(d.local)
-    path = O.write_input_file(L, nthreads=1)
+    path = write_input_file(L)
     P.finalize_plqcd()
     if P.init_plqcd(path) != 0:
         raise RuntimeError(P.last_error())
@@ -472,6 +516,7 @@ def run_e2e(torch, P, lat, g64, fe, fo, d: Dist, args):
         np.complex128)
     qin, qout, u = mk(pq, nq).reshape(V, 12), mk(pout, nq).reshape(V, 12), mk(pu, nu).reshape(4 * V, 9)
     P.check(lib.plqcd_gauge_store_host(g64.handle, pu))
+    P.check(lib.plqcd_gauge_update(pu))
     aos = torch.zeros((V, 12), dtype=torch.complex128, device="cuda")
     lat.spinor_export(fe, P.F64, 0, aos)
     lat.spinor_export(fo, P.F64, 1, aos)
@@ -496,7 +541,8 @@ def run_e2e(torch, P, lat, g64, fe, fo, d: Dist, args):
            "h2d_bytes_per_step": int(2 * h2d), "d2h_bytes_per_step": int(2 * d2h), "steps": Ke,
            "ms_per_step": round(dt / Ke * 1e3, 3),
            "api": "plqcd_hopping_matrix_eo/oe_sse3_assymbly on amalloc'd (pinned) host arrays; "
-                  "gauge field cached on the device after the first call"}
+                  "link array registered once with plqcd_gauge_update (uploaded by the first call, "
+                  "kept on the device); each call moves its spinor parity up and its output down"}
     # keep copies for the CPU baseline before the pinned blocks go away
     res["_qin"] = np.array(qin)
     res["_u"] = np.array(u)
@@ -749,7 +795,9 @@ def run_reduced(torch, P, d: Dist, args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--sustained-s", type=float, default=3.0,
+                    help="seconds of the back-to-back headline loop of the `sustained` record (0: skip)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=40)

@@ -23,10 +23,13 @@
  * behaviour exactly.
  *
  * The SSE3-intrinsic names (lib/dirac.c:801, 1272, 1748, 2124) take the same
- * arguments and map to the same correct kernel. The gauge field is cached on
- * the device by host pointer plus a sampled fingerprint; call
- * plqcd_gauge_update() (plqcd_b200.h) after changing links in place, or set
- * PLQCD_GAUGE_CACHE=0 to upload on every call.
+ * arguments and map to the same correct kernel. Like the reference, every
+ * call reads the link array `u`: it is uploaded to the GPU on each call.
+ * A caller whose links stay fixed over many calls registers the array once
+ * with plqcd_gauge_update(u) (plqcd_b200.h); it is then uploaded once and
+ * kept on the device until the next plqcd_gauge_update or finalize_plqcd.
+ * After changing registered links in place, call plqcd_gauge_update(u)
+ * again.
  */
 #ifndef _DIRAC_H
 #define _DIRAC_H

@@ -135,18 +135,23 @@ int plqcd_spinor_gaussian(plqcd_lattice *lat, void *dst, int prec, int parity, u
 int plqcd_spinor_norm2(plqcd_lattice *lat, const void *fields, int prec, int nfields, double *norms_dev);
 
 /* Same result as plqcd_spinor_norm2, for callers that must not allocate
- * device memory: code running while a CUDA graph is captured in the global
- * capture mode (cudaMalloc is prohibited there), applications whose device
- * memory all comes from their own pool, and loops that cannot take the
- * device synchronisation of cudaMalloc / cudaFree. It calls no allocating
- * routine; its scratch is a static device array of about 303 KB that every
- * GPU loading the library keeps until the process exits.
+ * device memory: applications whose device memory all comes from their own
+ * pool (a framework that has reserved the GPU's memory, a service held to a
+ * fixed budget), where an allocation outside the pool fails or breaks the
+ * budget, and latency-bound loops that cannot take the device-wide
+ * synchronisation of cudaFree. It calls no cudaMalloc, cudaFree or other
+ * allocating routine; its scratch is a static device array of about 303 KB
+ * that every GPU loading the library keeps until the process exits.
  *  - nfields must be 1..PLQCD_NORM2_NOALLOC_MAX_FIELDS; larger batches are
  *    rejected with PLQCD_ERR_ARG.
- *  - The first call on each device looks up the scratch address
- *    (cudaGetSymbolAddress); make that first call before any stream capture.
- *  - All calls on a device share the one scratch array: calls that overlap
- *    on the GPU (e.g. from two streams at once) race and give wrong sums.
+ *  - The first call on each device (and again after cudaDeviceReset gives
+ *    the device a new context) does the set-up: it looks up the scratch
+ *    address with cudaGetSymbolAddress and loads the reduction kernel of
+ *    every precision. Make that first call before any stream capture.
+ *  - All calls on a device share the one scratch array, which keeps the
+ *    last call's contents (each call clears the arrival counters it uses):
+ *    calls that overlap on the GPU (e.g. from two streams at once) race and
+ *    give wrong sums.
  * Counterpart in the reference: none (the reference has no device code). */
 #define PLQCD_NORM2_NOALLOC_MAX_FIELDS 32
 int plqcd_spinor_norm2_noalloc(plqcd_lattice *lat, const void *fields, int prec, int nfields, double *norms_dev);
@@ -272,12 +277,34 @@ int plqcd_invert_cg_batch(plqcd_solve_item *items, int nitems, const plqcd_cg_pa
 int plqcd_selftest(int device, int verbose);
 
 /* ---- drop-in path controls ---------------------------------------------- */
-/* Mark the host gauge field `u` as changed (or a new field) so the next
- * drop-in call uploads it. */
+/* Register the host link array `u` of the drop-in hopping calls as
+ * current: the next call that passes `u` uploads it, and later calls with
+ * `u` reuse the device copy until the next plqcd_gauge_update (or
+ * finalize_plqcd). Call it again after changing the links in place. For the
+ * lane-packed names pass the su3_256 / su3_512 array, for the split family
+ * the u_re plane. NULL clears the registration, and every device copy is
+ * reloaded on its next use. Without a registration every call uploads its
+ * links, as the reference reads them on every call. Environment:
+ * PLQCD_GAUGE_CACHE=0 uploads on every call even when registered;
+ * PLQCD_GAUGE_CACHE=1 keeps any link array by address plus a fingerprint
+ * of sampled words, for callers that never change links in place. */
 int plqcd_gauge_update(const su3 *u);
 /* Device time (ms) of the kernels of the last drop-in hopping call and its
  * host<->device byte counts. */
 int plqcd_dropin_last_stats(double *kernel_ms, double *h2d_bytes, double *d2h_bytes);
+
+/* ---- failure detection ----------------------------------------------------- */
+/* Test hook of the bounded waits in the TMA-staged hopping kernels (no
+ * reference counterpart: the reference calls exit(1) when a face exchange
+ * fails, lib/dirac.c:128-130). With `enable` non-zero, every later launch
+ * of a TMA kernel in this process makes each consumer warp first wait, with
+ * a limit of `limit_ns` (1 us .. 2 s), on a shared-memory barrier that
+ * nothing completes. The wait runs out, the warps stop, the producer waits
+ * (bounded) for the tile loads it has in flight, the kernel returns, and
+ * the next plqcd_lattice_synchronize (or solver) reports PLQCD_ERR_TIMEOUT
+ * and clears the flag; that launch's output is incomplete. enable = 0
+ * restores normal operation. Nothing faults, traps or hangs. */
+int plqcd_tma_timeout_test(int enable, unsigned long long limit_ns);
 
 /* ---- host layout converters for the split entry points ------------------- */
 /* No reference counterpart: the reference leaves packing to its callers.

@@ -10,14 +10,38 @@
  *    needs -fcommon to link);
  *  - phip/phim stay NULL: the GPU kernel gathers neighbours directly and
  *    needs no half-spinor buffers;
- *  - the SIMD split-layout tables (ipt_*_sse_split, *_avx_split,
- *    *_mic_split) and the MIC buffers are not built.
+ *  - the SSE split-layout tables (ipt_eo_sse_split, ipt_lex_sse_split,
+ *    iup_sse_split, idn_sse_split) are members, in the reference's place,
+ *    so that the struct has the reference's default layout (no AVX_SPLIT,
+ *    no MIC: include/plqcd_global_params.h:147-196); they stay NULL. The
+ *    AVX and MIC members, which the reference compiles in only under
+ *    AVX_SPLIT / MIC, are not declared.
  */
 #ifndef PLQCD_GLOBAL_PARAMS_H_
 #define PLQCD_GLOBAL_PARAMS_H_
 
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
+#include <math.h>
+/* C callers get what the reference's header gives them
+ * (include/plqcd_global_params.h:24-61): <stdbool.h>, <complex.h>, the
+ * caller's MPI header when its include path has one (the reference's
+ * drivers call MPI_Barrier / MPI_Reduce / MPI_Bcast for their timing,
+ * tests/test_hopping.c:293,303-304) and <omp.h> under OpenMP. The library
+ * itself uses none of them. */
+#ifndef __cplusplus
+#include <stdbool.h>
+#include <complex.h>
+#if defined(__has_include)
+#if __has_include("mpi.h")
+#include "mpi.h"
+#endif
+#endif
+#endif
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include "su3.h"
 #include "utils.h"
 
@@ -45,6 +69,10 @@ struct _PLQCD_GLOBAL_PARAMS {
     int **idn;          /* idn[i][mu]: even/odd index of the -mu neighbour (periodic) */
     int *ipt_eo_yzt;    /* even/odd index within the y,z,t block */
     int *ipt_lex_yzt;   /* inverse of ipt_eo_yzt */
+    int *ipt_eo_sse_split;  /* SSE split-layout tables: NULL (not built) */
+    int *ipt_lex_sse_split;
+    int **iup_sse_split;
+    int **idn_sse_split;
     halfspinor *phip[4];/* unused by the GPU path (NULL) */
     halfspinor *phim[4];/* unused by the GPU path (NULL) */
     int ALIGN;          /* alignment exponent for amalloc (2^ALIGN bytes) */

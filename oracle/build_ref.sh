@@ -16,10 +16,16 @@
 # single-rank stub in oracle/mpi_stub. -DASSYMBLY without -DSSE2/-DSSE3
 # selects the plain-C macros (the inline-asm ones miscompile with gcc 13).
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]
+#        oracle/build_ref.sh --root      (print the reference root and exit)
+# The root is the argument, else $PLQCD_REFERENCE_ROOT, else /root/reference.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+if [ "${1:-}" = "--root" ]; then
+    echo "${PLQCD_REFERENCE_ROOT:-/root/reference}"
+    exit 0
+fi
+REF="${1:-${PLQCD_REFERENCE_ROOT:-/root/reference}}"
 CC="${CC:-gcc}"
 # -B points the driver at a gcc install dir that holds libgomp.spec (the
 # wrapper compiler in this image lacks it; harmless elsewhere).

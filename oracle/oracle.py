@@ -38,9 +38,21 @@ _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)
 
 
-def build(reference_root: str = "/root/reference") -> None:
+def reference_root() -> str:
+    """Root of the reference's sources: $PLQCD_REFERENCE_ROOT, else the
+    default of the build recipe (oracle/build_ref.sh --root). Only the
+    recipe and the tests that compile the reference's own files use it; no
+    GPU test, smoke() or bench.py reads the reference's sources."""
+    r = os.environ.get("PLQCD_REFERENCE_ROOT")
+    if r:
+        return r
+    out = subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), "--root"], capture_output=True, text=True)
+    return out.stdout.strip()
+
+
+def build(root: str | None = None) -> None:
     """Compile the oracles (oracle/build_ref.sh)."""
-    subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), reference_root], check=True)
+    subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), root or reference_root()], check=True)
 
 
 def _dims(L):

@@ -121,6 +121,7 @@ _SIGS = {
     "plqcd_tune_get": (_i, [ctypes.c_char_p, _ip, _ip, _dp]),
     "plqcd_selftest": (_i, [_i, _i]),
     "plqcd_gauge_update": (_i, [_vp]),
+    "plqcd_tma_timeout_test": (_i, [_i, ctypes.c_ulonglong]),
     "plqcd_dropin_last_stats": (_i, [_dp, _dp, _dp]),
     "plqcd_aos_to_split": (_i, [_vp, _vp, _vp, ctypes.c_long]),
     **{f"plqcd_hopping_matrix_{w}_{v}": (ctypes.c_double, [_vp, _vp, _vp])

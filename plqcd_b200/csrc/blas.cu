@@ -327,6 +327,16 @@ __global__ void __launch_bounds__(kBlasBlock) k_norm2_multi(const char *fields, 
 
 int norm2_blocks(long Vh) { return dev::blas_grid(Vh); }
 
+// Loads k_norm2_multi for every precision on the current device (with lazy
+// module loading a kernel is otherwise loaded by its first launch).
+int preload_norm2_multi() {
+    cudaFuncAttributes a;
+    for (const void *k : {(const void *)dev::k_norm2_multi<PLQCD_F64>, (const void *)dev::k_norm2_multi<PLQCD_F32>,
+                          (const void *)dev::k_norm2_multi<PLQCD_F16>, (const void *)dev::k_norm2_multi<PLQCD_BF16>})
+        PLQCD_CUDA_TRY(cudaFuncGetAttributes(&a, k));
+    return PLQCD_OK;
+}
+
 int launch_norm2_multi(const Geom &g, cudaStream_t s, const void *fields, int prec, int nf, double *partials,
                        unsigned *counters, double *out) {
     const int nb = dev::blas_grid(g.Vh);

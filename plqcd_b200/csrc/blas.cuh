@@ -58,6 +58,7 @@ int blas_sub_norm2(const Geom &g, cudaStream_t s, void *out, const void *a, cons
 // |x_f|^2 of nf fields stored back to back; scratch: nf * norm2_blocks(Vh)
 // partials and nf counters (zero on entry, left zero on exit)
 int norm2_blocks(long Vh);
+int preload_norm2_multi();
 int launch_norm2_multi(const Geom &g, cudaStream_t s, const void *fields, int prec, int nf, double *partials,
                        unsigned *counters, double *out);
 // y = a x + b y (F64 fields)

@@ -4,10 +4,15 @@
 // Each call copies the input parity of `qin` (API layout, host) to the
 // device, converts it to the kernel layout, runs the sm_100a hopping kernel
 // and copies the output parity back into `qout`; the other half of `qout` is
-// not touched, as in the reference. The gauge field is uploaded on first use
-// and kept on the device keyed by its host address plus a fingerprint of
-// 1024 sampled doubles; plqcd_gauge_update() or PLQCD_GAUGE_CACHE=0 force a
-// fresh upload. The return value is the call's wall-clock seconds
+// not touched, as in the reference. The reference reads the links on every
+// call, so by default so does this path: the link array is uploaded on
+// every call, unless the caller has registered it with
+// plqcd_gauge_update(u), which declares "these links are current until the
+// next plqcd_gauge_update": then it is uploaded once and kept on the device.
+// PLQCD_GAUGE_CACHE=1 keeps any link array by host address plus a
+// fingerprint of sampled words (for callers known never to change links in
+// place); PLQCD_GAUGE_CACHE=0 uploads on every call even when registered.
+// The return value is the call's wall-clock seconds
 // (lib/dirac.c:405-407), or -1 on failure with the reason in
 // plqcd_last_error(). Calls are serialised (the reference is not
 // re-entrant either: lib/dirac.c:12-13 and the global phip/phim buffers).
@@ -80,6 +85,11 @@ struct DropIn {
 
 std::mutex g_mu;
 DropIn g_d;
+// the link array declared current by plqcd_gauge_update. release_locked
+// keeps it, so a registration made between init_plqcd and the first call
+// survives that call's set-up (device copies still start out dirty);
+// finalize_plqcd clears it.
+const void *g_registered = nullptr;
 
 void release_locked() {
     if (g_d.lat) cudaSetDevice(g_d.lat->device);
@@ -163,6 +173,23 @@ uint64_t fingerprint(const su3 *u, long nlinks) {
     }
     h = (h ^ w[nwords - 1]) * 1099511628211ULL;
     return h;
+}
+
+// Whether the device copy of link array `u` (cached from the array at
+// `cached`, with sampled fingerprint `cached_fp`) can serve this call:
+//   PLQCD_GAUGE_CACHE unset: only a registered array, not marked dirty;
+//   PLQCD_GAUGE_CACHE=1:     any array whose address and fingerprint match;
+//   PLQCD_GAUGE_CACHE=0:     never.
+// `fp` computes the fingerprint (only the sampled mode needs it).
+template <class F>
+bool keep_cached_gauge(const void *u, const void *cached, bool dirty, uint64_t cached_fp, uint64_t *new_fp, F fp) {
+    const char *e = getenv("PLQCD_GAUGE_CACHE");
+    if (e && *e == '0') return false;
+    if (e && *e && *e != '0') {
+        *new_fp = fp();
+        return !dirty && cached == u && cached_fp == *new_fp;
+    }
+    return !dirty && cached == u && g_registered == u;
 }
 
 int ensure_locked() {
@@ -362,9 +389,9 @@ double hop_call(spinor *qin, spinor *qout, su3 *u, int out_parity) {
     }
     g_d.h2d = g_d.d2h = 0;
 
-    // gauge field: upload when new, changed or caching is disabled
-    uint64_t fp = fingerprint(u, 8 * Vh);
-    if (!env_flag("PLQCD_GAUGE_CACHE", true) || g_d.dirty || g_d.cached_u != u || g_d.fingerprint != fp) {
+    // gauge field: upload unless the device copy may serve (keep_cached_gauge)
+    uint64_t fp = 0;
+    if (!keep_cached_gauge(u, g_d.cached_u, g_d.dirty, g_d.fingerprint, &fp, [&] { return fingerprint(u, 8 * Vh); })) {
         if (plqcd_gauge_load_host(g_d.gauge, u) != PLQCD_OK) return -1.0;
         g_d.cached_u = u;
         g_d.fingerprint = fp;
@@ -489,9 +516,11 @@ double hop_call_split(double *qout_re, double *qout_im, double *u_re, double *u_
     g_d.h2d = g_d.d2h = 0;
     plqcd_gauge *&gf = short12 ? g_d.gauge12 : g_d.gauge_split;
     if (!gf && plqcd_gauge_create(lat, PLQCD_F64, short12 ? 12 : 18, &gf) != PLQCD_OK) return -1.0;
-    const uint64_t fp = fingerprint_split(u_re, u_im, 8 * Vh * 9);
     SplitCache &sc = short12 ? g_d.split12 : g_d.split18;
-    if (!env_flag("PLQCD_GAUGE_CACHE", true) || g_d.dirty_split || sc.re != u_re || sc.im != u_im || sc.fp != fp) {
+    uint64_t fp = 0;
+    // the split family registers its real-part plane u_re
+    if (sc.im != u_im ||
+        !keep_cached_gauge(u_re, sc.re, g_d.dirty_split, sc.fp, &fp, [&] { return fingerprint_split(u_re, u_im, 8 * Vh * 9); })) {
         if (load_gauge_split(gf, u_re, u_im) != PLQCD_OK) return -1.0;
         sc.re = u_re;
         sc.im = u_im;
@@ -635,9 +664,11 @@ double hop_call_packed(const void *qin, void *qout, const void *u, int out_parit
     g_d.h2d = g_d.d2h = 0;
     plqcd_gauge *&gf = short12 ? g_d.gauge_packed12 : g_d.gauge_packed;
     if (!gf && plqcd_gauge_create(lat, PLQCD_F64, short12 ? 12 : 18, &gf) != PLQCD_OK) return -1.0;
-    const uint64_t fp = fingerprint(static_cast<const su3 *>(u), 8 * Vh);
     auto &pc = short12 ? g_d.packed12 : g_d.packed18;
-    if (!env_flag("PLQCD_GAUGE_CACHE", true) || g_d.dirty_packed || pc.u != u || pc.lanes != lanes || pc.fp != fp) {
+    uint64_t fp = 0;
+    if (pc.lanes != lanes || !keep_cached_gauge(u, pc.u, g_d.dirty_packed, pc.fp, &fp, [&] {
+            return fingerprint(static_cast<const su3 *>(u), 8 * Vh);
+        })) {
         if (load_gauge_packed(gf, u, lanes) != PLQCD_OK) return -1.0;
         pc.u = u;
         pc.lanes = lanes;
@@ -686,15 +717,18 @@ double hop_call_packed(const void *qin, void *qout, const void *u, int out_parit
 }  // namespace
 
 namespace plqcd {
+// finalize_plqcd: drop every device copy and the registration (a later
+// array at the same host address is a different field)
 void dropin_release() {
     std::lock_guard<std::mutex> lk(g_mu);
     release_locked();
+    g_registered = nullptr;
 }
 }  // namespace plqcd
 
 extern "C" int plqcd_gauge_update(const su3 *u) {
     std::lock_guard<std::mutex> lk(g_mu);
-    (void)u;
+    g_registered = u;
     g_d.dirty = true;
     g_d.dirty_split = true;
     g_d.dirty_packed = true;

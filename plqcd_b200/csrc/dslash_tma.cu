@@ -74,6 +74,11 @@ struct TmaGeom {
     int nstage_a, split;
     uint32_t a_bytes, off_a_main[2], off_a_lo[2], off_a_hi[2], off_lk2;
     double a_up, a_low, b, g5_in;
+    // limit of a consumer's wait for a staged tile; with `stall` (the
+    // failure-detection test hook) each consumer warp first waits, with that
+    // limit, on a barrier that nothing completes, so the wait runs out
+    uint64_t cwait_ns;
+    int stall;
     void *out0, *out1;  // output of parity 0 / 1 (full); out0 otherwise
     const void *x;      // xpay operand (single parity)
 };
@@ -283,6 +288,27 @@ __device__ __forceinline__ void tma_issue_dir(const TmaMaps &m, const TmaGeom &g
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 constexpr uint64_t kDrainLimitNs = 200000000ull;  // 0.2 s
 
+// A consumer warp's wait for a stage. The outcome is made warp-uniform, so
+// a warp whose wait ran out (or saw another warp's abort) stops as a whole:
+// no lane leaves while the others go on to __syncwarp. Lane 0 records the
+// abort for the CTA's producer and the timeout for the host.
+__device__ __forceinline__ bool consumer_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns,
+                                              volatile int *abort) {
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(bar, parity, limit_ns, abort));
+    if (!ok && (threadIdx.x & 31) == 0) {
+        *abort = 1;
+        atomicExch(&g_tma_status, 1);
+    }
+    return ok;
+}
+
+// Failure-detection test: with g.stall the consumer warp waits on `never`,
+// an mbarrier with one expected arrival that nothing performs; the bounded
+// wait runs out after g.cwait_ns and the warp stops (consumer_wait).
+__device__ __forceinline__ bool stall_test_wait(const TmaGeom &g, uint32_t never, volatile int *abort) {
+    return !g.stall || consumer_wait(never, 0, g.cwait_ns, abort);
+}
+
 // ---- shared own-line variant ----------------------------------------------------
 // The x+-, y+- neighbours of a tile all sit in the own (z, t) line: rows
 // y0-1 .. y0+NY of the input. k_dslash_tma_xy stages them once per tile, in
@@ -456,10 +482,12 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
     using R = typename SIO::real;
     extern __shared__ uint8_t smem_raw[];
     __shared__ int s_abort;
+    __shared__ __align__(8) uint64_t s_never;  // the stall test's barrier
     const uint32_t raw = smem_addr(smem_raw);
     const uint32_t pad = ((raw + 127u) & ~127u) - raw;
     const uint8_t *sbase = smem_raw + pad;
     const uint32_t base = raw + pad;
+    const uint32_t never = smem_addr(&s_never);
     const uint32_t full_bar = base + (uint32_t)g.nstage * g.stage_bytes;
     const uint32_t empty_bar = full_bar + 8u * g.nstage;
     const int bid = blockIdx.x;
@@ -472,6 +500,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
             mbar_init(full_bar + 8u * b, 1);
             mbar_init(empty_bar + 8u * b, (uint32_t)g.ncw);
         }
+        mbar_init(never, 1);
         mbar_init_fence();
     }
     __syncthreads();
@@ -523,6 +552,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
     const int own = j * L0h + xh;
     const int SM = g.NY * L0h;  // plane stride of an NY-row box, in elements
     const R sg = (R)g.g5_in;
+    if (!stall_test_wait(g, never, abort)) return;
     int b = 0;
     uint32_t k = 0;
     for (int it = 0; it < nmine; it++) {
@@ -537,11 +567,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
 #pragma unroll
         for (int kd = 0; kd < 8; kd++) {
             const int d = dir_at(kd);
-            if (!mbar_wait(full_bar + 8u * b, k & 1, kWaitLimitNs, abort)) {
-                *abort = 1;
-                atomicExch(&g_tma_status, 1);
-                return;
-            }
+            if (!consumer_wait(full_bar + 8u * b, k & 1, g.cwait_ns, abort)) return;
             const uint8_t *st = sbase + (size_t)b * g.stage_bytes;
             // element index and plane stride of the neighbour spinor and the
             // link, in the NY-row box or in the one-row box of a y stage
@@ -594,6 +620,8 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
     constexpr int kStages = SPLIT ? 12 : 6;  // B stages per tile
     extern __shared__ uint8_t smem_raw[];
     __shared__ int s_abort;
+    __shared__ __align__(8) uint64_t s_never;  // the stall test's barrier
+    const uint32_t never = smem_addr(&s_never);
     const uint32_t raw = smem_addr(smem_raw);
     const uint32_t pad = ((raw + 127u) & ~127u) - raw;
     const uint8_t *sbase = smem_raw + pad;
@@ -618,6 +646,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
             mbar_init(fullB + 8u * b, 1);
             mbar_init(emptyB + 8u * b, (uint32_t)g.ncw);
         }
+        mbar_init(never, 1);
         mbar_init_fence();
     }
     __syncthreads();
@@ -679,6 +708,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
     const int SM = g.NY * L0h;  // plane stride of an NY-row box, in elements
     const R sg = (R)g.g5_in;
     const bool top = j + 1 == g.NY, bottom = j == 0;
+    if (!stall_test_wait(g, never, abort)) return;
     int a = 0, b = 0;
     uint32_t ka = 0, kb = 0;
     for (int it = 0; it < nmine; it++) {
@@ -690,21 +720,13 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
         cx<R> acc[12];
 #pragma unroll
         for (int e = 0; e < 12; e++) acc[e] = {R(0), R(0)};
-        if (!mbar_wait(fullA + 8u * a, ka & 1, kWaitLimitNs, abort)) {
-            *abort = 1;
-            atomicExch(&g_tma_status, 1);
-            return;
-        }
+        if (!consumer_wait(fullA + 8u * a, ka & 1, g.cwait_ns, abort)) return;
         const uint8_t *sa = sbase + (size_t)a * g.a_bytes;
         const uint8_t *sps = nullptr;  // split: the spinor stage waiting for its link stage
         int bsp = 0;
 #pragma unroll
         for (int s = 0; s < kStages; s++) {
-            if (!mbar_wait(fullB + 8u * b, kb & 1, kWaitLimitNs, abort)) {
-                *abort = 1;
-                atomicExch(&g_tma_status, 1);
-                return;
-            }
+            if (!consumer_wait(fullB + 8u * b, kb & 1, g.cwait_ns, abort)) return;
             const uint8_t *st = sbase + (size_t)nA * g.a_bytes + (size_t)b * g.stage_bytes;
             // directions of this stage: one, or the forward and backward
             // terms of x or y for a two-link stage
@@ -845,6 +867,9 @@ int encode_map(CUtensorMap *m, const void *base, const Geom &g, int eb, int plan
 }
 
 std::atomic<bool> g_tma_launched{false};
+// failure-detection test hook (plqcd_tma_timeout_test): the consumer wait
+// limit of the stall test, 0 when off
+std::atomic<unsigned long long> g_stall_test_ns{0};
 
 int sm_count() {
     static int n[64] = {0};
@@ -1069,6 +1094,12 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     tg.a_low = a.a_low;
     tg.b = a.b;
     tg.g5_in = a.g5_in;
+    tg.cwait_ns = dev::kWaitLimitNs;
+    tg.stall = 0;
+    if (const unsigned long long ns = g_stall_test_ns.load(std::memory_order_relaxed)) {
+        tg.stall = 1;
+        tg.cwait_ns = ns;
+    }
     tg.out0 = a.out[0];
     tg.out1 = full ? a.out[1] : a.out[0];
     tg.x = a.x;
@@ -1129,3 +1160,18 @@ int dslash_tma_status(bool reset) {
 }
 
 }  // namespace plqcd
+
+// Failure-detection test of the bounded stage waits (the reference's
+// counterpart is the exit(1) of lib/dirac.c:128-130): see plqcd_b200.h.
+extern "C" int plqcd_tma_timeout_test(int enable, unsigned long long limit_ns) {
+    using namespace plqcd;
+    clear_error();
+    if (!enable) {
+        g_stall_test_ns.store(0, std::memory_order_relaxed);
+        return PLQCD_OK;
+    }
+    if (limit_ns < 1000ull || limit_ns > dev::kWaitLimitNs)
+        return set_error(PLQCD_ERR_ARG, "plqcd_tma_timeout_test: limit %llu ns outside 1 us .. 2 s", limit_ns);
+    g_stall_test_ns.store(limit_ns, std::memory_order_relaxed);
+    return PLQCD_OK;
+}

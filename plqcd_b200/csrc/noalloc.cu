@@ -2,14 +2,15 @@
 //
 // plqcd_spinor_norm2 takes its reduction scratch (per-block partial sums and
 // arrival counters) from the lattice workspace, which is grown with
-// cudaMalloc. Some callers cannot allow that: code that runs while a CUDA
-// graph is being captured in the global capture mode (where cudaMalloc is a
-// prohibited call), applications whose device memory must all come from
-// their own pool allocator, and latency-bound loops that cannot take the
-// device synchronisation cudaMalloc / cudaFree may imply. For them,
-// plqcd_spinor_norm2_noalloc runs the same reduction kernel with its scratch
-// in the file-scope device array below, which every GPU that loads the
-// library holds until the process exits.
+// cudaMalloc. Some callers cannot allow that: applications whose device
+// memory must all come from their own pool allocator (a framework that has
+// reserved the GPU's memory, or a service held to a fixed memory budget,
+// where an allocation outside the pool fails or breaks the budget), and
+// latency-bound loops that cannot take the device-wide synchronisation
+// cudaFree implies. For them, plqcd_spinor_norm2_noalloc runs the same
+// reduction kernel with its scratch in the file-scope device array below,
+// which every GPU that loads the library holds until the process exits.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -32,20 +33,53 @@ static __device__ __align__(256) unsigned char g_norm2_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void *g_scratch_ptr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // context ID the address belongs to
 
-// Device address of the scratch on the current device, looked up once per
-// device (the first call on each device does this).
+// ID of the current CUDA context (unique within the process, never reused),
+// 0 when the driver does not provide it
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr, *q = nullptr;
+        cudaDriverEntryPointQueryResult r1 = cudaDriverEntryPointSymbolNotFound, r2 = r1;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r1) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &q, cudaEnableDefault, &r2) == cudaSuccess &&
+            r1 == cudaDriverEntryPointSuccess && r2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrent>(p);
+            get_id = reinterpret_cast<GetId>(q);
+        } else {
+            cudaGetLastError();
+        }
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the scratch on the current device. The set-up (the
+// first call on a device, with that device current) looks it up with
+// cudaGetSymbolAddress and loads the reduction kernel of every precision.
+// The address belongs to the device's CUDA context: after cudaDeviceReset
+// the context is a new one, with a new ID, and the set-up runs again.
 int scratch_address(int device, void **out) {
     if (device < 0 || device >= kMaxDevices)
         return plqcd::set_error(PLQCD_ERR_ARG, "plqcd_spinor_norm2_noalloc: device %d out of range", device);
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[device]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_scratch_ptr[device] || g_scratch_ctx[device] != ctx) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_norm2_scratch);
         if (e != cudaSuccess || !p)
             return plqcd::set_error(PLQCD_ERR_CUDA, "plqcd_spinor_norm2_noalloc: cudaGetSymbolAddress: %s",
                                     cudaGetErrorString(e));
+        PLQCD_TRY(plqcd::preload_norm2_multi());
         g_scratch_ptr[device] = p;
+        g_scratch_ctx[device] = ctx;
     }
     *out = g_scratch_ptr[device];
     return PLQCD_OK;

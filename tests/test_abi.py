@@ -61,6 +61,8 @@ class GlobalParams(ctypes.Structure):
                 ("nn_bndo", ctypes.c_void_p * 8), ("iup", ctypes.POINTER(ctypes.POINTER(ctypes.c_int))),
                 ("idn", ctypes.POINTER(ctypes.POINTER(ctypes.c_int))),
                 ("ipt_eo_yzt", ctypes.POINTER(ctypes.c_int)), ("ipt_lex_yzt", ctypes.POINTER(ctypes.c_int)),
+                ("ipt_eo_sse_split", ctypes.c_void_p), ("ipt_lex_sse_split", ctypes.c_void_p),
+                ("iup_sse_split", ctypes.c_void_p), ("idn_sse_split", ctypes.c_void_p),
                 ("phip", ctypes.c_void_p * 4), ("phim", ctypes.c_void_p * 4), ("ALIGN", ctypes.c_int),
                 ("init", ctypes.c_int)]
 

@@ -90,6 +90,49 @@ def test_dropin_gauge_cache_sees_in_place_update(dropin, restatement):
     assert relmax(out[: V // 2], want[: V // 2]) < TOL64
 
 
+def test_dropin_reads_links_on_every_call_by_default(dropin, restatement):
+    """Without a registration the drop-in call reads the link array every
+    time, as the reference does: one link changed in place (far from any
+    sampled word) shows up in the next call's output."""
+    L = (4, 4, 4, 8)
+    dropin(L)
+    V = O.volume(L)
+    rng = np.random.default_rng(6)
+    q, u = O.gaussian_spinor(V, rng), O.random_su3(4 * V, rng)
+    out = np.zeros_like(q)
+    P.hopping_matrix("eo", q, out, u)
+    P.hopping_matrix("eo", q, out, u)
+    k = 4 * (V // 2 + 37) + 2                 # U_z at odd site 37, read by the even outputs
+    u[k] = O.random_su3(1, rng)[0]
+    P.hopping_matrix("eo", q, out, u)
+    want = restatement.hop("eo", L, q, u)
+    assert relmax(out[: V // 2], want[: V // 2]) < TOL64
+    _, h2d, _ = P.dropin_last_stats()
+    assert h2d >= 4 * V * 144                 # the links went up again
+
+
+def test_dropin_registered_links_are_uploaded_once(dropin, restatement):
+    """plqcd_gauge_update(u) registers the array: later calls reuse the
+    device copy (only the spinor parity goes up) until the next
+    plqcd_gauge_update, which picks up links changed in place."""
+    L = (4, 4, 4, 8)
+    dropin(L)
+    V = O.volume(L)
+    rng = np.random.default_rng(7)
+    q, u = O.gaussian_spinor(V, rng), O.random_su3(4 * V, rng)
+    P.lib().plqcd_gauge_update(u.ctypes.data)
+    out = np.zeros_like(q)
+    P.hopping_matrix("eo", q, out, u)
+    P.hopping_matrix("eo", q, out, u)
+    _, h2d, _ = P.dropin_last_stats()
+    assert h2d < 4 * V * 144                  # spinor parity only
+    assert relmax(out[: V // 2], restatement.hop("eo", L, q, u)[: V // 2]) < TOL64
+    u[4 * (V // 2 + 11) + 1] = O.random_su3(1, rng)[0]
+    P.lib().plqcd_gauge_update(u.ctypes.data)
+    P.hopping_matrix("eo", q, out, u)
+    assert relmax(out[: V // 2], restatement.hop("eo", L, q, u)[: V // 2]) < TOL64
+
+
 def _pinned(lib, shape):
     """complex128 array on amalloc'd (pinned) host memory, and its block"""
     n = int(np.prod(shape)) * 16
@@ -718,3 +761,48 @@ def test_tma_kernel_on_whole_slice_ranges(cuda, monkeypatch, variant):
     assert bool((plane[:, :S * 16] == 7).all()) and bool((plane[:, 5 * S * 16:] == 7).all())
     assert not bool((plane[:, S * 16:5 * S * 16] == 7).all())
     del torch
+
+
+@pytest.mark.parametrize("variant", ["1204", "2204", "4304"])
+def test_tma_wait_that_runs_out_reports_timeout(cuda, monkeypatch, variant):
+    """Failure detection of the bounded stage waits: with the test hook on,
+    each consumer warp of the TMA kernels waits (limit 200 us) on a barrier
+    that nothing completes. The wait runs out, the kernel returns after its
+    tile loads in flight have landed, plqcd_lattice_synchronize reports
+    PLQCD_ERR_TIMEOUT and clears the flag, and the next normal launch gives
+    the gather kernel's bits again."""
+    L = (16, 8, 6, 4)
+    lat, g64, u = _device_setup(L, 48)
+    bs = lat.spinor_bytes(P.F64)
+    fe, fo = dev_bytes(bs), dev_bytes(bs)
+    lat.spinor_gaussian(fe, P.F64, 0, 13)
+    lat.spinor_gaussian(fo, P.F64, 1, 14)
+    monkeypatch.setenv("PLQCD_DSLASH_BLOCK", "64")
+    monkeypatch.setenv("PLQCD_DSLASH_STAGES", "2")
+    re_, ro_ = dev_bytes(bs), dev_bytes(bs)
+    lat.dslash_full(g64, re_, ro_, fe, fo, P.F64)
+    lat.synchronize()
+    monkeypatch.setenv("PLQCD_DSLASH_STAGES", variant)
+    lib = P.lib()
+    oe, oo = dev_bytes(bs), dev_bytes(bs)
+    P.check(lib.plqcd_tma_timeout_test(1, 200_000))
+    try:
+        P.check(lib.plqcd_dslash_full(lat.handle, g64.handle, oe.data_ptr(), oo.data_ptr(), fe.data_ptr(),
+                                      fo.data_ptr(), P.F64))
+        rc = lib.plqcd_lattice_synchronize(lat.handle)
+    finally:
+        P.check(lib.plqcd_tma_timeout_test(0, 0))
+    assert rc == P.ERR_TIMEOUT, (rc, P.last_error())
+    assert "TMA stage wait ran out" in P.last_error()
+    assert lib.plqcd_lattice_synchronize(lat.handle) == 0   # flag cleared, context usable
+    lat.dslash_full(g64, oe, oo, fe, fo, P.F64)
+    lat.synchronize()
+    assert bool((oe == re_).all()) and bool((oo == ro_).all())
+
+
+def test_tma_timeout_test_hook_rejects_bad_limits(cuda):
+    lib = P.lib()
+    for ns in (0, 999, 3_000_000_000):
+        assert lib.plqcd_tma_timeout_test(1, ns) == -1
+        assert "outside 1 us .. 2 s" in P.last_error()
+    assert lib.plqcd_tma_timeout_test(0, 0) == 0

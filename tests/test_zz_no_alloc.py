@@ -1,8 +1,9 @@
 """plqcd_spinor_norm2_noalloc: the batched norm without any device allocation.
 
-It serves callers that cannot allocate device memory (stream capture in the
-global mode, pool-only applications, loops that cannot take the implicit
-synchronisation of cudaMalloc). Its result must equal plqcd_spinor_norm2's,
+It serves callers that cannot allocate device memory: applications whose
+device memory all comes from their own pool or budget, and latency-bound
+loops that cannot take cudaFree's device-wide synchronisation. Its result
+must equal plqcd_spinor_norm2's,
 which gets its scratch from the lattice workspace, call after call: the
 static scratch keeps the previous call's contents and must not leak into
 the next result. Collected last so that a failure here stops a -x run only
