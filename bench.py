@@ -349,6 +349,11 @@ def run_ours(args, d: Dist):
         if d.rank == 0:
             print(json.dumps({"only": "sharded", "sharded": res}))
         return 0
+    if args.only == "mrhs":  # the multi-RHS kernels alone (profiling runs)
+        res = run_mrhs(torch, P, lat, g64, args)
+        if d.rank == 0:
+            print(json.dumps({"only": "mrhs", "lattice": list(L), "mrhs_dslash": res}))
+        return 0
     if args.only == "cg":  # profiling runs of the solver section alone
         cg = run_cg(torch, P, lat, g64, buf, args)
         if d.rank == 0:
@@ -665,10 +670,14 @@ def run_cg(torch, P, lat, g64, buf, args):
 
 def run_mrhs(torch, P, lat, g64, args, nrhs=8):
     """Multi-RHS hopping throughput at the benchmark lattice: bytes per site
-    and RHS = 2 * spinor + 8 * link / nrhs."""
+    and RHS = 2 * spinor + 8 * link / nrhs. For the 16-bit formats the
+    tensor-core kernel (variant 3001) and the scalar kernels are also timed
+    forced, beside the tuner's choice."""
     res = {"nrhs": nrhs}
     for name, prec, recon, sb, lb in (("f64_18", P.F64, 18, 192, 144), ("f32_12", P.F32, 12, 96, 48),
-                                      ("f16_12", P.F16, 12, 52, 24)):
+                                      ("f16_12", P.F16, 12, 52, 24), ("bf16_12", P.BF16, 12, 52, 24)):
+        if args.mrhs_formats and name not in args.mrhs_formats.split(","):
+            continue
         g = g64 if (prec, recon) == (P.F64, 18) else P.Gauge(lat, prec, recon)
         if g is not g64:
             g.copy_from(g64)
@@ -677,11 +686,26 @@ def run_mrhs(torch, P, lat, g64, args, nrhs=8):
         o = torch.empty(nrhs * bs, dtype=torch.uint8, device="cuda")
         for r in range(nrhs):
             lat.spinor_gaussian(a[r * bs:(r + 1) * bs], prec, 1, 900 + r)
-        t = time_kernel(torch, lambda: lat.dslash_mrhs(g, o, a, nrhs, P.EVEN, prec), 20, 3) / 20 / 1e3
         per = lat.Vh * nrhs
-        res[name] = {"gflops": round(per * FLOP_PER_SITE / t / 1e9, 1),
-                     "gbs": round(per * (2 * sb + 8 * lb / nrhs) / t / 1e9, 1),
-                     "site_rhs_per_s": per / t}
+
+        def rate(t):
+            return {"gflops": round(per * FLOP_PER_SITE / t / 1e9, 1),
+                    "gbs": round(per * (2 * sb + 8 * lb / nrhs) / t / 1e9, 1),
+                    "site_rhs_per_s": per / t, "us": round(t * 1e6, 2)}
+
+        hop = lambda: lat.dslash_mrhs(g, o, a, nrhs, P.EVEN, prec)
+        res[name] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)
+        cfg = tuned_config(P, f"dslash_mrhs|p{prec}|r{recon}|plain|n{nrhs}|{lat.dims[0]}x")
+        res[name]["tuned_variant"] = cfg[0] if cfg else None
+        if prec in (P.F16, P.BF16):
+            forced = {}
+            for v, blk in ((3001, 128), (1042, 128), (1022, 64), (2, 128), (102, 128)):
+                os.environ["PLQCD_MRHS_VARIANT"], os.environ["PLQCD_MRHS_BLOCK"] = str(v), str(blk)
+                try:
+                    forced[str(v)] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)["us"]
+                finally:
+                    del os.environ["PLQCD_MRHS_VARIANT"], os.environ["PLQCD_MRHS_BLOCK"]
+            res[name]["forced_us"] = forced
         del a, o
         if g is not g64:
             del g
@@ -809,10 +833,11 @@ def main():
     ap.add_argument("--delta", type=float, default=0.01, help="reliable-update threshold of the mixed solvers")
     ap.add_argument("--lattice", default=",".join(map(str, L_BENCH)),
                     help="L0,L1,L2,L3 of the hopping-matrix workload (default 32,32,32,64)")
-    ap.add_argument("--only", choices=["all", "dslash", "cg", "sharded"], default="all",
+    ap.add_argument("--only", choices=["all", "dslash", "cg", "mrhs", "sharded"], default="all",
                     help="dslash / cg: only that section (profiling runs); sharded: the t-slab "
                          "decomposition with --shards slabs held on one GPU")
     ap.add_argument("--shards", type=int, default=4, help="slabs of --only sharded")
+    ap.add_argument("--mrhs-formats", default="", help="comma list of the multi-RHS formats to time (default all)")
     args = ap.parse_args()
     args.lattice = tuple(int(x) for x in args.lattice.split(","))
     d = Dist()

@@ -283,6 +283,10 @@ static int mrhs_dispatch(const Geom &g, cudaStream_t s, int prec, int recon, con
     }
 }
 
+int launch_dslash_mrhs_tc(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
+                          const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b,
+                          int tiles);
+
 // out (nrhs fields) = a_up/a_low * H in + b * x; tuned over RHS tile and block
 int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
                        const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b) {
@@ -336,6 +340,16 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
             cands.push_back(t);
         }
     }
+    // tensor-core kernel (dslash_mrhs_tc.cu), 16-bit fields with 12-real
+    // links: variant 3000 + RHS tiles of 8 per warp (block fixed at 128)
+    if ((prec == PLQCD_F16 || prec == PLQCD_BF16) && recon == 12 && nrhs >= 8)
+        for (int tiles : {1, 2, 4}) {
+            if (tiles > 1 && 8 * tiles > nrhs) continue;
+            TuneResult t;
+            t.variant = 3000 + tiles;
+            t.block = 128;
+            cands.push_back(t);
+        }
     DslashCall dc;
     dc.gauge = gauge;
     dc.prec = prec;
@@ -360,10 +374,16 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
             DslashCall c2 = dc;
             return launch_dslash_config(g, s, c2, t.variant - 100, t.block);
         }
+        if (t.variant >= 3000)
+            return launch_dslash_mrhs_tc(g, s, gauge, prec, recon, out, in, nrhs, out_parity, flags, a, x, b,
+                                         t.variant - 3000);
         return mrhs_dispatch(g, s, prec, recon, m, t.variant, t.block, xpay);
     }
     auto launch = [&](const TuneResult &t, char *dst) -> int {
-        if (t.variant >= 100) {
+        if (t.variant >= 3000)
+            return launch_dslash_mrhs_tc(g, s, gauge, prec, recon, dst, in, nrhs, out_parity, flags, a, x, b,
+                                         t.variant - 3000);
+        if (t.variant >= 100 && t.variant < 1000) {
             DslashCall c2 = dc;
             c2.out = dst;
             return launch_dslash_config(g, s, c2, t.variant - 100, t.block);

@@ -485,6 +485,45 @@ def test_multi_rhs_every_variant(cuda, monkeypatch, variant, block, prec, recon,
         assert relmax(a, b) <= tol, (variant, r, relmax(a, b))
 
 
+@pytest.mark.parametrize("tiles,nrhs", [(1, 8), (1, 12), (2, 16), (2, 20), (4, 32), (1, 3)])
+@pytest.mark.parametrize("prec,tol", [(P.F16, 2e-3), (P.BF16, 1.6e-2)])
+@pytest.mark.parametrize("xpay", [False, True])
+def test_multi_rhs_tensor_core_kernel(cuda, monkeypatch, tiles, nrhs, prec, tol, xpay):
+    """The tensor-core multi-RHS kernel (mma.sync m16n8k8, 16-bit operands,
+    FP32 accumulation; variant 3000 + RHS tiles of 8 per warp), forced past
+    the tuner, agrees with the scalar single-RHS kernel for every field of
+    the block within the 16-bit storage error (relative L2), including
+    partial tiles, the xpay / gamma5 epilogue and both output parities."""
+    L = (8, 4, 6, 8)
+    lat, g64, u = _device_setup(L, 23)
+    g = P.Gauge(lat, prec, 12)
+    g.copy_from(g64)
+    bs = lat.spinor_bytes(prec)
+    for par in (0, 1):
+        blk_in, blk_out, blk_x = dev_bytes(nrhs * bs), dev_bytes(nrhs * bs), dev_bytes(nrhs * bs)
+        for r in range(nrhs):
+            lat.spinor_gaussian(blk_in[r * bs:(r + 1) * bs], prec, 1 - par, 500 + r)
+            lat.spinor_gaussian(blk_x[r * bs:(r + 1) * bs], prec, par, 600 + r)
+        flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT if xpay else 0
+        monkeypatch.setenv("PLQCD_MRHS_VARIANT", str(3000 + tiles))
+        if xpay:
+            lat.dslash_mrhs_xpay(g, blk_out, blk_in, nrhs, par, prec, 0.37, blk_x, -1.5, flags)
+        else:
+            lat.dslash_mrhs(g, blk_out, blk_in, nrhs, par, prec)
+        monkeypatch.delenv("PLQCD_MRHS_VARIANT")
+        half = slice(0, lat.V // 2) if par == 0 else slice(lat.V // 2, lat.V)
+        for r in range(nrhs):
+            sl = slice(r * bs, (r + 1) * bs)
+            one = dev_bytes(bs)
+            if xpay:
+                lat.dslash_xpay(g, one, blk_in[sl], par, prec, 0.37, blk_x[sl], -1.5, flags)
+            else:
+                lat.dslash(g, one, blk_in[sl], par, prec)
+            a = field_to_host(lat, blk_out[sl], prec, par)[half]
+            b = field_to_host(lat, one, prec, par)[half]
+            assert rel_l2(a, b) <= tol, (par, r, rel_l2(a, b))
+
+
 @pytest.mark.parametrize("variant", ["sse3_intrin_nohalfspinor", "avx_nohalfspinor", "single_mic_split",
                                      "single_mic_split_nohalfspinor", "single_mic_split_nohalfspinor_short"])
 def test_split_layout_entry_points(dropin, restatement, variant):
@@ -790,10 +829,11 @@ def test_tma_wait_that_runs_out_reports_timeout(cuda, monkeypatch, variant):
         P.check(lib.plqcd_dslash_full(lat.handle, g64.handle, oe.data_ptr(), oo.data_ptr(), fe.data_ptr(),
                                       fo.data_ptr(), P.F64))
         rc = lib.plqcd_lattice_synchronize(lat.handle)
+        msg = P.last_error()
     finally:
         P.check(lib.plqcd_tma_timeout_test(0, 0))
-    assert rc == P.ERR_TIMEOUT, (rc, P.last_error())
-    assert "TMA stage wait ran out" in P.last_error()
+    assert rc == P.ERR_TIMEOUT, (rc, msg)
+    assert "TMA stage wait ran out" in msg
     assert lib.plqcd_lattice_synchronize(lat.handle) == 0   # flag cleared, context usable
     lat.dslash_full(g64, oe, oo, fe, fo, P.F64)
     lat.synchronize()
