@@ -118,185 +118,300 @@ __device__ __forceinline__ uint32_t tc_mult(int imag, float f) {
     return imag ? Half2<PREC>::pack(-f, f) : Half2<PREC>::pack(f, f);
 }
 
+// asynchronous global -> shared copies that write zeros when `valid` is
+// false (source size 0: nothing is read; the address is still a valid one)
+__device__ __forceinline__ void cp_async16_zf(uint32_t dst, const void *src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4_zf(uint32_t dst, const void *src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 4 : 0)
+                 : "memory");
+}
+
+// the B fragment of M[cr][t] for lane (g, t), from its (re, im) in FP32:
+// g even: (Re, -Im), g odd: (Im, Re) (columns 2c and 2c + 1 of the real form)
+template <int PREC>
+__device__ __forceinline__ uint32_t b_frag(float2 m, int g) {
+    return (g & 1) ? Half2<PREC>::pack(m.y, m.x) : Half2<PREC>::pack(m.x, -m.y);
+}
+
+// Shared memory of one warp: 2 stages x NT tiles; a tile holds, for the 8
+// RHS of the tile, the neighbour spinor (record g: 12 words = the 3 planes
+// of 16 bytes, complex number 3 s + c at word 3 s + c) and its norm
+// (word 96 + g). Lane (g, t < 3) copies plane t of RHS g, lane (g, 3) the
+// norm; the fragment reads (word 12 g + 3 s + t) hit 24 distinct banks.
+constexpr int kTcTileWords = 8 * 12 + 8;
+constexpr int kTcWarps = 4;
+
 template <int PREC, int NT, bool XPAY>
-__global__ void __launch_bounds__(128) k_dslash_mrhs_tc(const TcArgs a) {
-    const int lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(32 * kTcWarps) k_dslash_mrhs_tc(const TcArgs a) {
+    // 3 buffers per warp: stages 0 / 1 of the direction pipeline and the
+    // epilogue's (xpay operand in, output out)
+    constexpr int kStage = NT * kTcTileWords;
+    __shared__ __align__(16) uint32_t smem[kTcWarps][3][kStage];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    const long h = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (h >= a.Vh) return;  // warp-uniform
+    // the warp's chunk: 32 consecutive sites; lane i works out the neighbour
+    // indices of site h0 + i once (32-bit), the loop below takes them by shuffle
+    const int Vh = (int)a.Vh;
+    const int h0 = (blockIdx.x * kTcWarps + w) * 32;
+    if (h0 >= Vh) return;  // warp-uniform
+    const int nsite = min(32, Vh - h0);
     const int rhs0 = blockIdx.y * 8 * NT;
     const int par = a.out_parity, opp = par ^ 1;
-    const long Vh = a.Vh;
-    const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
-    const Coords c = site_coords(h, par, L0h, L1, L2);
-    const int xh = (int)(h - c.row * L0h);
-    const long L01 = L1, L012 = (long)L1 * L2;
-    const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
-    const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
-    long nb[8];
-    nb[0] = (xp >> 1) + L0h * c.row;
-    nb[1] = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
-    nb[2] = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
-    nb[3] = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
-    nb[4] = (xm >> 1) + L0h * c.row;
-    nb[5] = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
-    nb[6] = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
-    nb[7] = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
-
-    // link of direction d: forward U_mu(x) (this parity, this site),
-    // backward U_mu(x - mu) (other parity, neighbour `site`); complex
-    // element idx = 3 row + col of rows 0, 1
-    const uint32_t *gw = static_cast<const uint32_t *>(a.gauge);
-    auto link_word = [&](int d, long site, int idx) -> uint32_t {
-        const int blk = d < 4 ? par * 4 + d : opp * 4 + (d - 4);
-        return __ldg(gw + (((long)blk * 3 + (idx >> 1)) * Vh + site) * 2 + (idx & 1));
-    };
-    // row 2 of the eight links, rebuilt once per site: lane (g, t < 3)
-    // computes U_g[2][t] = conj(U[0][t1] U[1][t2] - U[0][t2] U[1][t1]) of
-    // direction g (its site picked by selects: nb stays in registers)
-    float2 r2 = make_float2(0.f, 0.f);
-    if (t < 3) {
-        long sg_site = h;
-#pragma unroll
-        for (int d = 4; d < 8; d++) sg_site = g == d ? nb[d] : sg_site;
-        const int t1 = t == 2 ? 0 : t + 1, t2 = t == 0 ? 2 : t - 1;
-        const float2 a1 = Half2<PREC>::unpack(link_word(g, sg_site, t1));
-        const float2 b2 = Half2<PREC>::unpack(link_word(g, sg_site, 3 + t2));
-        const float2 a2 = Half2<PREC>::unpack(link_word(g, sg_site, t2));
-        const float2 b1 = Half2<PREC>::unpack(link_word(g, sg_site, 3 + t1));
-        const float re = (a1.x * b2.x - a1.y * b2.y) - (a2.x * b1.x - a2.y * b1.y);
-        const float im = (a1.x * b2.y + a1.y * b2.x) - (a2.x * b1.y + a2.y * b1.x);
-        r2 = make_float2(re, -im);
+    int nbl[8];
+    {
+        const int hl = min(h0 + lane, Vh - 1);
+        const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
+        const int row = hl / L0h, xh = hl - row * L0h;
+        const int y = row % L1, zt = row / L1, z = zt % L2, tt = zt / L2;
+        const int x = 2 * xh + ((y + z + tt + par) & 1);
+        const int xp = (x + 1 == a.L0) ? 0 : x + 1, xm = (x == 0) ? a.L0 - 1 : x - 1;
+        const int L01 = L1, L012 = L1 * L2;
+        nbl[0] = (xp >> 1) + L0h * row;
+        nbl[1] = xh + L0h * (row + ((y + 1 == L1) ? -(L1 - 1) : 1));
+        nbl[2] = xh + L0h * (row + ((z + 1 == L2) ? -(L2 - 1) * L01 : L01));
+        nbl[3] = xh + L0h * (row + ((tt + 1 == L3) ? -(L3 - 1) * L012 : L012));
+        nbl[4] = (xm >> 1) + L0h * row;
+        nbl[5] = xh + L0h * (row + ((y == 0) ? (L1 - 1) : -1));
+        nbl[6] = xh + L0h * (row + ((z == 0) ? (L2 - 1) * L01 : -L01));
+        nbl[7] = xh + L0h * (row + ((tt == 0) ? (L3 - 1) * L012 : -L012));
     }
 
-    // byte offsets of psi(spin s, colour t) inside a site of a field: the
-    // complex number 3 s + t sits in plane (3 s + t) / 4, slot (3 s + t) % 4
-    const int tc = t < 3 ? t : 0;
-    long off[4];
-#pragma unroll
-    for (int s = 0; s < 4; s++) {
-        const int idx = 3 * s + tc;
-        off[s] = (long)(idx >> 2) * Vh * 16 + (idx & 3) * 4;
-    }
-    const long norm_off = 3 * Vh * 16;
-
-    // accumulators: lane (g, t < 3) owns spins 0..3 at colour t of RHS
-    // rhs0 + 8 j + g, j < NT
-    cx<float> acc[NT][4];
-#pragma unroll
-    for (int j = 0; j < NT; j++)
-#pragma unroll
-        for (int s = 0; s < 4; s++) acc[j][s] = {0.f, 0.f};
-
-    const float sg_in = a.g5_in;
-#pragma unroll
-    for (int kd = 0; kd < 8; kd++) {
-        const int d = dir_at(kd);
-        const int mu = d & 3;
-        const bool fwd = d < 4;
-        // B fragment: M[cr][t] with cr = g / 2, M = U (forward) or U^dag
-        // (backward: conj(U[t][cr])); row 2 from the lane that rebuilt it
-        const int cr = g >> 1;
-        const int row = fwd ? cr : t, col = fwd ? t : cr;
-        const float2 sh = make_float2(__shfl_sync(0xffffffffu, r2.x, 4 * d + (col < 3 ? col : 0)),
-                                      __shfl_sync(0xffffffffu, r2.y, 4 * d + (col < 3 ? col : 0)));
-        uint32_t b0 = 0;
-        if (g < 6 && t < 3) {
-            float2 m = row < 2 ? Half2<PREC>::unpack(link_word(d, fwd ? h : nb[d], 3 * row + col)) : sh;
-            if (!fwd) m.y = -m.y;  // U^dag: conjugate
-            b0 = (g & 1) ? Half2<PREC>::pack(m.y, m.x) : Half2<PREC>::pack(m.x, -m.y);
-        }
-        // projection multipliers; backward and gamma5-on-input flip the
-        // lower-spin sign
-        const float sg = fwd ? sg_in : -sg_in;
-        const uint32_t f0 = tc_mult<PREC>(tc_imag(mu), sg * tc_sign(mu, 0));
-        const uint32_t f1 = tc_mult<PREC>(tc_imag(mu), sg * tc_sign(mu, 1));
-        const int s0 = tc_sigma(mu, 0), s1 = tc_sigma(mu, 1);
-        const long nsite = nb[d] * 16;
-#pragma unroll
-        for (int j = 0; j < NT; j++) {
-            const int r = rhs0 + 8 * j + g;
-            uint32_t a0 = 0, a1 = 0;
-            float n = 0.f;
-            if (t < 3 && r < a.nrhs) {
-                const char *f = a.in + (size_t)r * a.fbytes;
-                const uint32_t p0 = __ldg(reinterpret_cast<const uint32_t *>(f + nsite + off[0]));
-                const uint32_t p1 = __ldg(reinterpret_cast<const uint32_t *>(f + nsite + off[1]));
-                uint32_t q0 = __ldg(reinterpret_cast<const uint32_t *>(f + nsite + off[s0]));
-                uint32_t q1 = __ldg(reinterpret_cast<const uint32_t *>(f + nsite + off[s1]));
-                n = __ldg(reinterpret_cast<const float *>(f + norm_off) + nb[d]);
-                if (tc_imag(mu)) {
-                    q0 = swap_halves(q0);
-                    q1 = swap_halves(q1);
-                }
-                a0 = H2<PREC>::fma(q0, f0, p0);
-                a1 = H2<PREC>::fma(q1, f1, p1);
-            }
-            float dd[4] = {0.f, 0.f, 0.f, 0.f};
-            mma_16x8x8<PREC>(dd, a0, a1, b0);
-            // chi0 = (dd[0], dd[1]), chi1 = (dd[2], dd[3]); rebuild as
-            // dslash_core.cuh::accumulate (LS = +1 forward, -1 backward)
-            const float p = fwd ? n : -n, q = -p;
-            cx<float> *o = acc[j];
-            o[0] = {fmaf(n, dd[0], o[0].re), fmaf(n, dd[1], o[0].im)};
-            o[1] = {fmaf(n, dd[2], o[1].re), fmaf(n, dd[3], o[1].im)};
-            if (mu == 0) {
-                o[2] = {fmaf(p, dd[0], o[2].re), fmaf(p, dd[1], o[2].im)};
-                o[3] = {fmaf(p, dd[2], o[3].re), fmaf(p, dd[3], o[3].im)};
-            } else if (mu == 1) {
-                o[2] = {fmaf(p, dd[3], o[2].re), fmaf(q, dd[2], o[2].im)};
-                o[3] = {fmaf(p, dd[1], o[3].re), fmaf(q, dd[0], o[3].im)};
-            } else if (mu == 2) {
-                o[2] = {fmaf(q, dd[2], o[2].re), fmaf(q, dd[3], o[2].im)};
-                o[3] = {fmaf(p, dd[0], o[3].re), fmaf(p, dd[1], o[3].im)};
-            } else {
-                o[2] = {fmaf(p, dd[1], o[2].re), fmaf(q, dd[0], o[2].im)};
-                o[3] = {fmaf(q, dd[3], o[3].re), fmaf(p, dd[2], o[3].im)};
-            }
-        }
-    }
-
-    // epilogue: a_up / a_low (gamma5 on output) [+ b x], then the 16-bit
-    // store with the site norm = max |component| over the quad's lanes
+    // the lane's source: plane t (t < 3) or the norm plane (t = 3) of RHS
+    // rhs0 + 8 j + g; RHS past the block copy zeros from a valid address
+    const char *src[NT];
+    bool valid[NT];
+    const long plane_off = t < 3 ? (long)t * Vh * 16 : 3L * Vh * 16;
+    const int esz = t < 3 ? 16 : 4;
 #pragma unroll
     for (int j = 0; j < NT; j++) {
         const int r = rhs0 + 8 * j + g;
-        const bool mine = t < 3 && r < a.nrhs;
-        cx<float> v[4];
+        valid[j] = r < a.nrhs;
+        src[j] = a.in + (size_t)(valid[j] ? r : 0) * a.fbytes + plane_off;
+    }
+    const uint32_t s_warp = smem_addr(&smem[w][0][0]);
+    const uint32_t dst_lane = 4u * (t < 3 ? (uint32_t)(12 * g + 4 * t) : (uint32_t)(96 + g));
+    // copies of direction kd's neighbour (site index n) into stage kd & 1
+    auto issue = [&](int kd, int n) {
+        const uint32_t sb = s_warp + 4u * (uint32_t)((kd & 1) * kStage) + dst_lane;
 #pragma unroll
-        for (int s = 0; s < 4; s++) {
-            const float as = s < 2 ? a.a_up : a.a_low;
-            v[s] = {as * acc[j][s].re, as * acc[j][s].im};
+        for (int j = 0; j < NT; j++) {
+            const uint32_t dst = sb + 4u * (uint32_t)(j * kTcTileWords);
+            const char *p = src[j] + (long)n * esz;
+            if (t < 3)
+                cp_async16_zf(dst, p, valid[j]);
+            else
+                cp_async4_zf(dst, p, valid[j]);
         }
-        if (XPAY && mine) {
-            const char *f = a.x + (size_t)r * a.fbytes;
-            const float nx = __ldg(reinterpret_cast<const float *>(f + norm_off) + h) * a.b;
+        cp_async_commit();
+    };
+    const uint32_t *gw = static_cast<const uint32_t *>(a.gauge);
+    const long Vh2 = 2L * Vh;
+    // 32-bit word of complex element idx (= 3 row + col, rows 0, 1) of the
+    // link block blk (parity * 4 + mu) at `site`
+    auto link_word = [&](int blk, int site, int idx) -> uint32_t {
+        return __ldg(gw + ((long)blk * 3 + (idx >> 1)) * Vh2 + 2L * site + (idx & 1));
+    };
+    const float sgi = a.g5_in;
+    const uint32_t m_re[2] = {Half2<PREC>::pack(sgi, sgi), Half2<PREC>::pack(-sgi, -sgi)};
+    const uint32_t m_im[2] = {Half2<PREC>::pack(-sgi, sgi), Half2<PREC>::pack(sgi, -sgi)};
+
+    int nb[8];
+#pragma unroll
+    for (int d = 0; d < 8; d++) nb[d] = __shfl_sync(0xffffffffu, nbl[d], 0);
+    issue(0, nb[0]);
+    issue(1, nb[4]);
+
+    for (int k = 0; k < nsite; k++) {
+        const int h = h0 + k;
+        // row 2 of the eight links of site h: lane (g, t < 3) computes
+        // U_g[2][t] = conj(U[0][t1] U[1][t2] - U[0][t2] U[1][t1]) of
+        // direction g (forward: this site; backward: the neighbour)
+        float2 r2 = make_float2(0.f, 0.f);
+        if (t < 3) {
+            int lsite = h;
+#pragma unroll
+            for (int d = 4; d < 8; d++) lsite = g == d ? nb[d] : lsite;
+            const int blk = g < 4 ? par * 4 + g : opp * 4 + (g - 4);
+            const int t1 = t == 2 ? 0 : t + 1, t2 = t == 0 ? 2 : t - 1;
+            const float2 a1 = Half2<PREC>::unpack(link_word(blk, lsite, t1));
+            const float2 b2 = Half2<PREC>::unpack(link_word(blk, lsite, 3 + t2));
+            const float2 a2 = Half2<PREC>::unpack(link_word(blk, lsite, t2));
+            const float2 b1 = Half2<PREC>::unpack(link_word(blk, lsite, 3 + t1));
+            const float re = (a1.x * b2.x - a1.y * b2.y) - (a2.x * b1.x - a2.y * b1.y);
+            const float im = (a1.x * b2.y + a1.y * b2.x) - (a2.x * b1.y + a2.y * b1.x);
+            r2 = make_float2(re, -im);
+        }
+
+        float2 acc[NT][4];
+#pragma unroll
+        for (int j = 0; j < NT; j++)
+#pragma unroll
+            for (int s = 0; s < 4; s++) acc[j][s] = make_float2(0.f, 0.f);
+
+#pragma unroll
+        for (int kd = 0; kd < 8; kd++) {
+            const int d = dir_at(kd);
+            const int mu = d & 3;
+            const bool fwd = d < 4;
+            const bool imag = mu == 1 || mu == 3;  // the lower spins take a factor i
+            // B fragment: M[cr][t] with cr = g / 2, M = U (forward) or U^dag
+            // (backward: conj(U[t][cr])); row 2 from the lane that rebuilt it.
+            // For mu 1 and 3 a second fragment holds i M, so that the mma
+            // also returns i chi for the lower spins.
+            const int cr = g >> 1;
+            const int row = fwd ? cr : t, col = fwd ? t : cr;
+            const int srcl = 4 * d + (col < 3 ? col : 0);
+            const float2 sh = make_float2(__shfl_sync(0xffffffffu, r2.x, srcl), __shfl_sync(0xffffffffu, r2.y, srcl));
+            float2 m = make_float2(0.f, 0.f);
+            if (g < 6 && t < 3) {
+                m = row < 2 ? Half2<PREC>::unpack(link_word(fwd ? par * 4 + mu : opp * 4 + mu, fwd ? h : nb[d],
+                                                            3 * row + col))
+                            : sh;
+                if (!fwd) m.y = -m.y;  // U^dag: conjugate
+            }
+            const uint32_t b0 = b_frag<PREC>(m, g);
+            const uint32_t bi = imag ? b_frag<PREC>(make_float2(-m.y, m.x), g) : 0u;
+            // projection: spin s (0, 1) pairs with spin sigma(s) of the lower
+            // half; the sign carries the direction (forward +, backward -)
+            const int sg0 = (fwd ? 1 : -1) * tc_sign(mu, 0), sg1 = (fwd ? 1 : -1) * tc_sign(mu, 1);
+            const uint32_t f0 = imag ? m_im[sg0 > 0 ? 0 : 1] : m_re[sg0 > 0 ? 0 : 1];
+            const uint32_t f1 = imag ? m_im[sg1 > 0 ? 0 : 1] : m_re[sg1 > 0 ? 0 : 1];
+            const int s0 = tc_sigma(mu, 0), s1 = tc_sigma(mu, 1);
+            if (kd < 7)
+                cp_async_wait<1>();
+            else
+                cp_async_wait<0>();
+            __syncwarp();
+            const uint32_t *st = &smem[w][kd & 1][0];
+            const float LS = fwd ? 1.f : -1.f;
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const uint32_t *rec = st + j * kTcTileWords + 12 * g;
+                uint32_t a0 = 0, a1 = 0;
+                if (t < 3) {
+                    uint32_t q0 = rec[3 * s0 + t], q1 = rec[3 * s1 + t];
+                    if (imag) {
+                        q0 = swap_halves(q0);
+                        q1 = swap_halves(q1);
+                    }
+                    a0 = H2<PREC>::fma(q0, f0, rec[t]);
+                    a1 = H2<PREC>::fma(q1, f1, rec[3 + t]);
+                }
+                const float n = *reinterpret_cast<const float *>(st + j * kTcTileWords + 96 + g);
+                float dd[4] = {0.f, 0.f, 0.f, 0.f}, di[4] = {0.f, 0.f, 0.f, 0.f};
+                mma_16x8x8<PREC>(dd, a0, a1, b0);
+                if (imag) mma_16x8x8<PREC>(di, a0, a1, bi);
+                // rebuild as dslash_core.cuh::accumulate: spins 0, 1 += n chi;
+                // spins 2, 3 from chi (mu 0, 2) or i chi (mu 1, 3) with the
+                // direction's signs (p = LS n, q = -p)
+                const float2 nn = make_float2(n, n), pp = make_float2(LS * n, LS * n);
+                const float2 qq = make_float2(-LS * n, -LS * n);
+                const float2 c0 = make_float2(dd[0], dd[1]), c1 = make_float2(dd[2], dd[3]);
+                const float2 i0 = make_float2(di[0], di[1]), i1 = make_float2(di[2], di[3]);
+                float2 *o = acc[j];
+                o[0] = __ffma2_rn(nn, c0, o[0]);
+                o[1] = __ffma2_rn(nn, c1, o[1]);
+                if (mu == 0) {
+                    o[2] = __ffma2_rn(pp, c0, o[2]);
+                    o[3] = __ffma2_rn(pp, c1, o[3]);
+                } else if (mu == 1) {
+                    o[2] = __ffma2_rn(qq, i1, o[2]);
+                    o[3] = __ffma2_rn(qq, i0, o[3]);
+                } else if (mu == 2) {
+                    o[2] = __ffma2_rn(qq, c1, o[2]);
+                    o[3] = __ffma2_rn(pp, c0, o[3]);
+                } else {
+                    o[2] = __ffma2_rn(qq, i0, o[2]);
+                    o[3] = __ffma2_rn(pp, i1, o[3]);
+                }
+            }
+            __syncwarp();  // every lane has read this stage before it is refilled
+            if (kd + 2 < 8) issue(kd + 2, nb[dir_at(kd + 2)]);
+        }
+
+        // the next site's first two directions go in flight during this
+        // site's epilogue
+        if (k + 1 < nsite) {
+#pragma unroll
+            for (int d = 0; d < 8; d++) nb[d] = __shfl_sync(0xffffffffu, nbl[d], k + 1);
+            issue(0, nb[0]);
+            issue(1, nb[4]);
+        }
+
+        // epilogue: a_up / a_low (gamma5 on output) [+ b x], then the 16-bit
+        // store with the site norm = max |component| over the quad's lanes,
+        // through the epilogue buffer (whole 16-byte planes per lane)
+        uint32_t *eb = &smem[w][2][0];
+        const uint32_t s_eb = s_warp + 4u * (uint32_t)(2 * kStage);
+        float2 xv[NT][4];
+        float xn[NT];
+        if (XPAY) {
+            const long xoff = t < 3 ? (long)t * Vh * 16 + (long)h * 16 : 3L * Vh * 16 + (long)h * 4;
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const char *p = a.x + (size_t)(valid[j] ? rhs0 + 8 * j + g : 0) * a.fbytes + xoff;
+                const uint32_t dst = s_eb + dst_lane + 4u * (uint32_t)(j * kTcTileWords);
+                if (t < 3)
+                    cp_async16_zf(dst, p, valid[j]);
+                else
+                    cp_async4_zf(dst, p, valid[j]);
+            }
+            cp_async_commit();
+            cp_async_wait<0>();  // (also completes the next site's two stages)
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const uint32_t *rec = eb + j * kTcTileWords + 12 * g;
+                xn[j] = *reinterpret_cast<const float *>(eb + j * kTcTileWords + 96 + g) * a.b;
+#pragma unroll
+                for (int s = 0; s < 4; s++) xv[j][s] = t < 3 ? Half2<PREC>::unpack(rec[3 * s + t]) : make_float2(0.f, 0.f);
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+            const bool mine = t < 3 && valid[j];
+            float2 v[4];
 #pragma unroll
             for (int s = 0; s < 4; s++) {
-                const float2 w = Half2<PREC>::unpack(__ldg(reinterpret_cast<const uint32_t *>(f + h * 16 + off[s])));
-                v[s] = {fmaf(nx, w.x, v[s].re), fmaf(nx, w.y, v[s].im)};
+                const float as = s < 2 ? a.a_up : a.a_low;
+                v[s] = __fmul2_rn(make_float2(as, as), acc[j][s]);
+                if (XPAY) v[s] = __ffma2_rn(make_float2(xn[j], xn[j]), xv[j][s], v[s]);
+            }
+            float mx = 0.f;
+            if (mine)
+#pragma unroll
+                for (int s = 0; s < 4; s++) mx = fmaxf(mx, fmaxf(fabsf(v[s].x), fabsf(v[s].y)));
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+            const float inv = mx > 0.f ? 1.f / mx : 0.f;
+            uint32_t *rec = eb + j * kTcTileWords + 12 * g;
+            if (t < 3)
+#pragma unroll
+                for (int s = 0; s < 4; s++) rec[3 * s + t] = Half2<PREC>::pack(v[s].x * inv, v[s].y * inv);
+            __syncwarp();
+            if (valid[j]) {
+                char *f = a.out + (size_t)(rhs0 + 8 * j + g) * a.fbytes;
+                if (t < 3)
+                    *reinterpret_cast<uint4 *>(f + (long)t * Vh * 16 + (long)h * 16) =
+                        *reinterpret_cast<const uint4 *>(rec + 4 * t);
+                else
+                    reinterpret_cast<float *>(f + 3L * Vh * 16)[h] = mx;
             }
         }
-        float m = 0.f;
-        if (mine)
-#pragma unroll
-            for (int s = 0; s < 4; s++) m = fmaxf(m, fmaxf(fabsf(v[s].re), fabsf(v[s].im)));
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
-        if (!mine) continue;
-        const float inv = m > 0.f ? 1.f / m : 0.f;
-        char *f = a.out + (size_t)r * a.fbytes;
-#pragma unroll
-        for (int s = 0; s < 4; s++)
-            *reinterpret_cast<uint32_t *>(f + h * 16 + off[s]) = Half2<PREC>::pack(v[s].re * inv, v[s].im * inv);
-        if (t == 0) reinterpret_cast<float *>(f + norm_off)[h] = m;
+        __syncwarp();  // the epilogue buffer is free for the next site
     }
 }
 
 template <int PREC, int NT>
 int launch_tc_nt(cudaStream_t s, const TcArgs &a, bool xpay) {
-    constexpr int kWarps = 4;
-    const long nblk = (a.Vh + kWarps - 1) / kWarps;
+    constexpr int kWarps = kTcWarps;
+    if (a.Vh > 0x3fffffffL) return set_error(PLQCD_ERR_ARG, "dslash_mrhs_tc: lattice too large");
+    const long nchunk = (a.Vh + 31) / 32;  // 32 consecutive sites per warp
+    const long nblk = (nchunk + kWarps - 1) / kWarps;
     const int ngroups = (a.nrhs + 8 * NT - 1) / (8 * NT);
     if (nblk > 0x7fffffffL || ngroups > 65535) return set_error(PLQCD_ERR_ARG, "dslash_mrhs_tc: grid too large");
     dim3 grid((unsigned)nblk, (unsigned)ngroups);
