@@ -316,9 +316,12 @@ __global__ void k_ctl_loop(McgControl *c, const McgState *st, int nst, int use_h
 
 namespace {
 
-inline int red_blocks(long Vh) {
-    long b = (Vh + kBlasBlock - 1) / kBlasBlock;
-    return (int)std::min<long>(b, 296);
+// blocks per RHS of the batched BLAS kernels: about kMaxRedBlocks (8 per
+// SM) in all, at least one per SM per RHS
+inline int red_blocks(long Vh, int nrhs) {
+    const long b = (Vh + kBlasBlock - 1) / kBlasBlock;
+    const long per = std::max<long>(148, kMaxRedBlocks / std::max(nrhs, 1));
+    return (int)std::min<long>(b, per);
 }
 
 #define MCG_PREC_SWITCH(prec, F)                                                     \
@@ -481,7 +484,7 @@ int setup_item(Batch &B, Item &it) {
     it.fbs = spinor_parity_bytes(Vh, it.ps);
     it.fbx = spinor_parity_bytes(Vh, it.xprec);
     it.st.nrhs = n;
-    it.st.nb = red_blocks(Vh);
+    it.st.nb = red_blocks(Vh, n);
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t need = 4 * al(it.fb64 * n) + 5 * al(it.fbs * n) + al(it.fbx * n) + 10 * al(sizeof(double) * n) +
                         2 * al(sizeof(int) * n) + al(sizeof(double) * n * it.st.nb) + al(sizeof(unsigned) * n);
@@ -519,15 +522,25 @@ int setup_item(Batch &B, Item &it) {
     // b' = b_e + kappa H_eo b_o ; |b'|^2 ; r = Mhat^dag b' (x = 0) ; |r|^2
     PLQCD_TRY(B.hop(it, in.g64, it.bprime, in.b_odd, PLQCD_EVEN, 0, in.b_even, B.kappa, 1.0));
     PLQCD_TRY(B.norm2(it, it.bprime, PLQCD_F64, M_BP2, false));
-    PLQCD_TRY(B.mhat(it, in.g64, it.r64, it.bprime, it.tmp64, true));
-    PLQCD_TRY(B.norm2(it, it.r64, PLQCD_F64, M_RR_INIT, false));
     PLQCD_CUDA_TRY(cudaMemsetAsync(in.x_even, 0, it.fb64 * n, s));
     PLQCD_CUDA_TRY(cudaMemsetAsync(it.xs, 0, it.fbx * n, s));
-    PLQCD_TRY(B.convert(it, it.rs, it.ps, it.r64, PLQCD_F64));
-    PLQCD_TRY(B.convert(it, it.p, it.ps, it.r64, PLQCD_F64));
+    const plqcd_gauge *gs = in.g_sloppy ? in.g_sloppy : in.g64;
+    if (B.mixed) {
+        // the start residual Mhat^dag b' only seeds the sloppy recursion (the
+        // FP64 Schur residual of b', which decides convergence, does not use
+        // it), so the sloppy operator computes it, as in plqcd_invert_cg
+        PLQCD_TRY(B.convert(it, it.t, it.ps, it.bprime, PLQCD_F64));
+        PLQCD_TRY(B.mhat(it, gs, it.rs, it.t, it.tmps, true));
+        PLQCD_TRY(B.norm2(it, it.rs, it.ps, M_RR_INIT, false));
+        PLQCD_CUDA_TRY(cudaMemcpyAsync(it.p, it.rs, it.fbs * n, cudaMemcpyDeviceToDevice, s));
+    } else {
+        PLQCD_TRY(B.mhat(it, in.g64, it.r64, it.bprime, it.tmp64, true));
+        PLQCD_TRY(B.norm2(it, it.r64, PLQCD_F64, M_RR_INIT, false));
+        PLQCD_TRY(B.convert(it, it.rs, it.ps, it.r64, PLQCD_F64));
+        PLQCD_TRY(B.convert(it, it.p, it.ps, it.r64, PLQCD_F64));
+    }
     // tune the sloppy operator's launch configurations before any capture
     // (t, Ap and tmps are overwritten by the first iteration)
-    const plqcd_gauge *gs = in.g_sloppy ? in.g_sloppy : in.g64;
     PLQCD_TRY(B.mhat(it, gs, it.t, it.p, it.tmps, false));
     PLQCD_TRY(B.mhat(it, gs, it.Ap, it.t, it.tmps, true));
     return PLQCD_OK;
