@@ -293,6 +293,37 @@ int plqcd_gauge_update(const su3 *u);
  * host<->device byte counts. */
 int plqcd_dropin_last_stats(double *kernel_ms, double *h2d_bytes, double *d2h_bytes);
 
+/* ---- site-range vector operations (t-slab solver) ------------------------- */
+/* FP64 operations of the even/odd CG on the half-sites [h_begin, h_begin +
+ * h_count) of one-parity F64 fields (plqcd_b200/shard.py runs its slab CG on
+ * the slab interior with them; no reference counterpart, the reference has
+ * no solver: include/plqcd_global_params.h:197-201). Asynchronous on the
+ * lattice stream; reductions accumulate in FP64 in a fixed order and write
+ * one double to device memory; scalars are read from device memory, so no
+ * host round trip is needed. Reduction scratch comes from the lattice's
+ * device workspace.
+ *   sites_norm2:     *out_dev = sum |x|^2
+ *   sites_cg_update: alpha = coef_dev[0] / coef_dev[1] (rr / pAp);
+ *                    x += alpha p; r -= alpha Ap; *rr_dev = sum |r|^2
+ *   sites_xpay:      beta = coef_dev[0] / coef_dev[1]; p = r + beta p
+ *   sites_sub_norm2: z = x - y; *out_dev = sum |z|^2
+ * out_dev, rr_dev and coef_dev must be 8-byte aligned device pointers. */
+int plqcd_sites_norm2(plqcd_lattice *lat, const void *x, long h_begin, long h_count, double *out_dev);
+int plqcd_sites_cg_update(plqcd_lattice *lat, void *x, void *r, const void *p, const void *Ap, long h_begin,
+                          long h_count, const double *coef_dev, double *rr_dev);
+int plqcd_sites_xpay(plqcd_lattice *lat, void *p, const void *r, long h_begin, long h_count,
+                     const double *coef_dev);
+int plqcd_sites_sub_norm2(plqcd_lattice *lat, void *z, const void *x, const void *y, long h_begin, long h_count,
+                          double *out_dev);
+
+/* Copy n device segments (dst[k] <- src[k], bytes[k] bytes each) in one
+ * launch on the lattice stream: the ghost-slice exchange of a t-slab
+ * decomposition held on one device (one run per SoA plane, direction and
+ * slab). Every pointer and size must be a multiple of 16 bytes; segments
+ * must not overlap; n <= PLQCD_COPY_MAX_SEGMENTS. */
+#define PLQCD_COPY_MAX_SEGMENTS 128
+int plqcd_copy_segments(plqcd_lattice *lat, int n, void *const *dst, const void *const *src, const size_t *bytes);
+
 /* ---- failure detection ----------------------------------------------------- */
 /* Test hook of the bounded waits in the TMA-staged hopping kernels (no
  * reference counterpart: the reference calls exit(1) when a face exchange

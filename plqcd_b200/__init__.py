@@ -122,6 +122,11 @@ _SIGS = {
     "plqcd_selftest": (_i, [_i, _i]),
     "plqcd_gauge_update": (_i, [_vp]),
     "plqcd_tma_timeout_test": (_i, [_i, ctypes.c_ulonglong]),
+    "plqcd_sites_norm2": (_i, [_vp, _vp, ctypes.c_long, ctypes.c_long, _vp]),
+    "plqcd_sites_cg_update": (_i, [_vp, _vp, _vp, _vp, _vp, ctypes.c_long, ctypes.c_long, _vp, _vp]),
+    "plqcd_sites_xpay": (_i, [_vp, _vp, _vp, ctypes.c_long, ctypes.c_long, _vp]),
+    "plqcd_sites_sub_norm2": (_i, [_vp, _vp, _vp, _vp, ctypes.c_long, ctypes.c_long, _vp]),
+    "plqcd_copy_segments": (_i, [_vp, _i, _vp, _vp, _vp]),
     "plqcd_dropin_last_stats": (_i, [_dp, _dp, _dp]),
     "plqcd_aos_to_split": (_i, [_vp, _vp, _vp, ctypes.c_long]),
     **{f"plqcd_hopping_matrix_{w}_{v}": (ctypes.c_double, [_vp, _vp, _vp])
@@ -289,6 +294,11 @@ class Lattice:
         self.device = device
         self.Vh = int(lib().plqcd_lattice_half_volume(h))
         self.V = 2 * self.Vh
+
+    @property
+    def stream(self) -> int:
+        """The lattice's CUDA stream handle (0: the legacy default stream)."""
+        return int(lib().plqcd_lattice_stream(self.handle) or 0)
 
     def close(self):
         if self.handle:

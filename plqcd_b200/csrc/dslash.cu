@@ -520,8 +520,12 @@ static int tune_dslash(const Geom &g, cudaStream_t s, const DslashCall &c, const
                         (a.h_end - a.h_begin) % slab == 0 && getenv("PLQCD_NO_TMA") == nullptr;
     if (tma_ok)
         // (kinds 3 and 5, two own-line buffers, lost to 2 and 4 at every
-        // measured point and are not tried)
-        for (int kind : {1, 2, 4})
+        // measured point and are not tried). The own-line kernels (4, 2)
+        // come first, so they keep a near-tie: they stage fewer bytes per
+        // site and hold a higher rate once the power cap settles the clock
+        // (FP64 full lattice at 32^3x64, 4 s back to back: 4304 0.666 of
+        // HBM against 0.651 for 1204, at 1515 / 1470 MHz)
+        for (int kind : {4, 2, 1})
             for (int ny : {4, 8, 16, 2})
                 for (int ns : {1, 2, 3, 4, 6}) {
                     if (kind == 2 ? ns == 6 : ns == 1) continue;

@@ -156,16 +156,51 @@ def _view(field, geo: SlabGeometry, group):
     return field[off:off + n * geo.Vh * eb].view(n, geo.Vh * eb)
 
 
+def copy_segments(lat, segs):
+    """Device copies [(dst_ptr, src_ptr, nbytes), ...] on the lattice's
+    stream, PLQCD_COPY_MAX_SEGMENTS per launch (plqcd_copy_segments)."""
+    import ctypes
+
+    from . import check, lib
+    for k in range(0, len(segs), 128):
+        part = segs[k:k + 128]
+        n = len(part)
+        dst = (ctypes.c_void_p * n)(*[d for d, _, _ in part])
+        src = (ctypes.c_void_p * n)(*[s_ for _, s_, _ in part])
+        nb = (ctypes.c_size_t * n)(*[b for _, _, b in part])
+        check(lib().plqcd_copy_segments(lat.handle, n, dst, src, nb))
+
+
 class LocalTransport:
     """All slabs in one process (one device): ghost slices are copied."""
 
     def __init__(self, nranks: int):
         self.nranks = nranks
 
-    def exchange(self, geos, fields, groups, lower: bool = True, upper: bool = True):
+    def exchange(self, geos, fields, groups, lower: bool = True, upper: bool = True, lat=None):
         """fields[r]: torch uint8 tensor of rank r's field; groups: its plane
-        groups (SlabGeometry.spinor_groups / gauge_groups). One strided copy
-        per plane group and direction."""
+        groups (SlabGeometry.spinor_groups / gauge_groups). With `lat` (device
+        fields): every plane's slice of every slab and direction in one
+        plqcd_copy_segments launch on lat's stream; otherwise one strided
+        copy per plane group and direction."""
+        if lat is not None and fields and fields[0].is_cuda:
+            segs = []
+            for r, geo in enumerate(geos):
+                base = fields[r].data_ptr()
+                for off, n, eb in groups:
+                    nbytes = geo.S * eb
+                    for k in range(n):
+                        plane = off + k * geo.Vh * eb
+                        if lower:  # my last interior slice -> ghost 0 of the rank above
+                            up = geos[geo.above]
+                            segs.append((fields[geo.above].data_ptr() + plane + 0 * up.S * eb,
+                                         base + plane + geo.Lt * geo.S * eb, nbytes))
+                        if upper:  # my first interior slice -> ghost Lt+1 of the rank below
+                            dn = geos[geo.below]
+                            segs.append((fields[geo.below].data_ptr() + plane + (dn.Lt + 1) * dn.S * eb,
+                                         base + plane + 1 * geo.S * eb, nbytes))
+            copy_segments(lat, segs)
+            return
         for r, geo in enumerate(geos):
             for gr in groups:
                 src = _view(fields[r], geo, gr)
@@ -297,7 +332,7 @@ def exchange_gauge(shards, gauges, transport):
     views = [_wrap(g.data, g.lat.gauge_bytes(g.prec, g.recon), g.lat.device) for g in gauges]
     groups = shards[0].geo.gauge_groups(gauges[0].prec, gauges[0].recon)
     if isinstance(transport, LocalTransport):
-        transport.exchange([s.geo for s in shards], views, groups, lower=True, upper=False)
+        transport.exchange([s.geo for s in shards], views, groups, lower=True, upper=False, lat=shards[0].lat)
     else:
         transport.start(shards[0].geo, views[0], groups, lower=True, upper=False).wait()
 
@@ -311,7 +346,7 @@ def dslash(shards, gauges, outs, ins, out_parity: int, prec: int, transport, fla
     groups = shards[0].geo.spinor_groups(prec)
     xs = xs if xs is not None else [None] * len(shards)
     if isinstance(transport, LocalTransport):
-        transport.exchange([s.geo for s in shards], ins, groups)
+        transport.exchange([s.geo for s in shards], ins, groups, lat=shards[0].lat)
         for s, g, o, i, x in zip(shards, gauges, outs, ins, xs):
             h0, n = s.geo.interior()
             s.lat.dslash_sites(g, o, i, p, prec, h0, n, flags, a, x, b)
@@ -332,56 +367,80 @@ def dslash(shards, gauges, outs, ins, out_parity: int, prec: int, transport, fla
 # even/odd CG over the slabs (FP64)
 # ---------------------------------------------------------------------------
 
-def _f64(f):
-    """float64 view of a uint8 device field."""
-    import torch
-    return f.view(torch.float64)
-
-
-def _interior_f64(geo: SlabGeometry, f):
-    """float64 view of a field's interior sites: (12 planes, sites, re/im)."""
-    v = _f64(f).view(12, geo.Vh, 2)
-    h0, n = geo.interior()
-    return v[:, h0:h0 + n, :]
-
-
 class _Slabs:
-    """The fields of one logical spinor over the slabs this process holds,
-    with reductions summed over all slabs (all ranks)."""
+    """The fields of one logical spinor over the slabs this process holds.
+    Vector updates and interior dot products are the library's site-range
+    kernels (plqcd_sites_*) on each slab's interior; a dot product over all
+    slabs is the sum of the slabs' partial results, all-reduced over the
+    ranks on the device (one NCCL all-reduce of one double). The scalars of
+    the recursion live in a small device array `st`; the host reads one
+    value when it needs to steer."""
+
+    # slots of st: cg_update reads (st[RR], st[PAP]) as (rr, pAp); xpay
+    # reads (st[RRN], st[RR_COPY]) as (rr_new, rr)
+    RR, PAP, RRN, RR_COPY, AUX = 0, 1, 2, 3, 4
 
     def __init__(self, shards, transport):
+        import torch
         self.shards, self.transport = shards, transport
+        self.dev = f"cuda:{shards[0].lat.device}"
+        # torch work of the solver (partial sums, scalar copies, the
+        # all-reduce) runs on the slabs' stream, ordered with the kernels
+        self.stream = torch.cuda.ExternalStream(shards[0].lat.stream, device=self.dev)
+        with torch.cuda.stream(self.stream):
+            self.st = torch.zeros(8, dtype=torch.float64, device=self.dev)
+            self.part = torch.zeros((len(shards), 1), dtype=torch.float64, device=self.dev)
 
     def new(self):
         return [s.field(F64) for s in self.shards]
 
-    def norm2(self, fs) -> float:
-        return self.allsum(sum(float((_interior_f64(s.geo, f) ** 2).sum()) for s, f in zip(self.shards, fs)))
+    def _ptr(self, slot: int) -> int:
+        return self.st.data_ptr() + 8 * slot
 
-    def allsum(self, v: float) -> float:
-        if isinstance(self.transport, LocalTransport):
-            return v
+    def _finish(self, slot: int):
+        """st[slot] = the sum of the slabs' partials, over every rank."""
         import torch
-        dist = self.transport.dist
-        dev = f"cuda:{self.shards[0].lat.device}" if dist.get_backend(self.transport.group) == "nccl" else "cpu"
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, group=self.transport.group)
-        return float(t.item())
+        with torch.cuda.stream(self.stream):
+            torch.sum(self.part[:, 0], dim=0, keepdim=True, out=self.st[slot:slot + 1])
+            if not isinstance(self.transport, LocalTransport):
+                self.transport.dist.all_reduce(self.st[slot:slot + 1], group=self.transport.group)
 
-    @staticmethod
-    def axpy(a, xs, ys):          # y += a x
-        for x, y in zip(xs, ys):
-            _f64(y).add_(_f64(x), alpha=a)
+    def _each(self, fn, *fields):
+        from . import check, lib
+        for k, s in enumerate(self.shards):
+            h0, n = s.geo.interior()
+            check(fn(lib(), s.lat.handle, h0, n, k, *[f[k].data_ptr() for f in fields]))
 
-    @staticmethod
-    def xpay(xs, b, ys):          # y = x + b y
-        for x, y in zip(xs, ys):
-            _f64(y).mul_(b).add_(_f64(x))
+    def norm2(self, fs, slot: int):
+        self._each(lambda L, lat, h0, n, k, x: L.plqcd_sites_norm2(lat, x, h0, n, self.part[k].data_ptr()), fs)
+        self._finish(slot)
 
-    @staticmethod
-    def sub(xs, ys, zs):          # z = x - y
-        for x, y, z in zip(xs, ys, zs):
-            _f64(z).copy_(_f64(x)).sub_(_f64(y))
+    def cg_update(self, x, r, p, ap):
+        """alpha = st[RR] / st[PAP]; x += alpha p; r -= alpha Ap; st[RRN] = |r|^2"""
+        self._each(lambda L, lat, h0, n, k, xx, rr, pp, aa: L.plqcd_sites_cg_update(
+            lat, xx, rr, pp, aa, h0, n, self._ptr(self.RR), self.part[k].data_ptr()), x, r, p, ap)
+        self._finish(self.RRN)
+
+    def xpay(self, r, p):
+        """beta = st[RRN] / st[RR]; p = r + beta p; then st[RR] = st[RRN]"""
+        import torch
+        with torch.cuda.stream(self.stream):
+            self.st[self.RR_COPY] = self.st[self.RR]
+        self._each(lambda L, lat, h0, n, k, pp, rr: L.plqcd_sites_xpay(lat, pp, rr, h0, n, self._ptr(self.RRN)),
+                   p, r)
+        with torch.cuda.stream(self.stream):
+            self.st[self.RR] = self.st[self.RRN]
+
+    def sub_norm2(self, x, y, z, slot: int):
+        """z = x - y; st[slot] = |z|^2"""
+        self._each(lambda L, lat, h0, n, k, zz, xx, yy: L.plqcd_sites_sub_norm2(
+            lat, zz, xx, yy, h0, n, self.part[k].data_ptr()), z, x, y)
+        self._finish(slot)
+
+    def value(self, slot: int) -> float:
+        import torch
+        with torch.cuda.stream(self.stream):
+            return float(self.st[slot].item())
 
     @staticmethod
     def copy(src, dst):
@@ -398,8 +457,9 @@ def cg_solve(shards, g64s, b_even, b_odd, kappa: float, transport, tol: float = 
     FP64. b_even/b_odd: lists of per-slab fields of global parity 0 / 1.
     Returns (x_even, x_odd, iterations, schur_residual). The hops are the
     library's kernels with one ghost exchange each; the vector updates and
-    interior dot products run as torch operations, the dot products summed
-    over the ranks with one all-reduce each."""
+    interior dot products are the library's site-range kernels
+    (plqcd_sites_*), each dot product summed over the ranks with one
+    all-reduce on the device; the host reads one scalar per iteration."""
     from . import DSLASH_G5_IN, DSLASH_G5_OUT, EVEN, ODD
     S = _Slabs(shards, transport)
 
@@ -416,7 +476,8 @@ def cg_solve(shards, g64s, b_even, b_odd, kappa: float, transport, tol: float = 
 
     bprime, rhs = S.new(), S.new()
     hop(bprime, b_odd, EVEN, 0, kappa, b_even, 1.0)
-    bp2 = S.norm2(bprime)
+    S.norm2(bprime, S.AUX)
+    bp2 = S.value(S.AUX)
     x_e, x_o = S.new(), S.new()
     if not bp2 > 0:
         hop(x_o, x_e, ODD, 0, kappa, b_odd, 1.0)
@@ -425,30 +486,26 @@ def cg_solve(shards, g64s, b_even, b_odd, kappa: float, transport, tol: float = 
     r, p, t, Ap, r64 = S.new(), S.new(), S.new(), S.new(), S.new()
     S.copy(rhs, r)
     S.copy(rhs, p)
-    rr = S.norm2(r)
-    target = tol * tol * rr
+    S.norm2(r, S.RR)
+    target = tol * tol * S.value(S.RR)
     sr2 = bp2
     it = 0
     for it in range(1, max_iter + 1):
         mhat(t, p, False)
-        pap = S.norm2(t)
+        S.norm2(t, S.PAP)
         mhat(Ap, t, True)
-        alpha = rr / pap
-        S.axpy(alpha, p, x_e)
-        S.axpy(-alpha, Ap, r)
-        rr_new = S.norm2(r)
-        if rr_new <= target:
+        S.cg_update(x_e, r, p, Ap)          # alpha from the device, st[RRN] = |r|^2
+        if S.value(S.RRN) <= target:        # the one host read of an iteration
             # FP64 Schur residual decides convergence
             mhat(t, x_e, False)
-            S.sub(bprime, t, r64)
-            sr2 = S.norm2(r64)
+            S.sub_norm2(bprime, t, r64, S.AUX)
+            sr2 = S.value(S.AUX)
             if sr2 <= tol * tol * bp2:
                 break
             mhat(r, r64, True)
-            rr_new = S.norm2(r)
-            if rr_new <= target:
+            S.norm2(r, S.RRN)
+            if S.value(S.RRN) <= target:
                 target *= 0.25
-        S.xpay(r, rr_new / rr, p)
-        rr = rr_new
+        S.xpay(r, p)                        # beta = rr_new / rr from the device
     hop(x_o, x_e, ODD, 0, kappa, b_odd, 1.0)
     return x_e, x_o, it, (sr2 / bp2) ** 0.5

@@ -115,3 +115,74 @@ def test_sharded_cg_matches_single_device_cg(cuda, N):
     assert res <= tol
     assert abs(iters - info.iterations) <= 2, (iters, info.iterations)
     assert relmax(got, want) < 1e-8
+
+
+def test_site_range_vector_ops_match_torch(cuda):
+    """plqcd_sites_norm2 / cg_update / xpay / sub_norm2 on a site range of
+    F64 fields against the same operations written in torch FP64; sites
+    outside the range are untouched; scalars come from device memory."""
+    import torch
+    L = (8, 4, 6, 8)
+    lat = new_lattice(L)
+    lib = P.lib()
+    Vh = lat.Vh
+    bs = lat.spinor_bytes(P.F64)
+    fs = [dev_bytes(bs) for _ in range(5)]
+    for k, f in enumerate(fs):
+        lat.spinor_gaussian(f, P.F64, 0, 70 + k)
+    x, r, p, ap, z = fs
+    v = lambda f: f.view(torch.float64).view(12, Vh, 2)
+    h0, n = 37, Vh - 80
+    sl = slice(h0, h0 + n)
+    out = torch.zeros(4, dtype=torch.float64, device="cuda")
+    coef = torch.tensor([2.5, 1.25], dtype=torch.float64, device="cuda")
+    x0, r0, p0, ap0 = (v(f).clone() for f in (x, r, p, ap))
+    P.check(lib.plqcd_sites_norm2(lat.handle, p.data_ptr(), h0, n, out.data_ptr()))
+    P.check(lib.plqcd_sites_cg_update(lat.handle, x.data_ptr(), r.data_ptr(), p.data_ptr(), ap.data_ptr(), h0, n,
+                                      coef.data_ptr(), out[1:].data_ptr()))
+    lat.synchronize()
+    alpha = 2.0
+    want_x, want_r = x0.clone(), r0.clone()
+    want_x[:, sl] += alpha * p0[:, sl]
+    want_r[:, sl] -= alpha * ap0[:, sl]
+    assert torch.allclose(v(x), want_x, rtol=0, atol=1e-14) and torch.allclose(v(r), want_r, rtol=0, atol=1e-14)
+    assert abs(out[0].item() - (p0[:, sl] ** 2).sum().item()) <= 1e-12 * out[0].item()
+    assert abs(out[1].item() - (want_r[:, sl] ** 2).sum().item()) <= 1e-12 * out[1].item()
+    P.check(lib.plqcd_sites_xpay(lat.handle, p.data_ptr(), r.data_ptr(), h0, n, coef.data_ptr()))
+    P.check(lib.plqcd_sites_sub_norm2(lat.handle, z.data_ptr(), x.data_ptr(), r.data_ptr(), h0, n,
+                                      out[2:].data_ptr()))
+    lat.synchronize()
+    want_p = p0.clone()
+    want_p[:, sl] = v(r)[:, sl] + alpha * p0[:, sl]
+    assert torch.allclose(v(p), want_p, rtol=0, atol=1e-14)
+    d = v(x)[:, sl] - v(r)[:, sl]
+    assert torch.allclose(v(z)[:, sl], d, rtol=0, atol=1e-14)
+    assert abs(out[2].item() - (d ** 2).sum().item()) <= 1e-12 * out[2].item()
+    # twice in a row: the reduction scratch is left clean
+    P.check(lib.plqcd_sites_norm2(lat.handle, p.data_ptr(), h0, n, out[3:].data_ptr()))
+    P.check(lib.plqcd_sites_norm2(lat.handle, p.data_ptr(), h0, n, out[3:].data_ptr()))
+    lat.synchronize()
+    assert abs(out[3].item() - (want_p[:, sl] ** 2).sum().item()) <= 1e-12 * out[3].item()
+    assert lib.plqcd_sites_norm2(lat.handle, p.data_ptr(), Vh - 4, 8, out.data_ptr()) == P.ERR_ARG
+
+
+def test_copy_segments_one_launch(cuda):
+    """plqcd_copy_segments copies every segment of its table and refuses
+    segments that are not 16-byte aligned."""
+    import ctypes
+    import torch
+    lat = new_lattice((4, 4, 4, 4))
+    src = torch.arange(4096, dtype=torch.int32, device="cuda").view(torch.uint8)
+    dst = torch.zeros_like(src)
+    # destinations back to back (no overlap), sources overlapping
+    segs = [(dst.data_ptr() + 8 * k * (k + 1), src.data_ptr() + 16 * k * 5, 16 * (k + 1)) for k in range(20)]
+    SH.copy_segments(lat, segs)
+    lat.synchronize()
+    for d, s, b in segs:
+        o_d, o_s = d - dst.data_ptr(), s - src.data_ptr()
+        assert bool((dst[o_d:o_d + b] == src[o_s:o_s + b]).all())
+    n = 1
+    bad = (ctypes.c_void_p * n)(dst.data_ptr() + 8)
+    ok = (ctypes.c_void_p * n)(src.data_ptr())
+    nb = (ctypes.c_size_t * n)(16)
+    assert P.lib().plqcd_copy_segments(lat.handle, n, bad, ok, nb) == P.ERR_ARG
