@@ -32,7 +32,7 @@ extern "C" int plqcd_lattice_create(const int dims[4], int device, void *stream,
         return set_error(PLQCD_ERR_ARG, "plqcd_lattice_create: extents must be even and >= 2 (got %d %d %d %d)",
                          dims[0], dims[1], dims[2], dims[3]);
     long V = (long)dims[0] * dims[1] * dims[2] * dims[3];
-    if (V / 2 > (1L << 31)) return set_error(PLQCD_ERR_ARG, "plqcd_lattice_create: volume too large");
+    if (V / 2 >= (1L << 31)) return set_error(PLQCD_ERR_ARG, "plqcd_lattice_create: volume too large");
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
         cudaGetLastError();

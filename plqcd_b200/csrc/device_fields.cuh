@@ -519,16 +519,38 @@ struct Coords {
 };
 
 __device__ __forceinline__ Coords site_coords(long h, int par, int L0h, int L1, int L2) {
+    // 32-bit division (a 64-bit one is a long software sequence per site):
+    // plqcd_lattice_create keeps Vh < 2^31
     Coords c;
-    int xh = (int)(h % L0h);
-    c.row = h / L0h;
-    long r = c.row;
-    c.y = (int)(r % L1);
-    r /= L1;
-    c.z = (int)(r % L2);
-    c.t = (int)(r / L2);
+    const int hi = (int)h;
+    const int row = hi / L0h;
+    const int xh = hi - row * L0h;
+    const int zt = row / L1;
+    c.y = row - zt * L1;
+    c.t = zt / L2;
+    c.z = zt - c.t * L2;
+    c.row = row;
     c.x = 2 * xh + ((c.y + c.z + c.t + par) & 1);
     return c;
+}
+
+// even/odd indices of the eight neighbours of a site, in the order x+, y+,
+// z+, t+, x-, y-, z-, t- (d = 0..3 forward mu, 4..7 backward), periodic;
+// 32-bit like site_coords
+__device__ __forceinline__ void neighbour_sites(const Coords &c, int xh, int L0, int L0h, int L1, int L2, int L3,
+                                                int nb[8]) {
+    const int row = (int)c.row;
+    const int L012 = L1 * L2;
+    const int xp = (c.x + 1 == L0) ? 0 : c.x + 1;
+    const int xm = (c.x == 0) ? L0 - 1 : c.x - 1;
+    nb[0] = (xp >> 1) + L0h * row;
+    nb[1] = xh + L0h * (row + ((c.y + 1 == L1) ? -(L1 - 1) : 1));
+    nb[2] = xh + L0h * (row + ((c.z + 1 == L2) ? -(L2 - 1) * L1 : L1));
+    nb[3] = xh + L0h * (row + ((c.t + 1 == L3) ? -(L3 - 1) * L012 : L012));
+    nb[4] = (xm >> 1) + L0h * row;
+    nb[5] = xh + L0h * (row + ((c.y == 0) ? (L1 - 1) : -1));
+    nb[6] = xh + L0h * (row + ((c.z == 0) ? (L2 - 1) * L1 : -L1));
+    nb[7] = xh + L0h * (row + ((c.t == 0) ? (L3 - 1) * L012 : -L012));
 }
 
 }  // namespace dev

@@ -70,19 +70,12 @@ __global__ void __launch_bounds__(256) k_dslash(const DslashArgs a) {
     const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
     const Coords c = site_coords(h, par, L0h, L1, L2);
     const int xh = (int)(h - c.row * L0h);
-    const long L01 = L1, L012 = (long)L1 * L2;
 
     // neighbour half-site indices (periodic wrap on the device)
-    const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
-    const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
-    const long h_xp = (xp >> 1) + L0h * c.row;
-    const long h_xm = (xm >> 1) + L0h * c.row;
-    const long h_yp = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
-    const long h_ym = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
-    const long h_zp = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
-    const long h_zm = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
-    const long h_tp = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
-    const long h_tm = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
+    int nbs[8];
+    neighbour_sites(c, xh, a.L0, L0h, L1, L2, L3, nbs);
+    const int h_xp = nbs[0], h_yp = nbs[1], h_zp = nbs[2], h_tp = nbs[3];
+    const int h_xm = nbs[4], h_ym = nbs[5], h_zm = nbs[6], h_tm = nbs[7];
 
     const R sg = (R)a.g5_in;
     const int opp = par ^ 1;
@@ -152,18 +145,8 @@ __global__ void __launch_bounds__(256) k_dslash_pipe(const DslashArgs a) {
     const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
     const Coords c = site_coords(h, par, L0h, L1, L2);
     const int xh = (int)(h - c.row * L0h);
-    const long L01 = L1, L012 = (long)L1 * L2;
-    const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
-    const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
-    long nb[8];
-    nb[0] = (xp >> 1) + L0h * c.row;
-    nb[1] = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
-    nb[2] = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
-    nb[3] = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
-    nb[4] = (xm >> 1) + L0h * c.row;
-    nb[5] = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
-    nb[6] = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
-    nb[7] = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
+    int nb[8];
+    neighbour_sites(c, xh, a.L0, L0h, L1, L2, L3, nb);
     const int opp = par ^ 1;
     const int fpar = (COMPAT && par == 1) ? 0 : par;
 
@@ -253,8 +236,8 @@ __global__ void __launch_bounds__(256) k_dslash_spt2(const DslashArgs a) {
     void *out = static_cast<char *>(a.out[0]) + roff;
     const long Vh = a.Vh;
     const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
-    const long L01 = L1, L012 = (long)L1 * L2;
-    long hs[S], nb[S][8];
+    long hs[S];
+    int nb[S][8];
     bool ok[S];
 #pragma unroll
     for (int j = 0; j < S; j++) {
@@ -264,16 +247,7 @@ __global__ void __launch_bounds__(256) k_dslash_spt2(const DslashArgs a) {
         hs[j] = h;
         const Coords c = site_coords(h, par, L0h, L1, L2);
         const int xh = (int)(h - c.row * L0h);
-        const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
-        const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
-        nb[j][0] = (xp >> 1) + L0h * c.row;
-        nb[j][1] = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
-        nb[j][2] = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
-        nb[j][3] = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
-        nb[j][4] = (xm >> 1) + L0h * c.row;
-        nb[j][5] = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
-        nb[j][6] = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
-        nb[j][7] = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
+        neighbour_sites(c, xh, a.L0, L0h, L1, L2, L3, nb[j]);
     }
     if (!ok[0]) return;
     const R sg = (R)a.g5_in;

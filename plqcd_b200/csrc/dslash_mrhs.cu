@@ -50,18 +50,8 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs(const MrhsArgs a) {
     const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
     const Coords c = site_coords(h, par, L0h, L1, L2);
     const int xh = (int)(h - c.row * L0h);
-    const long L01 = L1, L012 = (long)L1 * L2;
-    const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
-    const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
-    long nb[8];
-    nb[0] = (xp >> 1) + L0h * c.row;
-    nb[1] = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
-    nb[2] = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
-    nb[3] = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
-    nb[4] = (xm >> 1) + L0h * c.row;
-    nb[5] = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
-    nb[6] = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
-    nb[7] = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
+    int nb[8];
+    neighbour_sites(c, xh, a.L0, L0h, L1, L2, L3, nb);
     const R sg = (R)a.g5_in;
 
     cx<R> acc[NR][12];
@@ -133,18 +123,8 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
     const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
     const Coords c = site_coords(h, par, L0h, L1, L2);
     const int xh = (int)(h - c.row * L0h);
-    const long L01 = L1, L012 = (long)L1 * L2;
-    const int xp = (c.x + 1 == a.L0) ? 0 : c.x + 1;
-    const int xm = (c.x == 0) ? a.L0 - 1 : c.x - 1;
-    long nb[8];
-    nb[0] = (xp >> 1) + L0h * c.row;
-    nb[1] = xh + L0h * (c.row + ((c.y + 1 == L1) ? -(long)(L1 - 1) : 1L));
-    nb[2] = xh + L0h * (c.row + ((c.z + 1 == L2) ? -(long)(L2 - 1) * L01 : L01));
-    nb[3] = xh + L0h * (c.row + ((c.t + 1 == L3) ? -(long)(L3 - 1) * L012 : L012));
-    nb[4] = (xm >> 1) + L0h * c.row;
-    nb[5] = xh + L0h * (c.row + ((c.y == 0) ? (long)(L1 - 1) : -1L));
-    nb[6] = xh + L0h * (c.row + ((c.z == 0) ? (long)(L2 - 1) * L01 : -L01));
-    nb[7] = xh + L0h * (c.row + ((c.t == 0) ? (long)(L3 - 1) * L012 : -L012));
+    int nb[8];
+    neighbour_sites(c, xh, a.L0, L0h, L1, L2, L3, nb);
     const R sg = (R)a.g5_in;
 
     const int stride = B * 16;

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -147,9 +148,16 @@ int tune_launch(const std::string &key, cudaStream_t s, const std::vector<TuneRe
         *ms /= reps;
         return true;
     };
-    double best = 1e30;
-    TuneResult bestc = cands[0];
-    for (const TuneResult &c : cands) {
+    // pass 1: every candidate alone (best of three batches)
+    struct Timed {
+        size_t idx;
+        int reps;
+        float t;
+        std::vector<float> rounds;
+    };
+    std::vector<Timed> timed;
+    for (size_t i = 0; i < cands.size(); i++) {
+        const TuneResult &c = cands[i];
         if (run(c, true) != PLQCD_OK) {  // infeasible candidate (e.g. shared memory)
             clear_error();
             cudaGetLastError();
@@ -165,13 +173,36 @@ int tune_launch(const std::string &key, cudaStream_t s, const std::vector<TuneRe
             ok = time_batch(c, reps, &ms);
             if (ok && ms < t) t = ms;
         }
-        if (!ok) continue;
+        if (ok) timed.push_back({i, reps, t, {}});
+    }
+    // pass 2: the fastest four again, round-robin, so that all of them see
+    // the same clock: a long tuning run drifts down to the power-capped
+    // clock, which would otherwise favour whatever was timed first. The
+    // score is the median of five rounds.
+    std::vector<Timed> fin = timed;
+    std::sort(fin.begin(), fin.end(), [](const Timed &a, const Timed &b) { return a.t < b.t; });
+    if (fin.size() > 4) fin.resize(4);
+    std::sort(fin.begin(), fin.end(), [](const Timed &a, const Timed &b) { return a.idx < b.idx; });
+    if (fin.size() > 1)
+        for (int round = 0; round < 5; round++)
+            for (Timed &f : fin) {
+                float ms = 0;
+                if (time_batch(cands[f.idx], 2 * f.reps, &ms)) f.rounds.push_back(ms);
+            }
+    double best = 1e30;
+    TuneResult bestc = cands[0];
+    for (Timed &f : fin) {
+        float score = f.t;
+        if (!f.rounds.empty()) {
+            std::sort(f.rounds.begin(), f.rounds.end());
+            score = f.rounds[f.rounds.size() / 2];
+        }
         // a later candidate must win by more than 1%: near-ties (timing
-        // noise) keep the earlier, simpler configuration on every GPU
-        if (t < best * 0.99) {
-            best = t;
-            bestc = c;
-            bestc.ms = t;
+        // noise) keep the earlier configuration on every GPU
+        if (score < best * 0.99) {
+            best = score;
+            bestc = cands[f.idx];
+            bestc.ms = score;
         }
     }
     cudaEventDestroy(e0);
