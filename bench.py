@@ -53,6 +53,7 @@ BYTES_HALF_12 = 52 + 8 * 24 + 52
 DRAM_BYTES_PER_SITE_F64_FULL = {
     2: 2127234136 / 2097152, 1204: 2191090112 / 2097152, 2204: 2253279192 / 2097152,
     4304: 2204120856 / 2097152, 1304: 2527646688 / 2097152, 1408: 2198568976 / 2097152,
+    2216: 2277960096 / 2097152,
 }
 
 
