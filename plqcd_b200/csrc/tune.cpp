@@ -148,14 +148,20 @@ int tune_launch(const std::string &key, cudaStream_t s, const std::vector<TuneRe
         *ms /= reps;
         return true;
     };
-    // pass 1: every candidate alone (best of three batches)
+    // pass 1: every candidate (best of three batches), scored against the
+    // first feasible candidate timed right before it, so that the clock
+    // drift of a long tuning run (the power cap settles in) does not favour
+    // the candidates timed first
     struct Timed {
         size_t idx;
         int reps;
-        float t;
+        float t;    // pass 1 score: time / reference time
+        float raw;  // pass 1 time (ms)
         std::vector<float> rounds;
     };
     std::vector<Timed> timed;
+    long ref = -1;
+    int ref_reps = 2;
     for (size_t i = 0; i < cands.size(); i++) {
         const TuneResult &c = cands[i];
         if (run(c, true) != PLQCD_OK) {  // infeasible candidate (e.g. shared memory)
@@ -167,32 +173,52 @@ int tune_launch(const std::string &key, cudaStream_t s, const std::vector<TuneRe
         if (!time_batch(c, 2, &probe)) continue;
         int reps = probe > 0 ? (int)(2.0f / probe) : 50;
         reps = reps < 2 ? 2 : (reps > 200 ? 200 : reps);
+        float tref = 1.f;
+        if (ref >= 0 && !time_batch(cands[ref], ref_reps, &tref)) continue;
         float t = 1e30f, ms = 0;
         bool ok = true;
         for (int k = 0; k < 3 && ok; k++) {
             ok = time_batch(c, reps, &ms);
             if (ok && ms < t) t = ms;
         }
-        if (ok) timed.push_back({i, reps, t, {}});
+        if (!ok) continue;
+        if (ref < 0) {
+            ref = (long)i;
+            ref_reps = reps;
+            tref = t;
+        }
+        timed.push_back({i, reps, t / (tref > 0 ? tref : 1.f), t, {}});
     }
-    // pass 2: the fastest four again, round-robin, so that all of them see
-    // the same clock: a long tuning run drifts down to the power-capped
-    // clock, which would otherwise favour whatever was timed first. The
-    // score is the median of five rounds.
+    // pass 2: the fastest four again. Short launches: round-robin, so that
+    // all of them see the same clock (median of five rounds). Launches of
+    // 100 us or more (large lattices, run back to back for long stretches):
+    // each finalist alone for ~0.2 s until the power cap has settled the
+    // clock at that kernel's own draw, then timed for ~0.1 s; a kernel that
+    // draws less power holds a higher clock there.
     std::vector<Timed> fin = timed;
     std::sort(fin.begin(), fin.end(), [](const Timed &a, const Timed &b) { return a.t < b.t; });
     if (fin.size() > 4) fin.resize(4);
     std::sort(fin.begin(), fin.end(), [](const Timed &a, const Timed &b) { return a.idx < b.idx; });
-    if (fin.size() > 1)
+    bool long_launch = false;
+    for (const Timed &f : fin) long_launch = long_launch || f.raw >= 0.1f;
+    if (fin.size() > 1 && long_launch) {
+        for (Timed &f : fin) {
+            const int settle = (int)(200.f / f.raw) + 1, timed_reps = (int)(100.f / f.raw) + 1;
+            float ms = 0;
+            if (time_batch(cands[f.idx], settle, &ms) && time_batch(cands[f.idx], timed_reps, &ms))
+                f.rounds.push_back(ms);
+        }
+    } else if (fin.size() > 1) {
         for (int round = 0; round < 5; round++)
             for (Timed &f : fin) {
                 float ms = 0;
                 if (time_batch(cands[f.idx], 2 * f.reps, &ms)) f.rounds.push_back(ms);
             }
+    }
     double best = 1e30;
     TuneResult bestc = cands[0];
     for (Timed &f : fin) {
-        float score = f.t;
+        float score = f.raw;
         if (!f.rounds.empty()) {
             std::sort(f.rounds.begin(), f.rounds.end());
             score = f.rounds[f.rounds.size() / 2];
