@@ -21,7 +21,11 @@ lattice is cut along t only, one slab per rank (one process per GPU):
   boundary slices; the kernels are the single-device ones, run on site ranges
   (plqcd_dslash_sites), with the periodic wrap never reached in t;
 * links: the backward t-link of slice t' = 1 sits in ghost slice 0, filled
-  once per gauge field from the rank below.
+  once per gauge field from the rank below;
+* streams: every slab's kernels and torch work run on its lattice's stream.
+  Slabs held by one process may each have their own stream: an exchange
+  then waits for all of them (on the first slab's stream) and they wait for
+  it, so the hops of the slabs run side by side on the device.
 
 Transports move the ghost slices: DistTransport (torch.distributed
 point-to-point, NCCL between GPUs, gloo on the host) and LocalTransport (all
@@ -156,18 +160,27 @@ def _view(field, geo: SlabGeometry, group):
     return field[off:off + n * geo.Vh * eb].view(n, geo.Vh * eb)
 
 
-def copy_segments(lat, segs):
-    """Device copies [(dst_ptr, src_ptr, nbytes), ...] on the lattice's
-    stream, PLQCD_COPY_MAX_SEGMENTS per launch (plqcd_copy_segments)."""
+def segment_tables(segs):
+    """[(dst_ptr, src_ptr, nbytes), ...] as the argument arrays of
+    plqcd_copy_segments, PLQCD_COPY_MAX_SEGMENTS segments per table."""
     import ctypes
-
-    from . import check, lib
+    tables = []
     for k in range(0, len(segs), 128):
         part = segs[k:k + 128]
         n = len(part)
-        dst = (ctypes.c_void_p * n)(*[d for d, _, _ in part])
-        src = (ctypes.c_void_p * n)(*[s_ for _, s_, _ in part])
-        nb = (ctypes.c_size_t * n)(*[b for _, _, b in part])
+        tables.append((n, (ctypes.c_void_p * n)(*[d for d, _, _ in part]),
+                       (ctypes.c_void_p * n)(*[s_ for _, s_, _ in part]),
+                       (ctypes.c_size_t * n)(*[b for _, _, b in part])))
+    return tables
+
+
+def copy_segments(lat, segs):
+    """Device copies [(dst_ptr, src_ptr, nbytes), ...] on the lattice's
+    stream, PLQCD_COPY_MAX_SEGMENTS per launch (plqcd_copy_segments).
+    `segs` may also be the result of segment_tables."""
+    from . import check, lib
+    tables = segs if segs and len(segs[0]) == 4 else segment_tables(segs)
+    for n, dst, src, nb in tables:
         check(lib().plqcd_copy_segments(lat.handle, n, dst, src, nb))
 
 
@@ -176,14 +189,22 @@ class LocalTransport:
 
     def __init__(self, nranks: int):
         self.nranks = nranks
+        self._tables = {}  # segment tables of the fields exchanged so far
 
     def exchange(self, geos, fields, groups, lower: bool = True, upper: bool = True, lat=None):
         """fields[r]: torch uint8 tensor of rank r's field; groups: its plane
         groups (SlabGeometry.spinor_groups / gauge_groups). With `lat` (device
         fields): every plane's slice of every slab and direction in one
-        plqcd_copy_segments launch on lat's stream; otherwise one strided
-        copy per plane group and direction."""
+        plqcd_copy_segments launch on lat's stream (the segment table of a set
+        of field addresses is built once); otherwise one strided copy per
+        plane group and direction."""
         if lat is not None and fields and fields[0].is_cuda:
+            key = (tuple(f.data_ptr() for f in fields), tuple(tuple(g) for g in groups), lower, upper,
+                   tuple((g.L, g.rank, g.nranks) for g in geos))
+            tables = self._tables.get(key)
+            if tables is not None:
+                copy_segments(lat, tables)
+                return
             segs = []
             for r, geo in enumerate(geos):
                 base = fields[r].data_ptr()
@@ -199,7 +220,11 @@ class LocalTransport:
                             dn = geos[geo.below]
                             segs.append((fields[geo.below].data_ptr() + plane + (dn.Lt + 1) * dn.S * eb,
                                          base + plane + 1 * geo.S * eb, nbytes))
-            copy_segments(lat, segs)
+            tables = segment_tables(segs)
+            if len(self._tables) >= 256:
+                self._tables.clear()
+            self._tables[key] = tables
+            copy_segments(lat, tables)
             return
         for r, geo in enumerate(geos):
             for gr in groups:
@@ -278,14 +303,17 @@ class ShardedLattice:
         self.lat = Lattice(self.geo.local_dims, device, stream)
 
     def field(self, prec: int):
+        """Zeroed field, allocated and cleared on the slab's stream."""
         import torch
-        return torch.zeros(self.lat.spinor_bytes(prec), dtype=torch.uint8, device=f"cuda:{self.lat.device}")
+        with torch.cuda.stream(_torch_stream(self.lat)):
+            return torch.zeros(self.lat.spinor_bytes(prec), dtype=torch.uint8, device=f"cuda:{self.lat.device}")
 
     def import_global(self, q_global: np.ndarray, global_parity: int, prec: int = F64, ghosts: bool = False):
         """Device field of one global parity from a global API-layout array."""
         import torch
         q = self.geo.local_spinor_from_global(q_global, ghosts)
-        aos = torch.from_numpy(q).to(f"cuda:{self.lat.device}")
+        with torch.cuda.stream(_torch_stream(self.lat)):
+            aos = torch.from_numpy(q).to(f"cuda:{self.lat.device}")
         f = self.field(prec)
         self.lat.spinor_import(aos, self.geo.local_parity(global_parity), f, prec)
         return f
@@ -294,7 +322,8 @@ class ShardedLattice:
         """(global even/odd indices, API-layout values) of the interior sites
         of a field of one global parity."""
         import torch
-        aos = torch.zeros((2 * self.geo.Vh, 12), dtype=torch.complex128, device=f"cuda:{self.lat.device}")
+        with torch.cuda.stream(_torch_stream(self.lat)):
+            aos = torch.zeros((2 * self.geo.Vh, 12), dtype=torch.complex128, device=f"cuda:{self.lat.device}")
         p = self.geo.local_parity(global_parity)
         self.lat.spinor_export(f, prec, p, aos)
         self.lat.synchronize()
@@ -326,13 +355,79 @@ def _wrap(ptr: int, nbytes: int, device: int):
     return torch.as_tensor(a, device=f"cuda:{device}")
 
 
+def _torch_stream(lat: Lattice):
+    """The lattice's CUDA stream as a torch stream (0: the default stream)."""
+    import torch
+    dev = f"cuda:{lat.device}"
+    if not lat.stream:
+        return torch.cuda.default_stream(dev)
+    return torch.cuda.ExternalStream(lat.stream, device=dev)
+
+
+class _StreamSet:
+    """The distinct streams of a list of slabs with one reusable event per
+    stream (a wait takes the event's state when it is issued, so an event
+    can be recorded again at once)."""
+
+    def __init__(self, lats):
+        import torch
+        self.streams = [_torch_stream(lat) for lat in lats]
+        self.events = [torch.cuda.Event() for _ in lats]
+
+    def join(self):
+        for st, ev in zip(self.streams[1:], self.events[1:]):
+            ev.record(st)
+            self.streams[0].wait_event(ev)
+
+    def fork(self):
+        ev = self.events[0]
+        ev.record(self.streams[0])
+        for st in self.streams[1:]:
+            st.wait_event(ev)
+
+
+_STREAM_SETS: dict = {}
+
+
+def _streams(shards):
+    """The _StreamSet of the slabs' distinct streams (first slab's first),
+    or None when they all share one stream."""
+    key = tuple(sh.lat.stream for sh in shards) + (shards[0].lat.device,)
+    ss = _STREAM_SETS.get(key, 0)
+    if ss == 0:
+        firsts = {}
+        for sh in shards:
+            firsts.setdefault(sh.lat.stream, sh.lat)
+        ss = _StreamSet(list(firsts.values())) if len(firsts) > 1 else None
+        _STREAM_SETS[key] = ss
+    return ss
+
+
+def join_streams(shards):
+    """The first slab's stream waits for the work queued on every other
+    slab's stream (no-op when all slabs share one stream)."""
+    ss = _streams(shards)
+    if ss is not None:
+        ss.join()
+
+
+def fork_streams(shards):
+    """Every slab's stream waits for the work queued on the first slab's
+    stream (no-op when all slabs share one stream)."""
+    ss = _streams(shards)
+    if ss is not None:
+        ss.fork()
+
+
 def exchange_gauge(shards, gauges, transport):
     """Fill ghost slice 0 of every shard's gauge field (the backward t-link
     of the first interior slice) from the rank below."""
     views = [_wrap(g.data, g.lat.gauge_bytes(g.prec, g.recon), g.lat.device) for g in gauges]
     groups = shards[0].geo.gauge_groups(gauges[0].prec, gauges[0].recon)
     if isinstance(transport, LocalTransport):
+        join_streams(shards)
         transport.exchange([s.geo for s in shards], views, groups, lower=True, upper=False, lat=shards[0].lat)
+        fork_streams(shards)
     else:
         transport.start(shards[0].geo, views[0], groups, lower=True, upper=False).wait()
 
@@ -341,12 +436,19 @@ def dslash(shards, gauges, outs, ins, out_parity: int, prec: int, transport, fla
            xs=None, b: float = 0.0):
     """out = a H in (+ b x) on every shard's interior, out_parity global.
     shards/gauges/outs/ins/xs: one entry per slab this process holds (all N
-    with LocalTransport, one with DistTransport)."""
+    with LocalTransport, one with DistTransport). Slab k's output is written
+    on slab k's stream; slabs of one process may share a stream or have one
+    each (their hops then overlap on the device)."""
     p = SlabGeometry.local_parity(out_parity)
     groups = shards[0].geo.spinor_groups(prec)
     xs = xs if xs is not None else [None] * len(shards)
     if isinstance(transport, LocalTransport):
+        # the exchange (on the first slab's stream) follows every slab's
+        # earlier work; each slab's hop then runs on its own stream, so the
+        # launches of slabs with separate streams overlap
+        join_streams(shards)
         transport.exchange([s.geo for s in shards], ins, groups, lat=shards[0].lat)
+        fork_streams(shards)
         for s, g, o, i, x in zip(shards, gauges, outs, ins, xs):
             h0, n = s.geo.interior()
             s.lat.dslash_sites(g, o, i, p, prec, h0, n, flags, a, x, b)
@@ -386,7 +488,7 @@ class _Slabs:
         self.dev = f"cuda:{shards[0].lat.device}"
         # torch work of the solver (partial sums, scalar copies, the
         # all-reduce) runs on the slabs' stream, ordered with the kernels
-        self.stream = torch.cuda.ExternalStream(shards[0].lat.stream, device=self.dev)
+        self.stream = _torch_stream(shards[0].lat)
         with torch.cuda.stream(self.stream):
             self.st = torch.zeros(8, dtype=torch.float64, device=self.dev)
             self.part = torch.zeros((len(shards), 1), dtype=torch.float64, device=self.dev)
@@ -400,6 +502,7 @@ class _Slabs:
     def _finish(self, slot: int):
         """st[slot] = the sum of the slabs' partials, over every rank."""
         import torch
+        join_streams(self.shards)
         with torch.cuda.stream(self.stream):
             torch.sum(self.part[:, 0], dim=0, keepdim=True, out=self.st[slot:slot + 1])
             if not isinstance(self.transport, LocalTransport):
@@ -407,6 +510,7 @@ class _Slabs:
 
     def _each(self, fn, *fields):
         from . import check, lib
+        fork_streams(self.shards)  # the scalars and fields the first stream produced
         for k, s in enumerate(self.shards):
             h0, n = s.geo.interior()
             check(fn(lib(), s.lat.handle, h0, n, k, *[f[k].data_ptr() for f in fields]))
@@ -442,10 +546,13 @@ class _Slabs:
         with torch.cuda.stream(self.stream):
             return float(self.st[slot].item())
 
-    @staticmethod
-    def copy(src, dst):
-        for s, d in zip(src, dst):
-            d.copy_(s)
+    def copy(self, src, dst):
+        import torch
+        join_streams(self.shards)
+        with torch.cuda.stream(self.stream):
+            for s_, d in zip(src, dst):
+                d.copy_(s_)
+        fork_streams(self.shards)
 
 
 def cg_solve(shards, g64s, b_even, b_odd, kappa: float, transport, tol: float = 1e-10, max_iter: int = 10000):
@@ -508,4 +615,5 @@ def cg_solve(shards, g64s, b_even, b_odd, kappa: float, transport, tol: float = 
                 target *= 0.25
         S.xpay(r, p)                        # beta = rr_new / rr from the device
     hop(x_o, x_e, ODD, 0, kappa, b_odd, 1.0)
+    join_streams(shards)  # the solution is complete on the first slab's stream
     return x_e, x_o, it, (sr2 / bp2) ** 0.5

@@ -15,6 +15,7 @@ from oracle import oracle as O
 from tests.gpu_util import dev_bytes, field_from_host, field_to_host, new_lattice, relmax
 
 pytestmark = pytest.mark.gpu
+_STREAMS = []  # side streams of the per-slab-stream tests (kept alive)
 
 
 def _global(L, seed):
@@ -26,10 +27,13 @@ def _global(L, seed):
     return lat, g64, u, q
 
 
-def _shards(L, N, u, prec, recon):
+def _shards(L, N, u, prec, recon, own_streams=False):
     import torch
     stream = torch.cuda.current_stream().cuda_stream
-    shards = [SH.ShardedLattice(L, r, N, 0, stream) for r in range(N)]
+    side = [torch.cuda.Stream() for _ in range(N - 1)] if own_streams else []
+    _STREAMS.extend(side)
+    shards = [SH.ShardedLattice(L, r, N, 0, stream if (r == 0 or not own_streams) else side[r - 1].cuda_stream)
+              for r in range(N)]
     gauges = [s.gauge_from_global(u, prec, recon) for s in shards]
     SH.exchange_gauge(shards, gauges, SH.LocalTransport(N))
     return shards, gauges
@@ -43,15 +47,15 @@ def _gather(shards, fields, parity, prec, V):
     return out
 
 
-@pytest.mark.parametrize("N", [1, 2, 4])
+@pytest.mark.parametrize("N,own_streams", [(1, False), (2, False), (4, False), (4, True)])
 @pytest.mark.parametrize("prec,recon", [(P.F64, 18), (P.F32, 12), (P.F16, 12)])
-def test_sharded_hop_is_bit_identical(cuda, N, prec, recon):
+def test_sharded_hop_is_bit_identical(cuda, N, own_streams, prec, recon):
     L = (8, 8, 4, 16)
     lat, g64, u, q = _global(L, 31)
     g = g64 if (prec, recon) == (P.F64, 18) else P.Gauge(lat, prec, recon)
     if g is not g64:
         g.copy_from(g64)
-    shards, gauges = _shards(L, N, u, prec, recon)
+    shards, gauges = _shards(L, N, u, prec, recon, own_streams)
     T = SH.LocalTransport(N)
     flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
     for p in (P.EVEN, P.ODD):
@@ -93,8 +97,8 @@ def test_sharded_hop_matches_oracle(cuda, restatement):
     assert relmax(got, want) < 1e-14
 
 
-@pytest.mark.parametrize("N", [2, 4])
-def test_sharded_cg_matches_single_device_cg(cuda, N):
+@pytest.mark.parametrize("N,own_streams", [(2, False), (4, False), (4, True)])
+def test_sharded_cg_matches_single_device_cg(cuda, N, own_streams):
     L = (8, 8, 4, 16)
     kappa, tol = 0.12, 1e-10
     lat, g64, u, q = _global(L, 33)
@@ -105,7 +109,7 @@ def test_sharded_cg_matches_single_device_cg(cuda, N):
     want = field_to_host(lat, xe, P.F64, 0)
     want[lat.Vh:] = field_to_host(lat, xo, P.F64, 1)[lat.Vh:]
 
-    shards, gauges = _shards(L, N, u, P.F64, 18)
+    shards, gauges = _shards(L, N, u, P.F64, 18, own_streams)
     T = SH.LocalTransport(N)
     b_e = [s.import_global(q, 0) for s in shards]
     b_o = [s.import_global(q, 1) for s in shards]
