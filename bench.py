@@ -705,9 +705,10 @@ def run_cg(torch, P, lat, g64, buf, args):
 
 def run_mrhs(torch, P, lat, g64, args, nrhs=8):
     """Multi-RHS hopping throughput at the benchmark lattice: bytes per site
-    and RHS = 2 * spinor + 8 * link / nrhs. For the 16-bit formats the
-    tensor-core kernel (variant 3001) and the scalar kernels are also timed
-    forced, beside the tuner's choice."""
+    and RHS = 2 * spinor + 8 * link / nrhs. For the FP32-computing formats
+    the RHS-pair kernel (variant 2002) and the scalar kernels, and for the
+    16-bit ones the tensor-core kernel (3001), are also timed forced (keys
+    variant/block), beside the tuner's choice."""
     res = {"nrhs": nrhs}
     for name, prec, recon, sb, lb in (("f64_18", P.F64, 18, 192, 144), ("f32_12", P.F32, 12, 96, 48),
                                       ("f16_12", P.F16, 12, 52, 24), ("bf16_12", P.BF16, 12, 52, 24)):
@@ -732,12 +733,16 @@ def run_mrhs(torch, P, lat, g64, args, nrhs=8):
         res[name] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)
         cfg = tuned_config(P, f"dslash_mrhs|p{prec}|r{recon}|plain|n{nrhs}|{lat.dims[0]}x")
         res[name]["tuned_variant"] = cfg[0] if cfg else None
-        if prec in (P.F16, P.BF16):
+        if prec != P.F64:
             forced = {}
-            for v, blk in ((3001, 128), (1042, 128), (1022, 64), (2, 128), (102, 128)):
+            cand = [(2002, 64), (2002, 128), (2022, 64), (2022, 128), (2032, 64), (2032, 128), (102, 128),
+                    (2, 128)]
+            if prec in (P.F16, P.BF16):
+                cand += [(3001, 128), (1042, 128), (1022, 64)]
+            for v, blk in cand:
                 os.environ["PLQCD_MRHS_VARIANT"], os.environ["PLQCD_MRHS_BLOCK"] = str(v), str(blk)
                 try:
-                    forced[str(v)] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)["us"]
+                    forced[f"{v}/{blk}"] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)["us"]
                 finally:
                     del os.environ["PLQCD_MRHS_VARIANT"], os.environ["PLQCD_MRHS_BLOCK"]
             res[name]["forced_us"] = forced

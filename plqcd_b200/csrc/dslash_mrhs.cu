@@ -15,6 +15,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <type_traits>
 #include <vector>
 
 #include "dslash_core.cuh"
@@ -197,6 +198,208 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
     }
 }
 
+// RHS-pair kernel: one thread, one output site, two right-hand sides on the
+// two lanes of Blackwell's packed FP32 instructions (FFMA2 / FMUL2 / FADD2):
+// lane 0 carries RHS r0, lane 1 RHS r0 + 1. The link is loaded, converted,
+// rebuilt and broadcast to both lanes once per pair, and every arithmetic
+// instruction serves both RHS. Each lane runs the scalar sequence of
+// compute_dir with the same rounding, so the results are the bits of the
+// other kernels. An odd last RHS runs in both lanes and is stored once.
+// (FP32-computing formats: F32, F16, BF16.)
+template <class SIO, class LIO, bool XPAY>
+__global__ void __launch_bounds__(256) k_dslash_mrhs_pair(const MrhsArgs a) {
+    static_assert(std::is_same<typename SIO::real, float>::value, "packed lanes hold FP32");
+    const int tile = blockIdx.x % a.ntiles;
+    const int h = (blockIdx.x / a.ntiles) * blockDim.x + threadIdx.x;
+    if (h >= a.Vh) return;
+    const int r0 = 2 * tile;
+    const bool two = r0 + 1 < a.nrhs;
+    const char *in0 = a.in + (size_t)r0 * a.fbytes;
+    const char *in1 = two ? in0 + a.fbytes : in0;
+    const int par = a.out_parity, opp = par ^ 1;
+    const long Vh = a.Vh;
+    const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
+    const Coords c = site_coords(h, par, L0h, L1, L2);
+    const int xh = h - c.row * L0h;
+    int nb[8];
+    neighbour_sites(c, xh, a.L0, L0h, L1, L2, L3, nb);
+    const f2 sg((float)a.g5_in);
+
+    cx<f2> acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = {f2(0.f), f2(0.f)};
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int d = dir_at(k);
+        cx<float> U[9];
+        if (d < 4)
+            LIO::load(a.gauge, Vh, par, d, h, U);
+        else
+            LIO::load(a.gauge, Vh, opp, d - 4, nb[d], U);
+        cx<f2> Ub[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++) Ub[e] = {f2(U[e].re), f2(U[e].im)};
+        cx<float> sa[12], sb[12];
+        float na, nbv;
+        SIO::load_raw(in0, Vh, nb[d], sa, na);
+        SIO::load_raw(in1, Vh, nb[d], sb, nbv);
+        cx<f2> s[12];
+#pragma unroll
+        for (int e = 0; e < 12; e++) s[e] = zip(sa[e], sb[e]);
+        compute_dir_n<false, SIO::kScaled, f2>(d, acc, s, Ub, sg, f2(na, nbv));
+    }
+
+    const float aup = (float)a.a_up, alow = (float)a.a_low, b = (float)a.b;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        if (j == 1 && !two) break;
+        cx<float> o[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) o[k] = lane(acc[k], j);
+        if (XPAY) {
+            cx<float> xv[12];
+            SIO::load(a.x + (size_t)(r0 + j) * a.fbytes, Vh, h, xv);
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const float ak = k < 6 ? aup : alow;
+                o[k] = {fmaf(ak, o[k].re, b * xv[k].re), fmaf(ak, o[k].im, b * xv[k].im)};
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const float ak = k < 6 ? aup : alow;
+                o[k] = {ak * o[k].re, ak * o[k].im};
+            }
+        }
+        SIO::store(a.out + (size_t)(r0 + j) * a.fbytes, Vh, h, o);
+    }
+}
+
+// Pipelined RHS-pair kernel: the link and the two neighbour spinors of a
+// direction are copied global->shared with cp.async into slots private to
+// the thread, ST directions ahead of the one being computed (as in
+// k_dslash_mrhs_pipe), so the loads stay in flight without holding the
+// registers the packed arithmetic needs.
+template <class SIO, class LIO, int ST, bool XPAY>
+__global__ void __launch_bounds__(256) k_dslash_mrhs_pair_pipe(const MrhsArgs a) {
+    static_assert(std::is_same<typename SIO::real, float>::value, "packed lanes hold FP32");
+    extern __shared__ uint4 smem[];
+    constexpr int NS = LIO::NSLOT + 2 * SIO::NSLOT;
+    const int B = blockDim.x;
+    const int tile = blockIdx.x % a.ntiles;
+    const int h = (blockIdx.x / a.ntiles) * B + threadIdx.x;
+    if (h >= a.Vh) return;  // no block-level barrier below
+    const int r0 = 2 * tile;
+    const bool two = r0 + 1 < a.nrhs;
+    const char *in0 = a.in + (size_t)r0 * a.fbytes;
+    const char *in1 = two ? in0 + a.fbytes : in0;
+    const int par = a.out_parity, opp = par ^ 1;
+    const long Vh = a.Vh;
+    const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
+    const Coords c = site_coords(h, par, L0h, L1, L2);
+    const int xh = h - c.row * L0h;
+    int nb[8];
+    neighbour_sites(c, xh, a.L0, L0h, L1, L2, L3, nb);
+    const f2 sg((float)a.g5_in);
+
+    const int stride = B * 16;
+    const uint32_t s_thread = smem_addr(smem) + threadIdx.x * 16;
+    // k-th direction of dir_at into slot k % ST: link, then RHS r0, r0 + 1
+    auto issue = [&](int k) {
+        const int d = dir_at(k);
+        const uint32_t s0 = s_thread + (uint32_t)((k % ST) * NS) * stride;
+        if (d < 4)
+            LIO::issue(a.gauge, Vh, par, d, h, s0, stride);
+        else
+            LIO::issue(a.gauge, Vh, opp, d - 4, nb[d], s0, stride);
+        SIO::issue(in0, Vh, nb[d], s0 + (uint32_t)LIO::NSLOT * stride, stride);
+        SIO::issue(in1, Vh, nb[d], s0 + (uint32_t)(LIO::NSLOT + SIO::NSLOT) * stride, stride);
+    };
+#pragma unroll
+    for (int k = 0; k < ST; k++) {
+        issue(k);
+        cp_async_commit();
+    }
+    cx<f2> acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = {f2(0.f), f2(0.f)};
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int d = dir_at(k);
+        cp_async_wait<ST - 1>();
+        const uint4 *s0 = smem + threadIdx.x + (k % ST) * NS * B;
+        cx<float> U[9];
+        LIO::load_staged(s0, B, U);
+        cx<f2> Ub[9];
+#pragma unroll
+        for (int e = 0; e < 9; e++) Ub[e] = {f2(U[e].re), f2(U[e].im)};
+        cx<float> sa[12], sb[12];
+        float na, nbv;
+        SIO::load_staged_raw(s0 + LIO::NSLOT * B, B, sa, na);
+        SIO::load_staged_raw(s0 + (LIO::NSLOT + SIO::NSLOT) * B, B, sb, nbv);
+        cx<f2> s[12];
+#pragma unroll
+        for (int e = 0; e < 12; e++) s[e] = zip(sa[e], sb[e]);
+        compute_dir_n<false, SIO::kScaled, f2>(d, acc, s, Ub, sg, f2(na, nbv));
+        // the slot just consumed is refilled only after its values were used
+        if (k + ST < 8) issue(k + ST);
+        cp_async_commit();
+    }
+
+    const float aup = (float)a.a_up, alow = (float)a.a_low, b = (float)a.b;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        if (j == 1 && !two) break;
+        cx<float> o[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) o[k] = lane(acc[k], j);
+        if (XPAY) {
+            cx<float> xv[12];
+            SIO::load(a.x + (size_t)(r0 + j) * a.fbytes, Vh, h, xv);
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const float ak = k < 6 ? aup : alow;
+                o[k] = {fmaf(ak, o[k].re, b * xv[k].re), fmaf(ak, o[k].im, b * xv[k].im)};
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const float ak = k < 6 ? aup : alow;
+                o[k] = {ak * o[k].re, ak * o[k].im};
+            }
+        }
+        SIO::store(a.out + (size_t)(r0 + j) * a.fbytes, Vh, h, o);
+    }
+}
+
+// ST = 0: direct loads (k_dslash_mrhs_pair), else the cp.async pipeline of depth ST
+template <class SIO, class LIO, int ST>
+static int launch_pair(const Geom &g, cudaStream_t s, MrhsArgs a, int block, bool xpay) {
+    if constexpr (!std::is_same<typename SIO::real, float>::value) {
+        return set_error(PLQCD_ERR_ARG, "dslash_mrhs: the RHS-pair kernel computes in FP32 only");
+    } else {
+        if (g.Vh >= (1L << 31)) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: lattice too large for 32-bit sites");
+        a.ntiles = (a.nrhs + 1) / 2;
+        const long nblk = (g.Vh + block - 1) / block * a.ntiles;
+        if (nblk > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: grid too large");
+        if constexpr (ST == 0) {
+            if (xpay)
+                k_dslash_mrhs_pair<SIO, LIO, true><<<(unsigned)nblk, block, 0, s>>>(a);
+            else
+                k_dslash_mrhs_pair<SIO, LIO, false><<<(unsigned)nblk, block, 0, s>>>(a);
+        } else {
+            constexpr int NS = LIO::NSLOT + 2 * SIO::NSLOT;
+            const size_t smem = (size_t)ST * NS * 16 * block;
+            if (smem > 227 * 1024) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: %zu bytes of shared memory", smem);
+            auto k = xpay ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true> : k_dslash_mrhs_pair_pipe<SIO, LIO, ST, false>;
+            PLQCD_TRY(smem_optin((const void *)k, 227 * 1024));
+            k<<<(unsigned)nblk, block, smem, s>>>(a);
+        }
+        PLQCD_CUDA_TRY(cudaGetLastError());
+        return PLQCD_OK;
+    }
+}
+
 template <class SIO, class LIO, int NR, int ST>
 static int launch_nr_pipe(const Geom &g, cudaStream_t s, MrhsArgs a, int block, bool xpay) {
     a.ntiles = (a.nrhs + NR - 1) / NR;
@@ -236,6 +439,11 @@ static int launch_pr(const Geom &g, cudaStream_t s, const MrhsArgs &a, int nr, i
         case 1042:
             if constexpr (P != PLQCD_F64) return launch_nr_pipe<S, L, 4, 2>(g, s, a, block, xpay);
             break;
+        // 2002: RHS-pair kernel on packed FP32 lanes; 2022 / 2032: its
+        // cp.async pipeline of depth 2 / 3
+        case 2002: return launch_pair<S, L, 0>(g, s, a, block, xpay);
+        case 2022: return launch_pair<S, L, 2>(g, s, a, block, xpay);
+        case 2032: return launch_pair<S, L, 3>(g, s, a, block, xpay);
         case 1: return launch_nr<S, L, 1>(g, s, a, block, xpay);
         case 2: return launch_nr<S, L, 2>(g, s, a, block, xpay);
         case 4:
@@ -267,6 +475,22 @@ int launch_dslash_mrhs_tc(const Geom &g, cudaStream_t s, const void *gauge, int 
                           const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b,
                           int tiles);
 
+// tuner key of a multi-RHS hop
+static void mrhs_key(char *key, size_t n, const Geom &g, int prec, int recon, int nrhs, bool xpay) {
+    snprintf(key, n, "%sdslash_mrhs|p%d|r%d|%s|n%d|%dx%dx%dx%d", device_tag().c_str(), prec, recon,
+             xpay ? "xpay" : "plain", nrhs, g.L[0], g.L[1], g.L[2], g.L[3]);
+}
+
+// true when a launch of this multi-RHS hop would not tune (a tuned entry
+// exists, tuning is off, or the environment fixes the configuration)
+bool dslash_mrhs_tuned(const Geom &g, int prec, int recon, int nrhs, bool xpay) {
+    const char *ev = getenv("PLQCD_MRHS_VARIANT");
+    if ((ev && *ev) || !tune_enabled()) return true;
+    char key[256];
+    mrhs_key(key, sizeof key, g, prec, recon, nrhs, xpay);
+    return tune_lookup(key, nullptr);
+}
+
 // out (nrhs fields) = a_up/a_low * H in + b * x; tuned over RHS tile and block
 int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
                        const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b) {
@@ -294,8 +518,7 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
     m.g5_in = (flags & PLQCD_DSLASH_G5_IN) ? -1.0 : 1.0;
     const bool xpay = x != nullptr;
     char key[256];
-    snprintf(key, sizeof key, "%sdslash_mrhs|p%d|r%d|%s|n%d|%dx%dx%dx%d", device_tag().c_str(), prec, recon,
-             xpay ? "xpay" : "plain", nrhs, g.L[0], g.L[1], g.L[2], g.L[3]);
+    mrhs_key(key, sizeof key, g, prec, recon, nrhs, xpay);
     // two families of candidates: the RHS-tile kernel above (variant = tile
     // size 1, 2, 4), and the single-RHS kernels with the RHS index folded
     // into the grid, RHS fastest, so the blocks of one site range run
@@ -309,8 +532,10 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
             t.block = blk;
             cands.push_back(t);
         }
-    for (int nr : {1022, 1042, 2, 1, 4}) {
-        const int tile = nr >= 1000 ? (nr / 10) % 10 : nr;
+    for (int nr : {2022, 2032, 2002, 1022, 1042, 2, 1, 4}) {
+        const bool pair = nr >= 2000;
+        if (pair && (prec == PLQCD_F64 || nrhs < 2)) continue;
+        const int tile = pair ? 2 : nr >= 1000 ? (nr / 10) % 10 : nr;
         if (tile == 4 && prec == PLQCD_F64) continue;
         if (tile > nrhs && tile != 1) continue;
         for (int blk : {64, 128, 256}) {

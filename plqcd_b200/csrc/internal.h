@@ -143,6 +143,8 @@ int launch_dslash_config(const Geom &g, cudaStream_t s, const DslashCall &c, int
 // nrhs one-parity fields back to back: out = a * H in (+ b * x if x != null)
 int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
                        const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b);
+// true when launch_dslash_mrhs of this configuration would not tune
+bool dslash_mrhs_tuned(const Geom &g, int prec, int recon, int nrhs, bool xpay);
 
 // dynamic shared-memory opt-in of kernel `func` on the current device, set
 // once per (kernel, device) to at least `bytes` (utils.cpp)

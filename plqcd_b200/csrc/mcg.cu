@@ -475,7 +475,11 @@ struct Batch {
     }
 };
 
-int setup_item(Batch &B, Item &it) {
+// workspace and state arrays of one item (outside the timed solve). The
+// item takes its lattice's solver workspace, kept across solves as
+// plqcd_invert_cg keeps it, unless an earlier item of the batch holds it:
+// then it allocates its own (`it.mem`, freed after the solve).
+int alloc_item(Batch &B, Item &it, bool own_ws) {
     const plqcd_solve_item &in = it.in;
     it.g = &in.lat->geom;
     const long Vh = it.g->Vh;
@@ -488,11 +492,17 @@ int setup_item(Batch &B, Item &it) {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t need = 4 * al(it.fb64 * n) + 5 * al(it.fbs * n) + al(it.fbx * n) + 10 * al(sizeof(double) * n) +
                         2 * al(sizeof(int) * n) + al(sizeof(double) * n * it.st.nb) + al(sizeof(unsigned) * n);
-    if (cudaMalloc(&it.mem, need) != cudaSuccess) {
-        cudaGetLastError();
-        return set_error(PLQCD_ERR_NOMEM, "batch cg: workspace of %zu bytes", need);
+    void *ws = nullptr;
+    if (own_ws) {
+        if (cudaMalloc(&it.mem, need) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(PLQCD_ERR_NOMEM, "batch cg: workspace of %zu bytes", need);
+        }
+        ws = it.mem;
+    } else {
+        PLQCD_TRY(lattice_workspace(in.lat, need, &ws));
     }
-    char *w = static_cast<char *>(it.mem);
+    char *w = static_cast<char *>(ws);
     auto take = [&](size_t x) {
         char *p = w;
         w += al(x);
@@ -519,7 +529,35 @@ int setup_item(Batch &B, Item &it) {
     PLQCD_CUDA_TRY(cudaMemsetAsync(it.st.counters, 0, sizeof(unsigned) * n, s));
     PLQCD_CUDA_TRY(cudaMemsetAsync(it.st.conv_iter, 0xff, sizeof(int) * n, s));
     dev::k_mfill_int<<<1, 256, 0, s>>>(it.st.active, n, 1);
-    // b' = b_e + kappa H_eo b_o ; |b'|^2 ; r = Mhat^dag b' (x = 0) ; |r|^2
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+// tune the plain and xpay hops of the sloppy and the FP64 operator on this
+// item's block (zeroed fields) when the tuner has no entry for them yet: a
+// captured launch cannot tune and would take the first candidate
+int tune_item(Batch &B, Item &it) {
+    const plqcd_solve_item &in = it.in;
+    const plqcd_gauge *gs = in.g_sloppy ? in.g_sloppy : in.g64;
+    const int n = in.nrhs;
+    const bool done = dslash_mrhs_tuned(*it.g, gs->prec, gs->recon, n, false) &&
+                      dslash_mrhs_tuned(*it.g, gs->prec, gs->recon, n, true) &&
+                      dslash_mrhs_tuned(*it.g, PLQCD_F64, in.g64->recon, n, false) &&
+                      dslash_mrhs_tuned(*it.g, PLQCD_F64, in.g64->recon, n, true);
+    if (done) return PLQCD_OK;
+    cudaStream_t s = B.s;
+    PLQCD_CUDA_TRY(cudaMemsetAsync(it.p, 0, it.fbs * n, s));
+    PLQCD_CUDA_TRY(cudaMemsetAsync(it.r64, 0, it.fb64 * n, s));
+    PLQCD_TRY(B.mhat(it, gs, it.t, it.p, it.tmps, false));
+    return B.mhat(it, in.g64, it.t64, it.r64, it.tmp64, false);
+}
+
+// start of the solve: b' = b_e + kappa H_eo b_o, |b'|^2, x = 0, the start
+// residual r = Mhat^dag b' and |r|^2, p = r
+int start_item(Batch &B, Item &it) {
+    const plqcd_solve_item &in = it.in;
+    const int n = in.nrhs;
+    cudaStream_t s = B.s;
     PLQCD_TRY(B.hop(it, in.g64, it.bprime, in.b_odd, PLQCD_EVEN, 0, in.b_even, B.kappa, 1.0));
     PLQCD_TRY(B.norm2(it, it.bprime, PLQCD_F64, M_BP2, false));
     PLQCD_CUDA_TRY(cudaMemsetAsync(in.x_even, 0, it.fb64 * n, s));
@@ -539,14 +577,12 @@ int setup_item(Batch &B, Item &it) {
         PLQCD_TRY(B.convert(it, it.rs, it.ps, it.r64, PLQCD_F64));
         PLQCD_TRY(B.convert(it, it.p, it.ps, it.r64, PLQCD_F64));
     }
-    // tune the sloppy operator's launch configurations before any capture
-    // (t, Ap and tmps are overwritten by the first iteration)
-    PLQCD_TRY(B.mhat(it, gs, it.t, it.p, it.tmps, false));
-    PLQCD_TRY(B.mhat(it, gs, it.Ap, it.t, it.tmps, true));
     return PLQCD_OK;
 }
 
-int run_graph(Batch &B, int *graph_launches) {
+// capture the iteration loop (WHILE node: sloppy part, IF node with the
+// reliable update, direction part) and instantiate it; nothing runs
+int build_graph(Batch &B, cudaGraph_t *gout, cudaGraphExec_t *geout) {
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;
     int rc = PLQCD_OK;
@@ -621,12 +657,15 @@ int run_graph(Batch &B, int *graph_launches) {
         }
         if (rc) break;
         if (!cuda(cudaGraphInstantiate(&ge, g, 0), "instantiate")) break;
-        if (!cuda(cudaGraphLaunch(ge, s), "launch")) break;
-        *graph_launches = 1;
-        cuda(cudaStreamSynchronize(s), "sync");
     } while (0);
-    if (ge) cudaGraphExecDestroy(ge);
-    if (g) cudaGraphDestroy(g);
+    if (rc) {
+        if (ge) cudaGraphExecDestroy(ge);
+        if (g) cudaGraphDestroy(g);
+        ge = nullptr;
+        g = nullptr;
+    }
+    *gout = g;
+    *geout = ge;
     return rc;
 }
 
@@ -694,6 +733,8 @@ extern "C" int plqcd_invert_cg_batch(plqcd_solve_item *items, int nitems, const 
 
     int rc = PLQCD_OK;
     McgControl *hctl = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
     plqcd_batch_info inf;
     memset(&inf, 0, sizeof inf);
     do {
@@ -712,15 +753,19 @@ extern "C" int plqcd_invert_cg_batch(plqcd_solve_item *items, int nitems, const 
                       ? PLQCD_OK
                       : set_error(PLQCD_ERR_CUDA, "plqcd_invert_cg_batch: control upload")))
             break;
-        cudaEventRecord(ev0, B.s);
+        // outside the timed solve: workspaces, tuning of every hop the loop
+        // launches, and the graph (capture and instantiation run nothing)
         B.items.resize(nitems);
         for (int k = 0; k < nitems && rc == PLQCD_OK; k++) {
             Item &it = B.items[k];
             it.in = items[k];
             it.ps = prm->sloppy_prec;
             it.xprec = (it.ps == PLQCD_F64) ? PLQCD_F64 : PLQCD_F32;
-            rc = setup_item(B, it);
+            bool shared = false;
+            for (int j = 0; j < k; j++) shared = shared || items[j].lat == items[k].lat;
+            rc = alloc_item(B, it, shared);
         }
+        for (int k = 0; k < nitems && rc == PLQCD_OK; k++) rc = tune_item(B, B.items[k]);
         if (rc) break;
         std::vector<McgState> hst(nitems);
         for (int k = 0; k < nitems; k++) hst[k] = B.items[k].st;
@@ -730,8 +775,20 @@ extern "C" int plqcd_invert_cg_batch(plqcd_solve_item *items, int nitems, const 
             break;
         }
         cudaStreamSynchronize(B.s);  // hst is a host temporary
-        rc = use_graph ? run_graph(B, &inf.graph_launches) : run_eager(B, hctl);
+        if (use_graph && (rc = build_graph(B, &graph, &gexec))) break;
+        // the solve: start residuals, the loop, x_o
+        cudaEventRecord(ev0, B.s);
+        for (int k = 0; k < nitems && rc == PLQCD_OK; k++) rc = start_item(B, B.items[k]);
         if (rc) break;
+        if (use_graph) {
+            if (cudaGraphLaunch(gexec, B.s) != cudaSuccess) {
+                rc = set_error(PLQCD_ERR_CUDA, "batch cg graph: launch: %s", cudaGetErrorString(cudaGetLastError()));
+                break;
+            }
+            inf.graph_launches = 1;
+        } else if ((rc = run_eager(B, hctl))) {
+            break;
+        }
         // fold in unconverged sloppy solutions, rebuild x_o, full-lattice residuals
         for (Item &it : B.items) {
             dim3 grid(it.st.nb, it.in.nrhs);
@@ -790,6 +847,8 @@ extern "C" int plqcd_invert_cg_batch(plqcd_solve_item *items, int nitems, const 
     } while (0);
 
     cudaStreamSynchronize(B.s);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
     for (Item &it : B.items)
         if (it.mem) cudaFree(it.mem);
     if (B.ctl) cudaFree(B.ctl);

@@ -485,6 +485,43 @@ def test_multi_rhs_every_variant(cuda, monkeypatch, variant, block, prec, recon,
         assert relmax(a, b) <= tol, (variant, r, relmax(a, b))
 
 
+@pytest.mark.parametrize("variant", [2002, 2022, 2032])
+@pytest.mark.parametrize("nrhs", [1, 2, 5, 8])
+@pytest.mark.parametrize("prec,recon", [(P.F32, 18), (P.F32, 12), (P.F16, 12), (P.BF16, 12)])
+@pytest.mark.parametrize("xpay", [False, True])
+def test_multi_rhs_pair_kernel_is_bit_identical(cuda, monkeypatch, variant, nrhs, prec, recon, xpay):
+    """The RHS-pair kernels (two RHS on the lanes of packed FP32
+    instructions: 2002 direct loads, 2022 / 2032 cp.async pipeline of depth
+    2 / 3), forced past the tuner, store the same bytes as the single-RHS
+    kernel for every field of the block, an odd last RHS included."""
+    L = (8, 4, 6, 8)
+    lat, g64, u = _device_setup(L, 23)
+    g = P.Gauge(lat, prec, recon)
+    g.copy_from(g64)
+    bs = lat.spinor_bytes(prec)
+    blk_in, blk_out, blk_x = dev_bytes(nrhs * bs), dev_bytes(nrhs * bs), dev_bytes(nrhs * bs)
+    for r in range(nrhs):
+        lat.spinor_gaussian(blk_in[r * bs:(r + 1) * bs], prec, 1, 500 + r)
+        lat.spinor_gaussian(blk_x[r * bs:(r + 1) * bs], prec, 0, 600 + r)
+    monkeypatch.setenv("PLQCD_MRHS_VARIANT", str(variant))
+    monkeypatch.setenv("PLQCD_MRHS_BLOCK", "64")
+    flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
+    if xpay:
+        lat.dslash_mrhs_xpay(g, blk_out, blk_in, nrhs, 0, prec, -0.29, blk_x, 1.25, flags)
+    else:
+        lat.dslash_mrhs(g, blk_out, blk_in, nrhs, 0, prec)
+    monkeypatch.delenv("PLQCD_MRHS_VARIANT")
+    for r in range(nrhs):
+        sl = slice(r * bs, (r + 1) * bs)
+        one = dev_bytes(bs)
+        if xpay:
+            lat.dslash_xpay(g, one, blk_in[sl], 0, prec, -0.29, blk_x[sl], 1.25, flags)
+        else:
+            lat.dslash(g, one, blk_in[sl], 0, prec)
+        lat.synchronize()
+        assert bool((blk_out[sl] == one).all()), (r, prec, recon, xpay)
+
+
 @pytest.mark.parametrize("tiles,nrhs", [(1, 8), (1, 12), (2, 16), (2, 20), (4, 32), (1, 3)])
 @pytest.mark.parametrize("prec,tol", [(P.F16, 2e-3), (P.BF16, 1.6e-2)])
 @pytest.mark.parametrize("xpay", [False, True])
