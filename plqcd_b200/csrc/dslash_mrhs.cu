@@ -206,8 +206,8 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
 // compute_dir with the same rounding, so the results are the bits of the
 // other kernels. An odd last RHS runs in both lanes and is stored once.
 // (FP32-computing formats: F32, F16, BF16.)
-template <class SIO, class LIO, bool XPAY>
-__global__ void __launch_bounds__(256) k_dslash_mrhs_pair(const MrhsArgs a) {
+template <class SIO, class LIO, bool XPAY, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_dslash_mrhs_pair(const MrhsArgs a) {
     static_assert(std::is_same<typename SIO::real, float>::value, "packed lanes hold FP32");
     const int tile = blockIdx.x % a.ntiles;
     const int h = (blockIdx.x / a.ntiles) * blockDim.x + threadIdx.x;
@@ -280,8 +280,8 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pair(const MrhsArgs a) {
 // the thread, ST directions ahead of the one being computed (as in
 // k_dslash_mrhs_pipe), so the loads stay in flight without holding the
 // registers the packed arithmetic needs.
-template <class SIO, class LIO, int ST, bool XPAY>
-__global__ void __launch_bounds__(256) k_dslash_mrhs_pair_pipe(const MrhsArgs a) {
+template <class SIO, class LIO, int ST, bool XPAY, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_dslash_mrhs_pair_pipe(const MrhsArgs a) {
     static_assert(std::is_same<typename SIO::real, float>::value, "packed lanes hold FP32");
     extern __shared__ uint4 smem[];
     constexpr int NS = LIO::NSLOT + 2 * SIO::NSLOT;
@@ -315,9 +315,16 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pair_pipe(const MrhsArgs a)
         SIO::issue(in0, Vh, nb[d], s0 + (uint32_t)LIO::NSLOT * stride, stride);
         SIO::issue(in1, Vh, nb[d], s0 + (uint32_t)(LIO::NSLOT + SIO::NSLOT) * stride, stride);
     };
+    // xpay: the two x spinors of the output site go in with the first
+    // direction, into slots after the ring, so the epilogue does not wait
+    const uint32_t s_x = s_thread + (uint32_t)(ST * NS) * stride;
 #pragma unroll
     for (int k = 0; k < ST; k++) {
         issue(k);
+        if (XPAY && k == 0) {
+            SIO::issue(a.x + (size_t)r0 * a.fbytes, Vh, h, s_x, stride);
+            SIO::issue(a.x + (size_t)(two ? r0 + 1 : r0) * a.fbytes, Vh, h, s_x + SIO::NSLOT * stride, stride);
+        }
         cp_async_commit();
     }
     cx<f2> acc[12];
@@ -355,7 +362,7 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pair_pipe(const MrhsArgs a)
         for (int k = 0; k < 12; k++) o[k] = lane(acc[k], j);
         if (XPAY) {
             cx<float> xv[12];
-            SIO::load(a.x + (size_t)(r0 + j) * a.fbytes, Vh, h, xv);
+            SIO::load_staged(smem + threadIdx.x + (ST * NS + j * SIO::NSLOT) * B, B, xv);
 #pragma unroll
             for (int k = 0; k < 12; k++) {
                 const float ak = k < 6 ? aup : alow;
@@ -372,8 +379,9 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pair_pipe(const MrhsArgs a)
     }
 }
 
-// ST = 0: direct loads (k_dslash_mrhs_pair), else the cp.async pipeline of depth ST
-template <class SIO, class LIO, int ST>
+// ST = 0: direct loads (k_dslash_mrhs_pair), else the cp.async pipeline of
+// depth ST; MINB = 2 caps the registers at 128 a thread (more warps per SM)
+template <class SIO, class LIO, int ST, int MINB = 1>
 static int launch_pair(const Geom &g, cudaStream_t s, MrhsArgs a, int block, bool xpay) {
     if constexpr (!std::is_same<typename SIO::real, float>::value) {
         return set_error(PLQCD_ERR_ARG, "dslash_mrhs: the RHS-pair kernel computes in FP32 only");
@@ -384,20 +392,130 @@ static int launch_pair(const Geom &g, cudaStream_t s, MrhsArgs a, int block, boo
         if (nblk > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: grid too large");
         if constexpr (ST == 0) {
             if (xpay)
-                k_dslash_mrhs_pair<SIO, LIO, true><<<(unsigned)nblk, block, 0, s>>>(a);
+                k_dslash_mrhs_pair<SIO, LIO, true, MINB><<<(unsigned)nblk, block, 0, s>>>(a);
             else
-                k_dslash_mrhs_pair<SIO, LIO, false><<<(unsigned)nblk, block, 0, s>>>(a);
+                k_dslash_mrhs_pair<SIO, LIO, false, MINB><<<(unsigned)nblk, block, 0, s>>>(a);
         } else {
             constexpr int NS = LIO::NSLOT + 2 * SIO::NSLOT;
-            const size_t smem = (size_t)ST * NS * 16 * block;
+            const size_t smem = (size_t)(ST * NS + (xpay ? 2 * SIO::NSLOT : 0)) * 16 * block;
             if (smem > 227 * 1024) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: %zu bytes of shared memory", smem);
-            auto k = xpay ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true> : k_dslash_mrhs_pair_pipe<SIO, LIO, ST, false>;
+            auto k = xpay ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB>
+                          : k_dslash_mrhs_pair_pipe<SIO, LIO, ST, false, MINB>;
             PLQCD_TRY(smem_optin((const void *)k, 227 * 1024));
             k<<<(unsigned)nblk, block, smem, s>>>(a);
         }
         PLQCD_CUDA_TRY(cudaGetLastError());
         return PLQCD_OK;
     }
+}
+
+// FP64 link-sharing kernel: a block of NRB warps covers 32 consecutive
+// output sites for NRB right-hand sides (warp w = RHS w of the block's
+// group, lane = site). Per direction the block copies the links of its 32
+// sites into shared memory once (cp.async, each warp a share of the
+// planes) and every warp copies its own neighbour spinors; all NRB warps
+// then read the links from shared memory. A link crosses L2->SM once per
+// NRB RHS instead of once per RHS, which is what bounds the FP64 multi-RHS
+// hop when each RHS is a separate block. The ring holds ST directions with
+// one block barrier per direction: stage k + ST - 1 is refilled into the
+// slot of stage k - 1 after the barrier that every warp passes once it has
+// computed k - 1. Threads past the last site or RHS copy in-bounds data and
+// store nothing. Same arithmetic, so the same bits, as the other kernels.
+template <class LIO, int NRB, int ST, bool XPAY>
+__global__ void __launch_bounds__(32 * NRB) k_dslash_mrhs_f64blk(const MrhsArgs a) {
+    using SIO = SpinorIO<PLQCD_F64>;
+    constexpr int NT = 32 * NRB;
+    constexpr int LP = LIO::NE;            // link planes, 16 bytes a site each
+    constexpr int LB = LP * 32;            // link slots of the block's sites
+    constexpr int STAGE = LB + SIO::NSLOT * NT;
+    extern __shared__ uint4 smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int grp = blockIdx.x % a.ntiles;
+    const int h0 = (blockIdx.x / a.ntiles) * 32;
+    const int r = grp * NRB + w;
+    const bool rhs_ok = r < a.nrhs;
+    const int h = h0 + lane;
+    const bool site_ok = h < a.Vh;
+    const int hc = site_ok ? h : h0;  // h0 < Vh: out-of-range lanes copy a valid site
+    const char *in = a.in + (size_t)(rhs_ok ? r : 0) * a.fbytes;
+    const int par = a.out_parity, opp = par ^ 1;
+    const long Vh = a.Vh;
+    const int L0h = a.L0h, L1 = a.L1, L2 = a.L2, L3 = a.L3;
+    const Coords c = site_coords(hc, par, L0h, L1, L2);
+    const int xh = hc - c.row * L0h;
+    int nb[8];
+    neighbour_sites(c, xh, a.L0, L0h, L1, L2, L3, nb);
+    const double sg = a.g5_in;
+
+    const uint32_t base = smem_addr(smem);
+    // direction k of dir_at into ring slot k % ST: link planes e = w, w + NRB,
+    // ... of site lane (the link of the lane's own site, or of its backward
+    // neighbour), then this thread's neighbour spinor
+    auto issue = [&](int k) {
+        const int d = dir_at(k);
+        const uint32_t st = base + (uint32_t)((k % ST) * STAGE) * 16u;
+        const int lsite = d < 4 ? hc : nb[d];
+        const int lpar = d < 4 ? par : opp;
+        const double2 *lp = static_cast<const double2 *>(a.gauge) + ((long)(lpar * 4 + (d & 3)) * LP) * Vh + lsite;
+#pragma unroll
+        for (int e = w; e < LP; e += NRB) cp_async16_cg(st + (uint32_t)(e * 32 + lane) * 16u, lp + e * Vh);
+        SIO::issue(in, Vh, nb[d], st + (uint32_t)(LB + threadIdx.x) * 16u, NT * 16);
+    };
+#pragma unroll
+    for (int k = 0; k < ST - 1; k++) {
+        issue(k);
+        cp_async_commit();
+    }
+    cx<double> acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = {0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        cp_async_wait<ST - 2>();  // this thread's copies of stage k
+        __syncthreads();          // everyone's copies of stage k; everyone done with k - 1
+        if (k + ST - 1 < 8) issue(k + ST - 1);
+        cp_async_commit();
+        const uint4 *stg = smem + (k % ST) * STAGE;
+        cx<double> U[9], s[12];
+        double n;
+        LIO::load_staged(stg + lane, 32, U);
+        SIO::load_staged_raw(stg + LB + threadIdx.x, NT, s, n);
+        compute_dir_n<false, false, double>(dir_at(k), acc, s, U, sg, n);
+    }
+    if (!site_ok || !rhs_ok) return;
+    const double aup = a.a_up, alow = a.a_low;
+    if (XPAY) {
+        cx<double> xv[12];
+        SIO::load(a.x + (size_t)r * a.fbytes, Vh, h, xv);
+        const double b = a.b;
+#pragma unroll
+        for (int k = 0; k < 12; k++) {
+            const double ak = k < 6 ? aup : alow;
+            acc[k] = {fma(ak, acc[k].re, b * xv[k].re), fma(ak, acc[k].im, b * xv[k].im)};
+        }
+    } else {
+#pragma unroll
+        for (int k = 6; k < 12; k++) acc[k] = {alow * acc[k].re, alow * acc[k].im};
+#pragma unroll
+        for (int k = 0; k < 6; k++) acc[k] = {aup * acc[k].re, aup * acc[k].im};
+    }
+    SIO::store(a.out + (size_t)r * a.fbytes, Vh, h, acc);
+}
+
+template <class LIO, int NRB, int ST>
+static int launch_f64blk(const Geom &g, cudaStream_t s, MrhsArgs a, bool xpay) {
+    if (g.Vh >= (1L << 31)) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: lattice too large for 32-bit sites");
+    a.ntiles = (a.nrhs + NRB - 1) / NRB;
+    const long nblk = (g.Vh + 31) / 32 * a.ntiles;
+    if (nblk > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: grid too large");
+    constexpr int STAGE = LIO::NE * 32 + SpinorIO<PLQCD_F64>::NSLOT * 32 * NRB;
+    const size_t smem = (size_t)ST * STAGE * 16;
+    if (smem > 227 * 1024) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: %zu bytes of shared memory", smem);
+    auto k = xpay ? k_dslash_mrhs_f64blk<LIO, NRB, ST, true> : k_dslash_mrhs_f64blk<LIO, NRB, ST, false>;
+    PLQCD_TRY(smem_optin((const void *)k, 227 * 1024));
+    k<<<(unsigned)nblk, 32 * NRB, smem, s>>>(a);
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
 }
 
 template <class SIO, class LIO, int NR, int ST>
@@ -444,6 +562,23 @@ static int launch_pr(const Geom &g, cudaStream_t s, const MrhsArgs &a, int nr, i
         case 2002: return launch_pair<S, L, 0>(g, s, a, block, xpay);
         case 2022: return launch_pair<S, L, 2>(g, s, a, block, xpay);
         case 2032: return launch_pair<S, L, 3>(g, s, a, block, xpay);
+        // 4000 + 100 * ring depth + RHS per block: FP64 link-sharing kernel
+        case 4208:
+        case 4204:
+        case 4308:
+        case 4304:
+            if constexpr (P == PLQCD_F64) {
+                switch (nr) {
+                    case 4208: return launch_f64blk<L, 8, 2>(g, s, a, xpay);
+                    case 4204: return launch_f64blk<L, 4, 2>(g, s, a, xpay);
+                    case 4308: return launch_f64blk<L, 8, 3>(g, s, a, xpay);
+                    default: return launch_f64blk<L, 4, 3>(g, s, a, xpay);
+                }
+            }
+            break;
+        // 2102 / 2122: the same with at most 128 registers a thread
+        case 2102: return launch_pair<S, L, 0, 2>(g, s, a, block, xpay);
+        case 2122: return launch_pair<S, L, 2, 2>(g, s, a, block, xpay);
         case 1: return launch_nr<S, L, 1>(g, s, a, block, xpay);
         case 2: return launch_nr<S, L, 2>(g, s, a, block, xpay);
         case 4:
@@ -532,7 +667,17 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
             t.block = blk;
             cands.push_back(t);
         }
-    for (int nr : {2022, 2032, 2002, 1022, 1042, 2, 1, 4}) {
+
+    // FP64: the link-sharing block kernel (4000 + 100 * depth + RHS per block)
+    if (prec == PLQCD_F64 && nrhs >= 4)
+        for (int v : {4208, 4204, 4308, 4304}) {
+            if ((v % 100) > nrhs) continue;
+            TuneResult t;
+            t.variant = v;
+            t.block = 32 * (v % 100);
+            cands.push_back(t);
+        }
+    for (int nr : {2022, 2122, 2032, 2002, 2102, 1022, 1042, 2, 1, 4}) {
         const bool pair = nr >= 2000;
         if (pair && (prec == PLQCD_F64 || nrhs < 2)) continue;
         const int tile = pair ? 2 : nr >= 1000 ? (nr / 10) % 10 : nr;
@@ -579,13 +724,13 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
             DslashCall c2 = dc;
             return launch_dslash_config(g, s, c2, t.variant - 100, t.block);
         }
-        if (t.variant >= 3000)
+        if (t.variant >= 3000 && t.variant < 4000)
             return launch_dslash_mrhs_tc(g, s, gauge, prec, recon, out, in, nrhs, out_parity, flags, a, x, b,
                                          t.variant - 3000);
         return mrhs_dispatch(g, s, prec, recon, m, t.variant, t.block, xpay);
     }
     auto launch = [&](const TuneResult &t, char *dst) -> int {
-        if (t.variant >= 3000)
+        if (t.variant >= 3000 && t.variant < 4000)
             return launch_dslash_mrhs_tc(g, s, gauge, prec, recon, dst, in, nrhs, out_parity, flags, a, x, b,
                                          t.variant - 3000);
         if (t.variant >= 100 && t.variant < 1000) {

@@ -35,6 +35,7 @@ namespace plqcd {
 struct McgState {  // device arrays of length nrhs, plus reduction scratch
     double *rr, *rr_old, *pAp, *alpha, *beta, *sr2, *bp2, *maxrr, *target, *aux;
     int *active, *conv_iter;
+    int *fresh;  // 1: the sloppy solution x_s was folded into x and counts as zero
     double *partials;  // nrhs * nb
     unsigned *counters;
     int nrhs, nb;
@@ -58,10 +59,11 @@ __device__ __forceinline__ void mapply(MOp op, int f, double s, const McgState &
             st.pAp[f] = s;
             st.alpha[f] = s > 0 ? st.rr[f] / s : 0.0;
             break;
-        case M_RR:
+        case M_RR:  // (k_mcg_update: every block has read fresh[f] by now)
             st.rr_old[f] = st.rr[f];
             st.rr[f] = s;
             st.beta[f] = st.rr_old[f] > 0 ? s / st.rr_old[f] : 0.0;
+            st.fresh[f] = 0;
             break;
         case M_SR2: st.sr2[f] = s; break;
         case M_RR_TRUE:
@@ -156,7 +158,33 @@ __global__ void __launch_bounds__(kBlasBlock) k_msub_norm2(char *out, const char
     mreduce(v, st, op, 0.0);
 }
 
-// x_s += alpha_f p ; r_s -= alpha_f Ap ; |r_s|^2 -> M_RR (active RHS only)
+// z = a - b (F64) ; |z|^2 -> op ; out = z in the sloppy format SP (the
+// FP64 z itself is not stored: the mixed solver only restarts from it)
+template <int SP>
+__global__ void __launch_bounds__(kBlasBlock) k_msub_norm2_to(char *out, size_t fbo, const char *a, const char *b,
+                                                              size_t fb, long Vh, McgState st, MOp op) {
+    using RS = typename SpinorIO<SP>::real;
+    const int f = blockIdx.y;
+    const size_t o = (size_t)f * fb;
+    double v = 0;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<double> av[12], bv[12];
+        SpinorIO<PLQCD_F64>::load(a + o, Vh, h, av);
+        SpinorIO<PLQCD_F64>::load(b + o, Vh, h, bv);
+        cx<RS> d[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) {
+            av[k] = csub(av[k], bv[k]);
+            d[k] = {(RS)av[k].re, (RS)av[k].im};
+        }
+        SpinorIO<SP>::store(out + (size_t)f * fbo, Vh, h, d);
+        v += n2(av);
+    }
+    mreduce(v, st, op, 0.0);
+}
+
+// x_s += alpha_f p (x_s = alpha_f p when fresh) ; r_s -= alpha_f Ap ;
+// |r_s|^2 -> M_RR (active RHS only)
 template <int P, int XP>
 __global__ void __launch_bounds__(kBlasBlock) k_mcg_update(char *xs, size_t fbx, char *rs, const char *p,
                                                            const char *Ap, size_t fb, long Vh, McgState st) {
@@ -168,6 +196,7 @@ __global__ void __launch_bounds__(kBlasBlock) k_mcg_update(char *xs, size_t fbx,
     const R a = (R)alpha;
     const RX ax = (RX)alpha;
     const size_t o = (size_t)f * fb, ox = (size_t)f * fbx;
+    const bool fresh = st.fresh[f] != 0;
     double v = 0;
     for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
         cx<R> pv[12], av[12], rv[12];
@@ -175,7 +204,12 @@ __global__ void __launch_bounds__(kBlasBlock) k_mcg_update(char *xs, size_t fbx,
         SpinorIO<P>::load(p + o, Vh, h, pv);
         SpinorIO<P>::load(Ap + o, Vh, h, av);
         SpinorIO<P>::load(rs + o, Vh, h, rv);
-        SpinorIO<XP>::load(xs + ox, Vh, h, xv);
+        if (fresh) {
+#pragma unroll
+            for (int k = 0; k < 12; k++) xv[k] = {RX(0), RX(0)};
+        } else {
+            SpinorIO<XP>::load(xs + ox, Vh, h, xv);
+        }
 #pragma unroll
         for (int k = 0; k < 12; k++) {
             xv[k] = {fma(ax, (RX)pv[k].re, xv[k].re), fma(ax, (RX)pv[k].im, xv[k].im)};
@@ -206,23 +240,23 @@ __global__ void __launch_bounds__(kBlasBlock) k_mcg_p(char *p, const char *rs, s
     }
 }
 
-// x64 += x_s ; x_s = 0 (every RHS; converged ones hold x_s = 0)
+// x64 += x_s for every RHS whose x_s is not fresh. x_s is not cleared:
+// k_ctl_reliable marks it fresh (zero) afterwards, and the next
+// k_mcg_update writes it without reading it.
 template <int XP>
-__global__ void __launch_bounds__(kBlasBlock) k_maccum_zero(char *x64, size_t fb64, char *xs, size_t fbx, long Vh) {
+__global__ void __launch_bounds__(kBlasBlock) k_maccum(char *x64, size_t fb64, const char *xs, size_t fbx, long Vh,
+                                                       McgState st) {
     const int f = blockIdx.y;
+    if (st.fresh[f]) return;
     using RX = typename SpinorIO<XP>::real;
     for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
         cx<double> xv[12];
-        cx<RX> sv[12], z[12];
+        cx<RX> sv[12];
         SpinorIO<PLQCD_F64>::load(x64 + (size_t)f * fb64, Vh, h, xv);
         SpinorIO<XP>::load(xs + (size_t)f * fbx, Vh, h, sv);
 #pragma unroll
-        for (int k = 0; k < 12; k++) {
-            xv[k] = {xv[k].re + (double)sv[k].re, xv[k].im + (double)sv[k].im};
-            z[k] = {RX(0), RX(0)};
-        }
+        for (int k = 0; k < 12; k++) xv[k] = {xv[k].re + (double)sv[k].re, xv[k].im + (double)sv[k].im};
         SpinorIO<PLQCD_F64>::store(x64 + (size_t)f * fb64, Vh, h, xv);
-        SpinorIO<XP>::store(xs + (size_t)f * fbx, Vh, h, z);
     }
 }
 
@@ -276,10 +310,12 @@ __global__ void k_ctl_iter(McgControl *c, const McgState *st, int nst, int mixed
     }
 }
 
-// after a reliable update: retire converged RHS, tighten convergence triggers
+// after a reliable update: every x_s was folded into x (fresh), retire
+// converged RHS, tighten convergence triggers
 __global__ void k_ctl_reliable(McgControl *c, const McgState *st, int nst) {
     for (int s = 0; s < nst; s++)
         for (int f = threadIdx.x; f < st[s].nrhs; f += blockDim.x) {
+            st[s].fresh[f] = 1;
             if (!st[s].active[f]) continue;
             st[s].maxrr[f] = st[s].rr[f];
             if (st[s].sr2[f] <= c->tol2 * st[s].bp2[f]) {
@@ -372,6 +408,27 @@ struct Batch {
         PLQCD_CUDA_TRY(cudaGetLastError());
         return PLQCD_OK;
     }
+    // out (sloppy format) = a - b, |a - b|^2 -> op
+    int sub_norm2_to(Item &it, void *out, int prec, const void *a, const void *b, MOp op) {
+        dim3 grid(it.st.nb, it.in.nrhs);
+        const size_t fbo = spinor_parity_bytes(it.g->Vh, prec);
+#define F(P) dev::k_msub_norm2_to<P><<<grid, kBlasBlock, 0, s>>>((char *)out, fbo, (const char *)a, (const char *)b, it.fb64, it.g->Vh, it.st, op)
+        MCG_PREC_SWITCH(prec, F)
+#undef F
+        PLQCD_CUDA_TRY(cudaGetLastError());
+        return PLQCD_OK;
+    }
+    int accum(Item &it) {
+        dim3 grid(it.st.nb, it.in.nrhs);
+        if (it.xprec == PLQCD_F64)
+            dev::k_maccum<PLQCD_F64><<<grid, kBlasBlock, 0, s>>>((char *)it.in.x_even, it.fb64, it.xs, it.fbx,
+                                                                it.g->Vh, it.st);
+        else
+            dev::k_maccum<PLQCD_F32><<<grid, kBlasBlock, 0, s>>>((char *)it.in.x_even, it.fb64, it.xs, it.fbx,
+                                                                it.g->Vh, it.st);
+        PLQCD_CUDA_TRY(cudaGetLastError());
+        return PLQCD_OK;
+    }
     int sub_norm2(Item &it, void *out, const void *a, const void *b, MOp op) {
         dim3 grid(it.st.nb, it.in.nrhs);
         dev::k_msub_norm2<<<grid, kBlasBlock, 0, s>>>((char *)out, (const char *)a, (const char *)b, it.fb64,
@@ -421,25 +478,19 @@ struct Batch {
     }
     int part_reliable() {
         for (Item &it : items) {
-            dim3 grid(it.st.nb, it.in.nrhs);
-            if (it.xprec == PLQCD_F64)
-                dev::k_maccum_zero<PLQCD_F64><<<grid, kBlasBlock, 0, s>>>((char *)it.in.x_even, it.fb64, it.xs,
-                                                                         it.fbx, it.g->Vh);
-            else
-                dev::k_maccum_zero<PLQCD_F32><<<grid, kBlasBlock, 0, s>>>((char *)it.in.x_even, it.fb64, it.xs,
-                                                                         it.fbx, it.g->Vh);
-            PLQCD_CUDA_TRY(cudaGetLastError());
+            PLQCD_TRY(accum(it));
             // FP64: solution and Schur residual b' - Mhat x (convergence)
             PLQCD_TRY(mhat(it, it.in.g64, it.t64, it.in.x_even, it.tmp64, false));
-            PLQCD_TRY(sub_norm2(it, it.r64, it.bprime, it.t64, M_SR2));
             // restart direction Mhat^dag r: the sloppy operator's accuracy
-            // suffices (FP64 when the solve is FP64)
+            // suffices (FP64 when the solve is FP64), so the mixed solve
+            // writes r only in the sloppy format
             if (mixed) {
                 const plqcd_gauge *gs = it.in.g_sloppy ? it.in.g_sloppy : it.in.g64;
-                PLQCD_TRY(convert(it, it.t, it.ps, it.r64, PLQCD_F64));
+                PLQCD_TRY(sub_norm2_to(it, it.t, it.ps, it.bprime, it.t64, M_SR2));
                 PLQCD_TRY(mhat(it, gs, it.rs, it.t, it.tmps, true));
                 PLQCD_TRY(norm2(it, it.rs, it.ps, M_RR_TRUE, false));
             } else {
+                PLQCD_TRY(sub_norm2(it, it.r64, it.bprime, it.t64, M_SR2));
                 PLQCD_TRY(mhat(it, it.in.g64, it.t64, it.r64, it.tmp64, true));
                 PLQCD_TRY(norm2(it, it.t64, PLQCD_F64, M_RR_TRUE, false));
                 PLQCD_TRY(convert(it, it.rs, it.ps, it.t64, PLQCD_F64));
@@ -491,7 +542,7 @@ int alloc_item(Batch &B, Item &it, bool own_ws) {
     it.st.nb = red_blocks(Vh, n);
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t need = 4 * al(it.fb64 * n) + 5 * al(it.fbs * n) + al(it.fbx * n) + 10 * al(sizeof(double) * n) +
-                        2 * al(sizeof(int) * n) + al(sizeof(double) * n * it.st.nb) + al(sizeof(unsigned) * n);
+                        3 * al(sizeof(int) * n) + al(sizeof(double) * n * it.st.nb) + al(sizeof(unsigned) * n);
     void *ws = nullptr;
     if (own_ws) {
         if (cudaMalloc(&it.mem, need) != cudaSuccess) {
@@ -523,12 +574,14 @@ int alloc_item(Batch &B, Item &it, bool own_ws) {
     for (double **d : dd) *d = reinterpret_cast<double *>(take(sizeof(double) * n));
     it.st.active = reinterpret_cast<int *>(take(sizeof(int) * n));
     it.st.conv_iter = reinterpret_cast<int *>(take(sizeof(int) * n));
+    it.st.fresh = reinterpret_cast<int *>(take(sizeof(int) * n));
     it.st.partials = reinterpret_cast<double *>(take(sizeof(double) * n * it.st.nb));
     it.st.counters = reinterpret_cast<unsigned *>(take(sizeof(unsigned) * n));
     cudaStream_t s = B.s;
     PLQCD_CUDA_TRY(cudaMemsetAsync(it.st.counters, 0, sizeof(unsigned) * n, s));
     PLQCD_CUDA_TRY(cudaMemsetAsync(it.st.conv_iter, 0xff, sizeof(int) * n, s));
     dev::k_mfill_int<<<1, 256, 0, s>>>(it.st.active, n, 1);
+    dev::k_mfill_int<<<1, 256, 0, s>>>(it.st.fresh, n, 1);  // x_s = 0
     PLQCD_CUDA_TRY(cudaGetLastError());
     return PLQCD_OK;
 }
@@ -561,7 +614,6 @@ int start_item(Batch &B, Item &it) {
     PLQCD_TRY(B.hop(it, in.g64, it.bprime, in.b_odd, PLQCD_EVEN, 0, in.b_even, B.kappa, 1.0));
     PLQCD_TRY(B.norm2(it, it.bprime, PLQCD_F64, M_BP2, false));
     PLQCD_CUDA_TRY(cudaMemsetAsync(in.x_even, 0, it.fb64 * n, s));
-    PLQCD_CUDA_TRY(cudaMemsetAsync(it.xs, 0, it.fbx * n, s));
     const plqcd_gauge *gs = in.g_sloppy ? in.g_sloppy : in.g64;
     if (B.mixed) {
         // the start residual Mhat^dag b' only seeds the sloppy recursion (the
@@ -791,13 +843,7 @@ extern "C" int plqcd_invert_cg_batch(plqcd_solve_item *items, int nitems, const 
         }
         // fold in unconverged sloppy solutions, rebuild x_o, full-lattice residuals
         for (Item &it : B.items) {
-            dim3 grid(it.st.nb, it.in.nrhs);
-            if (it.xprec == PLQCD_F64)
-                dev::k_maccum_zero<PLQCD_F64><<<grid, kBlasBlock, 0, B.s>>>((char *)it.in.x_even, it.fb64, it.xs,
-                                                                           it.fbx, it.g->Vh);
-            else
-                dev::k_maccum_zero<PLQCD_F32><<<grid, kBlasBlock, 0, B.s>>>((char *)it.in.x_even, it.fb64, it.xs,
-                                                                           it.fbx, it.g->Vh);
+            if ((rc = B.accum(it))) break;
             if ((rc = B.hop(it, it.in.g64, it.in.x_odd, it.in.x_even, PLQCD_ODD, 0, it.in.b_odd, B.kappa, 1.0))) break;
         }
         if (rc) break;

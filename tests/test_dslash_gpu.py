@@ -485,14 +485,14 @@ def test_multi_rhs_every_variant(cuda, monkeypatch, variant, block, prec, recon,
         assert relmax(a, b) <= tol, (variant, r, relmax(a, b))
 
 
-@pytest.mark.parametrize("variant", [2002, 2022, 2032])
+@pytest.mark.parametrize("variant", [2002, 2022, 2032, 2102, 2122])
 @pytest.mark.parametrize("nrhs", [1, 2, 5, 8])
 @pytest.mark.parametrize("prec,recon", [(P.F32, 18), (P.F32, 12), (P.F16, 12), (P.BF16, 12)])
 @pytest.mark.parametrize("xpay", [False, True])
 def test_multi_rhs_pair_kernel_is_bit_identical(cuda, monkeypatch, variant, nrhs, prec, recon, xpay):
     """The RHS-pair kernels (two RHS on the lanes of packed FP32
     instructions: 2002 direct loads, 2022 / 2032 cp.async pipeline of depth
-    2 / 3), forced past the tuner, store the same bytes as the single-RHS
+    2 / 3, 2102 / 2122 with at most 128 registers), forced past the tuner, store the same bytes as the single-RHS
     kernel for every field of the block, an odd last RHS included."""
     L = (8, 4, 6, 8)
     lat, g64, u = _device_setup(L, 23)
@@ -520,6 +520,44 @@ def test_multi_rhs_pair_kernel_is_bit_identical(cuda, monkeypatch, variant, nrhs
             lat.dslash(g, one, blk_in[sl], 0, prec)
         lat.synchronize()
         assert bool((blk_out[sl] == one).all()), (r, prec, recon, xpay)
+
+
+@pytest.mark.parametrize("variant", [4208, 4204, 4308, 4304])
+@pytest.mark.parametrize("nrhs", [4, 5, 11])
+@pytest.mark.parametrize("recon", [18, 12])
+@pytest.mark.parametrize("xpay", [False, True])
+def test_multi_rhs_f64_link_sharing_kernel_is_bit_identical(cuda, monkeypatch, variant, nrhs, recon, xpay):
+    """The FP64 link-sharing kernel (4000 + 100 * ring depth + RHS per block:
+    a block's warps are RHS of the same 32 sites and read each link from
+    shared memory), forced past the tuner, stores the same bytes as the
+    single-RHS kernel for every field, with a partial last RHS group and a
+    half volume (720) that is not a multiple of 32 sites."""
+    L = (6, 4, 6, 10)
+    lat, g64, u = _device_setup(L, 29)
+    g = g64 if recon == 18 else P.Gauge(lat, P.F64, 12)
+    if g is not g64:
+        g.copy_from(g64)
+    bs = lat.spinor_bytes(P.F64)
+    blk_in, blk_out, blk_x = dev_bytes(nrhs * bs), dev_bytes(nrhs * bs), dev_bytes(nrhs * bs)
+    for r in range(nrhs):
+        lat.spinor_gaussian(blk_in[r * bs:(r + 1) * bs], P.F64, 0, 700 + r)
+        lat.spinor_gaussian(blk_x[r * bs:(r + 1) * bs], P.F64, 1, 800 + r)
+    monkeypatch.setenv("PLQCD_MRHS_VARIANT", str(variant))
+    flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
+    if xpay:
+        lat.dslash_mrhs_xpay(g, blk_out, blk_in, nrhs, 1, P.F64, -0.0144, blk_x, 1.0, flags)
+    else:
+        lat.dslash_mrhs(g, blk_out, blk_in, nrhs, 1, P.F64)
+    monkeypatch.delenv("PLQCD_MRHS_VARIANT")
+    for r in range(nrhs):
+        sl = slice(r * bs, (r + 1) * bs)
+        one = dev_bytes(bs)
+        if xpay:
+            lat.dslash_xpay(g, one, blk_in[sl], 1, P.F64, -0.0144, blk_x[sl], 1.0, flags)
+        else:
+            lat.dslash(g, one, blk_in[sl], 1, P.F64)
+        lat.synchronize()
+        assert bool((blk_out[sl] == one).all()), (variant, r)
 
 
 @pytest.mark.parametrize("tiles,nrhs", [(1, 8), (1, 12), (2, 16), (2, 20), (4, 32), (1, 3)])
