@@ -59,11 +59,10 @@ __device__ __forceinline__ void mapply(MOp op, int f, double s, const McgState &
             st.pAp[f] = s;
             st.alpha[f] = s > 0 ? st.rr[f] / s : 0.0;
             break;
-        case M_RR:  // (k_mcg_update: every block has read fresh[f] by now)
+        case M_RR:
             st.rr_old[f] = st.rr[f];
             st.rr[f] = s;
             st.beta[f] = st.rr_old[f] > 0 ? s / st.rr_old[f] : 0.0;
-            st.fresh[f] = 0;
             break;
         case M_SR2: st.sr2[f] = s; break;
         case M_RR_TRUE:
@@ -183,77 +182,95 @@ __global__ void __launch_bounds__(kBlasBlock) k_msub_norm2_to(char *out, size_t 
     mreduce(v, st, op, 0.0);
 }
 
-// x_s += alpha_f p (x_s = alpha_f p when fresh) ; r_s -= alpha_f Ap ;
-// |r_s|^2 -> M_RR (active RHS only)
-template <int P, int XP>
-__global__ void __launch_bounds__(kBlasBlock) k_mcg_update(char *xs, size_t fbx, char *rs, const char *p,
-                                                           const char *Ap, size_t fb, long Vh, McgState st) {
+// r_s -= alpha_f Ap ; |r_s|^2 -> M_RR (active RHS only). The solution
+// update x_s += alpha_f p of the same iteration happens in k_mcg_p, which
+// reads p anyway (or, in an iteration with a reliable update, in k_maccum).
+template <int P>
+__global__ void __launch_bounds__(kBlasBlock) k_mcg_update(char *rs, const char *Ap, size_t fb, long Vh, McgState st) {
     const int f = blockIdx.y;
     if (!st.active[f]) return;
     using R = typename SpinorIO<P>::real;
-    using RX = typename SpinorIO<XP>::real;
-    const double alpha = st.alpha[f];
-    const R a = (R)alpha;
-    const RX ax = (RX)alpha;
-    const size_t o = (size_t)f * fb, ox = (size_t)f * fbx;
-    const bool fresh = st.fresh[f] != 0;
+    const R a = (R)st.alpha[f];
+    const size_t o = (size_t)f * fb;
     double v = 0;
     for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
-        cx<R> pv[12], av[12], rv[12];
-        cx<RX> xv[12];
-        SpinorIO<P>::load(p + o, Vh, h, pv);
+        cx<R> av[12], rv[12];
         SpinorIO<P>::load(Ap + o, Vh, h, av);
         SpinorIO<P>::load(rs + o, Vh, h, rv);
-        if (fresh) {
 #pragma unroll
-            for (int k = 0; k < 12; k++) xv[k] = {RX(0), RX(0)};
-        } else {
-            SpinorIO<XP>::load(xs + ox, Vh, h, xv);
-        }
-#pragma unroll
-        for (int k = 0; k < 12; k++) {
-            xv[k] = {fma(ax, (RX)pv[k].re, xv[k].re), fma(ax, (RX)pv[k].im, xv[k].im)};
-            rv[k] = {fma(-a, av[k].re, rv[k].re), fma(-a, av[k].im, rv[k].im)};
-        }
-        SpinorIO<XP>::store(xs + ox, Vh, h, xv);
+        for (int k = 0; k < 12; k++) rv[k] = {fma(-a, av[k].re, rv[k].re), fma(-a, av[k].im, rv[k].im)};
         SpinorIO<P>::store(rs + o, Vh, h, rv);
         v += n2(rv);
     }
     mreduce(v, st, M_RR, 0.0);
 }
 
-// p = r + beta_f p (active RHS only)
-template <int P>
-__global__ void __launch_bounds__(kBlasBlock) k_mcg_p(char *p, const char *rs, size_t fb, long Vh, McgState st) {
+// x_s += alpha_f p (x_s = alpha_f p when fresh), unless this iteration's
+// reliable update already folded alpha_f p into x; then p = r + beta_f p
+// (active RHS only)
+template <int P, int XP>
+__global__ void __launch_bounds__(kBlasBlock) k_mcg_p(char *p, const char *rs, char *xs, size_t fb, size_t fbx,
+                                                      long Vh, McgState st, const McgControl *ctl) {
     const int f = blockIdx.y;
     if (!st.active[f]) return;
     using R = typename SpinorIO<P>::real;
+    using RX = typename SpinorIO<XP>::real;
     const R beta = (R)st.beta[f];
-    const size_t o = (size_t)f * fb;
+    const RX ax = (RX)st.alpha[f];
+    const bool xup = !ctl->need_reliable, fresh = st.fresh[f] != 0;
+    const size_t o = (size_t)f * fb, ox = (size_t)f * fbx;
     for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
         cx<R> pv[12], rv[12];
         SpinorIO<P>::load(p + o, Vh, h, pv);
         SpinorIO<P>::load(rs + o, Vh, h, rv);
+        if (xup) {
+            cx<RX> xv[12];
+            if (fresh) {
+#pragma unroll
+                for (int k = 0; k < 12; k++) xv[k] = {RX(0), RX(0)};
+            } else {
+                SpinorIO<XP>::load(xs + ox, Vh, h, xv);
+            }
+#pragma unroll
+            for (int k = 0; k < 12; k++)
+                xv[k] = {fma(ax, (RX)pv[k].re, xv[k].re), fma(ax, (RX)pv[k].im, xv[k].im)};
+            SpinorIO<XP>::store(xs + ox, Vh, h, xv);
+        }
 #pragma unroll
         for (int k = 0; k < 12; k++) pv[k] = {fma(beta, pv[k].re, rv[k].re), fma(beta, pv[k].im, rv[k].im)};
         SpinorIO<P>::store(p + o, Vh, h, pv);
     }
 }
 
-// x64 += x_s for every RHS whose x_s is not fresh. x_s is not cleared:
-// k_ctl_reliable marks it fresh (zero) afterwards, and the next
-// k_mcg_update writes it without reading it.
-template <int XP>
-__global__ void __launch_bounds__(kBlasBlock) k_maccum(char *x64, size_t fb64, const char *xs, size_t fbx, long Vh,
-                                                       McgState st) {
+// x64 += x_s for every active RHS (WITH_P: x64 += x_s + alpha_f p, the
+// update of the current iteration, computed as k_mcg_p would); a fresh x_s
+// counts as zero. x_s is not cleared: k_ctl_reliable marks it fresh.
+template <int P, int XP, bool WITH_P>
+__global__ void __launch_bounds__(kBlasBlock) k_maccum(char *x64, size_t fb64, const char *xs, size_t fbx,
+                                                       const char *p, size_t fb, long Vh, McgState st) {
     const int f = blockIdx.y;
-    if (st.fresh[f]) return;
+    const bool fresh = st.fresh[f] != 0;
+    if (!st.active[f] || (fresh && !WITH_P)) return;
+    using R = typename SpinorIO<P>::real;
     using RX = typename SpinorIO<XP>::real;
+    const RX ax = (RX)st.alpha[f];
     for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
         cx<double> xv[12];
         cx<RX> sv[12];
         SpinorIO<PLQCD_F64>::load(x64 + (size_t)f * fb64, Vh, h, xv);
-        SpinorIO<XP>::load(xs + (size_t)f * fbx, Vh, h, sv);
+        if (fresh) {
+#pragma unroll
+            for (int k = 0; k < 12; k++) sv[k] = {RX(0), RX(0)};
+        } else {
+            SpinorIO<XP>::load(xs + (size_t)f * fbx, Vh, h, sv);
+        }
+        if (WITH_P) {
+            cx<R> pv[12];
+            SpinorIO<P>::load(p + (size_t)f * fb, Vh, h, pv);
+#pragma unroll
+            for (int k = 0; k < 12; k++)
+                sv[k] = {fma(ax, (RX)pv[k].re, sv[k].re), fma(ax, (RX)pv[k].im, sv[k].im)};
+        }
 #pragma unroll
         for (int k = 0; k < 12; k++) xv[k] = {xv[k].re + (double)sv[k].re, xv[k].im + (double)sv[k].im};
         SpinorIO<PLQCD_F64>::store(x64 + (size_t)f * fb64, Vh, h, xv);
@@ -331,7 +348,8 @@ __global__ void k_ctl_reliable(McgControl *c, const McgState *st, int nst) {
     }
 }
 
-// end of an iteration: continue while any RHS is active and iterations remain
+// end of an iteration: an x_s that k_mcg_p wrote is no longer fresh;
+// continue while any RHS is active and iterations remain
 __global__ void k_ctl_loop(McgControl *c, const McgState *st, int nst, int use_handle,
                            cudaGraphConditionalHandle h_while) {
     __shared__ int any;
@@ -339,7 +357,10 @@ __global__ void k_ctl_loop(McgControl *c, const McgState *st, int nst, int use_h
     __syncthreads();
     for (int s = 0; s < nst; s++)
         for (int f = threadIdx.x; f < st[s].nrhs; f += blockDim.x)
-            if (st[s].active[f]) atomicOr(&any, 1);
+            if (st[s].active[f]) {
+                atomicOr(&any, 1);
+                if (!c->need_reliable) st[s].fresh[f] = 0;
+            }
     __syncthreads();
     if (threadIdx.x == 0) {
         c->any_active = any;
@@ -418,14 +439,19 @@ struct Batch {
         PLQCD_CUDA_TRY(cudaGetLastError());
         return PLQCD_OK;
     }
-    int accum(Item &it) {
+    // x64 += x_s (with_p: + alpha p, the current iteration's update)
+    int accum(Item &it, bool with_p) {
         dim3 grid(it.st.nb, it.in.nrhs);
-        if (it.xprec == PLQCD_F64)
-            dev::k_maccum<PLQCD_F64><<<grid, kBlasBlock, 0, s>>>((char *)it.in.x_even, it.fb64, it.xs, it.fbx,
-                                                                it.g->Vh, it.st);
-        else
-            dev::k_maccum<PLQCD_F32><<<grid, kBlasBlock, 0, s>>>((char *)it.in.x_even, it.fb64, it.xs, it.fbx,
-                                                                it.g->Vh, it.st);
+#define G(P, XP, W) dev::k_maccum<P, XP, W><<<grid, kBlasBlock, 0, s>>>((char *)it.in.x_even, it.fb64, it.xs, it.fbx, it.p, it.fbs, it.g->Vh, it.st)
+#define F(P)                                                                 \
+    if (it.xprec == PLQCD_F64) {                                             \
+        if (with_p) G(P, PLQCD_F64, true); else G(P, PLQCD_F64, false);      \
+    } else {                                                                 \
+        if (with_p) G(P, PLQCD_F32, true); else G(P, PLQCD_F32, false);      \
+    }
+        MCG_PREC_SWITCH(it.ps, F)
+#undef F
+#undef G
         PLQCD_CUDA_TRY(cudaGetLastError());
         return PLQCD_OK;
     }
@@ -463,22 +489,16 @@ struct Batch {
             PLQCD_TRY(norm2(it, it.t, it.ps, M_ALPHA, true));
             PLQCD_TRY(mhat(it, gs, it.Ap, it.t, it.tmps, true));
             dim3 grid(it.st.nb, it.in.nrhs);
-            if (it.xprec == PLQCD_F64) {
-#define F(P) dev::k_mcg_update<P, PLQCD_F64><<<grid, kBlasBlock, 0, s>>>(it.xs, it.fbx, it.rs, it.p, it.Ap, it.fbs, it.g->Vh, it.st)
-                MCG_PREC_SWITCH(it.ps, F)
+#define F(P) dev::k_mcg_update<P><<<grid, kBlasBlock, 0, s>>>(it.rs, it.Ap, it.fbs, it.g->Vh, it.st)
+            MCG_PREC_SWITCH(it.ps, F)
 #undef F
-            } else {
-#define F(P) dev::k_mcg_update<P, PLQCD_F32><<<grid, kBlasBlock, 0, s>>>(it.xs, it.fbx, it.rs, it.p, it.Ap, it.fbs, it.g->Vh, it.st)
-                MCG_PREC_SWITCH(it.ps, F)
-#undef F
-            }
             PLQCD_CUDA_TRY(cudaGetLastError());
         }
         return PLQCD_OK;
     }
     int part_reliable() {
         for (Item &it : items) {
-            PLQCD_TRY(accum(it));
+            PLQCD_TRY(accum(it, true));
             // FP64: solution and Schur residual b' - Mhat x (convergence)
             PLQCD_TRY(mhat(it, it.in.g64, it.t64, it.in.x_even, it.tmp64, false));
             // restart direction Mhat^dag r: the sloppy operator's accuracy
@@ -501,7 +521,11 @@ struct Batch {
     int part_direction() {
         for (Item &it : items) {
             dim3 grid(it.st.nb, it.in.nrhs);
-#define F(P) dev::k_mcg_p<P><<<grid, kBlasBlock, 0, s>>>(it.p, it.rs, it.fbs, it.g->Vh, it.st)
+#define F(P)                                                                                                     \
+    if (it.xprec == PLQCD_F64)                                                                                   \
+        dev::k_mcg_p<P, PLQCD_F64><<<grid, kBlasBlock, 0, s>>>(it.p, it.rs, it.xs, it.fbs, it.fbx, it.g->Vh, it.st, ctl); \
+    else                                                                                                         \
+        dev::k_mcg_p<P, PLQCD_F32><<<grid, kBlasBlock, 0, s>>>(it.p, it.rs, it.xs, it.fbs, it.fbx, it.g->Vh, it.st, ctl);
             MCG_PREC_SWITCH(it.ps, F)
 #undef F
             PLQCD_CUDA_TRY(cudaGetLastError());
@@ -843,7 +867,7 @@ extern "C" int plqcd_invert_cg_batch(plqcd_solve_item *items, int nitems, const 
         }
         // fold in unconverged sloppy solutions, rebuild x_o, full-lattice residuals
         for (Item &it : B.items) {
-            if ((rc = B.accum(it))) break;
+            if ((rc = B.accum(it, false))) break;
             if ((rc = B.hop(it, it.in.g64, it.in.x_odd, it.in.x_even, PLQCD_ODD, 0, it.in.b_odd, B.kappa, 1.0))) break;
         }
         if (rc) break;
