@@ -36,6 +36,7 @@ struct MrhsArgs {
     int L0, L0h, L1, L2, L3;
     int out_parity;
     double a_up, a_low, b, g5_in;
+    RhsSink sink;  // fused CG sums (RHS-pair kernels, epi > 0)
 };
 
 template <class SIO, class LIO, int NR, bool XPAY>
@@ -198,6 +199,117 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
     }
 }
 
+__device__ __forceinline__ double sq_sum(const cx<float> v[12]) {
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < 12; k++) s += (double)v[k].re * v[k].re + (double)v[k].im * v[k].im;
+    return s;
+}
+
+// the block's per-RHS sums v0 (RHS r0) and v1 (r0 + 1) into the partials
+// [RHS][site block]; k_sink_finish adds them up
+__device__ void sink_block(const MrhsArgs &a, int r0, bool two, double v0, double v1) {
+    __shared__ double ws[2][8];
+    const int nsb = gridDim.x / a.ntiles, sb = blockIdx.x / a.ntiles;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+        v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+    }
+    if (lane == 0) {
+        ws[0][w] = v0;
+        ws[1][w] = v1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b0 = 0, b1 = 0;
+        for (int i = 0; i < nw; i++) {
+            b0 += ws[0][i];
+            b1 += ws[1][i];
+        }
+        a.sink.partials[(size_t)r0 * nsb + sb] = b0;
+        if (two) a.sink.partials[(size_t)(r0 + 1) * nsb + sb] = b1;
+    }
+}
+
+// one block per RHS: the sum of its nsb partials in a fixed order (thread
+// i takes i, i + blockDim, ..., then a fixed tree), applied to the solver's
+// scalars of an active RHS (see RhsSink)
+template <int EPI>
+__global__ void __launch_bounds__(1024) k_sink_finish(const RhsSink k, int nsb) {
+    __shared__ double ws[32];
+    const int f = blockIdx.x;
+    const double *p = k.partials + (size_t)f * nsb;
+    double t = 0;
+    for (int i = threadIdx.x; i < nsb; i += blockDim.x) t += p[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x != 0 || !k.active[f]) return;
+    double tot = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) tot += ws[i];
+    if (EPI == 1) {
+        k.pAp[f] = tot;
+        k.alpha[f] = tot > 0 ? k.rr[f] / tot : 0.0;
+    } else {
+        k.rr_old[f] = k.rr[f];
+        k.rr[f] = tot;
+        k.beta[f] = k.rr_old[f] > 0 ? tot / k.rr_old[f] : 0.0;
+    }
+}
+
+// epilogue of the RHS-pair kernels: scale (and xpay with x from xload(j,
+// xv)), then EPI 0 / 1: store (1: |out|^2 to the sink); EPI 2: r -= alpha
+// out in place, |r|^2 to the sink (out is not stored). Threads past the last
+// site (valid false) only take part in the sums.
+template <class SIO, bool XPAY, int EPI, class XLoad>
+__device__ __forceinline__ void pair_epilogue(const MrhsArgs &a, int r0, bool two, int h, bool valid,
+                                              const cx<f2> acc[12], XLoad xload) {
+    const float aup = (float)a.a_up, alow = (float)a.a_low, b = (float)a.b;
+    double v[2] = {0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        if ((j == 1 && !two) || !valid) break;
+        cx<float> o[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) o[k] = lane(acc[k], j);
+        if (XPAY) {
+            cx<float> xv[12];
+            xload(j, xv);
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const float ak = k < 6 ? aup : alow;
+                o[k] = {fmaf(ak, o[k].re, b * xv[k].re), fmaf(ak, o[k].im, b * xv[k].im)};
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                const float ak = k < 6 ? aup : alow;
+                o[k] = {ak * o[k].re, ak * o[k].im};
+            }
+        }
+        if (EPI == 2) {
+            const int f = r0 + j;
+            if (a.sink.active[f]) {
+                const float al = (float)a.sink.alpha[f];
+                char *rf = a.sink.rvec + (size_t)f * a.fbytes;
+                cx<float> rv[12];
+                SIO::load(rf, a.Vh, h, rv);
+#pragma unroll
+                for (int k = 0; k < 12; k++) rv[k] = {fmaf(-al, o[k].re, rv[k].re), fmaf(-al, o[k].im, rv[k].im)};
+                SIO::store(rf, a.Vh, h, rv);
+                v[j] = sq_sum(rv);
+            }
+        } else {
+            SIO::store(a.out + (size_t)(r0 + j) * a.fbytes, a.Vh, h, o);
+            if (EPI == 1) v[j] = sq_sum(o);
+        }
+    }
+    if (EPI > 0) sink_block(a, r0, two, v[0], v[1]);
+}
+
 // RHS-pair kernel: one thread, one output site, two right-hand sides on the
 // two lanes of Blackwell's packed FP32 instructions (FFMA2 / FMUL2 / FADD2):
 // lane 0 carries RHS r0, lane 1 RHS r0 + 1. The link is loaded, converted,
@@ -206,12 +318,14 @@ __global__ void __launch_bounds__(256) k_dslash_mrhs_pipe(const MrhsArgs a) {
 // compute_dir with the same rounding, so the results are the bits of the
 // other kernels. An odd last RHS runs in both lanes and is stored once.
 // (FP32-computing formats: F32, F16, BF16.)
-template <class SIO, class LIO, bool XPAY, int MINB = 1>
+template <class SIO, class LIO, bool XPAY, int MINB = 1, int EPI = 0>
 __global__ void __launch_bounds__(256, MINB) k_dslash_mrhs_pair(const MrhsArgs a) {
     static_assert(std::is_same<typename SIO::real, float>::value, "packed lanes hold FP32");
     const int tile = blockIdx.x % a.ntiles;
-    const int h = (blockIdx.x / a.ntiles) * blockDim.x + threadIdx.x;
-    if (h >= a.Vh) return;
+    const int hh = (blockIdx.x / a.ntiles) * blockDim.x + threadIdx.x;
+    const bool valid = hh < a.Vh;
+    if (EPI == 0 && !valid) return;  // (EPI > 0: every thread takes part in the sums)
+    const int h = valid ? hh : (int)a.Vh - 1;
     const int r0 = 2 * tile;
     const bool two = r0 + 1 < a.nrhs;
     const char *in0 = a.in + (size_t)r0 * a.fbytes;
@@ -248,31 +362,9 @@ __global__ void __launch_bounds__(256, MINB) k_dslash_mrhs_pair(const MrhsArgs a
         for (int e = 0; e < 12; e++) s[e] = zip(sa[e], sb[e]);
         compute_dir_n<false, SIO::kScaled, f2>(d, acc, s, Ub, sg, f2(na, nbv));
     }
-
-    const float aup = (float)a.a_up, alow = (float)a.a_low, b = (float)a.b;
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-        if (j == 1 && !two) break;
-        cx<float> o[12];
-#pragma unroll
-        for (int k = 0; k < 12; k++) o[k] = lane(acc[k], j);
-        if (XPAY) {
-            cx<float> xv[12];
-            SIO::load(a.x + (size_t)(r0 + j) * a.fbytes, Vh, h, xv);
-#pragma unroll
-            for (int k = 0; k < 12; k++) {
-                const float ak = k < 6 ? aup : alow;
-                o[k] = {fmaf(ak, o[k].re, b * xv[k].re), fmaf(ak, o[k].im, b * xv[k].im)};
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < 12; k++) {
-                const float ak = k < 6 ? aup : alow;
-                o[k] = {ak * o[k].re, ak * o[k].im};
-            }
-        }
-        SIO::store(a.out + (size_t)(r0 + j) * a.fbytes, Vh, h, o);
-    }
+    pair_epilogue<SIO, XPAY, EPI>(a, r0, two, h, valid, acc, [&](int j, cx<float> xv[12]) {
+        SIO::load(a.x + (size_t)(r0 + j) * a.fbytes, Vh, h, xv);
+    });
 }
 
 // Pipelined RHS-pair kernel: the link and the two neighbour spinors of a
@@ -280,15 +372,19 @@ __global__ void __launch_bounds__(256, MINB) k_dslash_mrhs_pair(const MrhsArgs a
 // the thread, ST directions ahead of the one being computed (as in
 // k_dslash_mrhs_pipe), so the loads stay in flight without holding the
 // registers the packed arithmetic needs.
-template <class SIO, class LIO, int ST, bool XPAY, int MINB = 1>
+template <class SIO, class LIO, int ST, bool XPAY, int MINB = 1, int EPI = 0>
 __global__ void __launch_bounds__(256, MINB) k_dslash_mrhs_pair_pipe(const MrhsArgs a) {
     static_assert(std::is_same<typename SIO::real, float>::value, "packed lanes hold FP32");
     extern __shared__ uint4 smem[];
     constexpr int NS = LIO::NSLOT + 2 * SIO::NSLOT;
     const int B = blockDim.x;
     const int tile = blockIdx.x % a.ntiles;
-    const int h = (blockIdx.x / a.ntiles) * B + threadIdx.x;
-    if (h >= a.Vh) return;  // no block-level barrier below
+    const int hh = (blockIdx.x / a.ntiles) * B + threadIdx.x;
+    const bool valid = hh < a.Vh;
+    // no block-level barrier below except the sums of EPI > 0, in which
+    // every thread (a past-the-end one on the last site) takes part
+    if (EPI == 0 && !valid) return;
+    const int h = valid ? hh : (int)a.Vh - 1;
     const int r0 = 2 * tile;
     const bool two = r0 + 1 < a.nrhs;
     const char *in0 = a.in + (size_t)r0 * a.fbytes;
@@ -352,56 +448,40 @@ __global__ void __launch_bounds__(256, MINB) k_dslash_mrhs_pair_pipe(const MrhsA
         if (k + ST < 8) issue(k + ST);
         cp_async_commit();
     }
-
-    const float aup = (float)a.a_up, alow = (float)a.a_low, b = (float)a.b;
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-        if (j == 1 && !two) break;
-        cx<float> o[12];
-#pragma unroll
-        for (int k = 0; k < 12; k++) o[k] = lane(acc[k], j);
-        if (XPAY) {
-            cx<float> xv[12];
-            SIO::load_staged(smem + threadIdx.x + (ST * NS + j * SIO::NSLOT) * B, B, xv);
-#pragma unroll
-            for (int k = 0; k < 12; k++) {
-                const float ak = k < 6 ? aup : alow;
-                o[k] = {fmaf(ak, o[k].re, b * xv[k].re), fmaf(ak, o[k].im, b * xv[k].im)};
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < 12; k++) {
-                const float ak = k < 6 ? aup : alow;
-                o[k] = {ak * o[k].re, ak * o[k].im};
-            }
-        }
-        SIO::store(a.out + (size_t)(r0 + j) * a.fbytes, Vh, h, o);
-    }
+    pair_epilogue<SIO, XPAY, EPI>(a, r0, two, h, valid, acc, [&](int j, cx<float> xv[12]) {
+        SIO::load_staged(smem + threadIdx.x + (ST * NS + j * SIO::NSLOT) * B, B, xv);
+    });
 }
 
 // ST = 0: direct loads (k_dslash_mrhs_pair), else the cp.async pipeline of
 // depth ST; MINB = 2 caps the registers at 128 a thread (more warps per SM)
+// epi > 0 (fused CG sums, xpay hops only): see RhsSink
 template <class SIO, class LIO, int ST, int MINB = 1>
-static int launch_pair(const Geom &g, cudaStream_t s, MrhsArgs a, int block, bool xpay) {
+static int launch_pair(const Geom &g, cudaStream_t s, MrhsArgs a, int block, bool xpay, int epi = 0) {
     if constexpr (!std::is_same<typename SIO::real, float>::value) {
         return set_error(PLQCD_ERR_ARG, "dslash_mrhs: the RHS-pair kernel computes in FP32 only");
     } else {
         if (g.Vh >= (1L << 31)) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: lattice too large for 32-bit sites");
+        if (epi && (!xpay || block > 256 || block % 32)) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: fused sums need an xpay hop");
         a.ntiles = (a.nrhs + 1) / 2;
         const long nblk = (g.Vh + block - 1) / block * a.ntiles;
         if (nblk > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: grid too large");
         if constexpr (ST == 0) {
-            if (xpay)
-                k_dslash_mrhs_pair<SIO, LIO, true, MINB><<<(unsigned)nblk, block, 0, s>>>(a);
-            else
-                k_dslash_mrhs_pair<SIO, LIO, false, MINB><<<(unsigned)nblk, block, 0, s>>>(a);
+            auto k = epi == 2 ? k_dslash_mrhs_pair<SIO, LIO, true, MINB, 2>
+                   : epi == 1 ? k_dslash_mrhs_pair<SIO, LIO, true, MINB, 1>
+                   : xpay     ? k_dslash_mrhs_pair<SIO, LIO, true, MINB, 0>
+                              : k_dslash_mrhs_pair<SIO, LIO, false, MINB, 0>;
+            k<<<(unsigned)nblk, block, 0, s>>>(a);
         } else {
             constexpr int NS = LIO::NSLOT + 2 * SIO::NSLOT;
             const size_t smem = (size_t)(ST * NS + (xpay ? 2 * SIO::NSLOT : 0)) * 16 * block;
             if (smem > 227 * 1024) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: %zu bytes of shared memory", smem);
-            auto k = xpay ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB>
-                          : k_dslash_mrhs_pair_pipe<SIO, LIO, ST, false, MINB>;
-            PLQCD_TRY(smem_optin((const void *)k, 227 * 1024));
+            auto k = epi == 2 ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB, 2>
+                   : epi == 1 ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB, 1>
+                   : xpay     ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB, 0>
+                              : k_dslash_mrhs_pair_pipe<SIO, LIO, ST, false, MINB, 0>;
+            // (the fused sums hold static shared memory, so opt in to what this launch needs)
+            PLQCD_TRY(smem_optin((const void *)k, smem));
             k<<<(unsigned)nblk, block, smem, s>>>(a);
         }
         PLQCD_CUDA_TRY(cudaGetLastError());
@@ -548,7 +628,9 @@ static int launch_nr(const Geom &g, cudaStream_t s, MrhsArgs a, int block, bool 
 }
 
 template <int P, int RC>
-static int launch_pr(const Geom &g, cudaStream_t s, const MrhsArgs &a, int nr, int block, bool xpay) {
+static int launch_pr(const Geom &g, cudaStream_t s, const MrhsArgs &a, int nr, int block, bool xpay, int epi) {
+    if (epi && (nr < 2000 || nr >= 3000))
+        return set_error(PLQCD_ERR_ARG, "dslash_mrhs: fused sums exist in the RHS-pair kernels only");
     using S = SpinorIO<P>;
     using L = LinkIO<P, RC>;
     switch (nr) {
@@ -559,9 +641,9 @@ static int launch_pr(const Geom &g, cudaStream_t s, const MrhsArgs &a, int nr, i
             break;
         // 2002: RHS-pair kernel on packed FP32 lanes; 2022 / 2032: its
         // cp.async pipeline of depth 2 / 3
-        case 2002: return launch_pair<S, L, 0>(g, s, a, block, xpay);
-        case 2022: return launch_pair<S, L, 2>(g, s, a, block, xpay);
-        case 2032: return launch_pair<S, L, 3>(g, s, a, block, xpay);
+        case 2002: return launch_pair<S, L, 0>(g, s, a, block, xpay, epi);
+        case 2022: return launch_pair<S, L, 2>(g, s, a, block, xpay, epi);
+        case 2032: return launch_pair<S, L, 3>(g, s, a, block, xpay, epi);
         // 4000 + 100 * ring depth + RHS per block: FP64 link-sharing kernel
         case 4208:
         case 4204:
@@ -577,8 +659,8 @@ static int launch_pr(const Geom &g, cudaStream_t s, const MrhsArgs &a, int nr, i
             }
             break;
         // 2102 / 2122: the same with at most 128 registers a thread
-        case 2102: return launch_pair<S, L, 0, 2>(g, s, a, block, xpay);
-        case 2122: return launch_pair<S, L, 2, 2>(g, s, a, block, xpay);
+        case 2102: return launch_pair<S, L, 0, 2>(g, s, a, block, xpay, epi);
+        case 2122: return launch_pair<S, L, 2, 2>(g, s, a, block, xpay, epi);
         case 1: return launch_nr<S, L, 1>(g, s, a, block, xpay);
         case 2: return launch_nr<S, L, 2>(g, s, a, block, xpay);
         case 4:
@@ -593,15 +675,15 @@ static int launch_pr(const Geom &g, cudaStream_t s, const MrhsArgs &a, int nr, i
 }  // namespace dev
 
 static int mrhs_dispatch(const Geom &g, cudaStream_t s, int prec, int recon, const dev::MrhsArgs &a, int nr,
-                         int block, bool xpay) {
+                         int block, bool xpay, int epi = 0) {
     if (block % 32 || block < 32 || block > 256) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: block %d", block);
     switch (prec * 100 + recon) {
-        case PLQCD_F64 * 100 + 18: return dev::launch_pr<PLQCD_F64, 18>(g, s, a, nr, block, xpay);
-        case PLQCD_F64 * 100 + 12: return dev::launch_pr<PLQCD_F64, 12>(g, s, a, nr, block, xpay);
-        case PLQCD_F32 * 100 + 18: return dev::launch_pr<PLQCD_F32, 18>(g, s, a, nr, block, xpay);
-        case PLQCD_F32 * 100 + 12: return dev::launch_pr<PLQCD_F32, 12>(g, s, a, nr, block, xpay);
-        case PLQCD_F16 * 100 + 12: return dev::launch_pr<PLQCD_F16, 12>(g, s, a, nr, block, xpay);
-        case PLQCD_BF16 * 100 + 12: return dev::launch_pr<PLQCD_BF16, 12>(g, s, a, nr, block, xpay);
+        case PLQCD_F64 * 100 + 18: return dev::launch_pr<PLQCD_F64, 18>(g, s, a, nr, block, xpay, epi);
+        case PLQCD_F64 * 100 + 12: return dev::launch_pr<PLQCD_F64, 12>(g, s, a, nr, block, xpay, epi);
+        case PLQCD_F32 * 100 + 18: return dev::launch_pr<PLQCD_F32, 18>(g, s, a, nr, block, xpay, epi);
+        case PLQCD_F32 * 100 + 12: return dev::launch_pr<PLQCD_F32, 12>(g, s, a, nr, block, xpay, epi);
+        case PLQCD_F16 * 100 + 12: return dev::launch_pr<PLQCD_F16, 12>(g, s, a, nr, block, xpay, epi);
+        case PLQCD_BF16 * 100 + 12: return dev::launch_pr<PLQCD_BF16, 12>(g, s, a, nr, block, xpay, epi);
         default: return set_error(PLQCD_ERR_ARG, "dslash_mrhs: unsupported format %d/%d", prec, recon);
     }
 }
@@ -627,13 +709,13 @@ bool dslash_mrhs_tuned(const Geom &g, int prec, int recon, int nrhs, bool xpay) 
 }
 
 // out (nrhs fields) = a_up/a_low * H in + b * x; tuned over RHS tile and block
-int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
-                       const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b) {
+static int mrhs_args(const Geom &g, const void *gauge, int prec, void *out, const void *in, int nrhs,
+                     int out_parity, unsigned flags, double a, const void *x, double b, dev::MrhsArgs &m) {
     if (nrhs < 1) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: nrhs must be >= 1");
     PLQCD_TRY(check_field_ptr(out, "dslash_mrhs"));
     PLQCD_TRY(check_field_ptr(in, "dslash_mrhs"));
     if (x) PLQCD_TRY(check_field_ptr(x, "dslash_mrhs"));
-    dev::MrhsArgs m{};
+    m = dev::MrhsArgs{};
     m.gauge = gauge;
     m.in = static_cast<const char *>(in);
     m.out = static_cast<char *>(out);
@@ -651,6 +733,54 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
     m.a_low = (flags & PLQCD_DSLASH_G5_OUT) ? -a : a;
     m.b = b;
     m.g5_in = (flags & PLQCD_DSLASH_G5_IN) ? -1.0 : 1.0;
+    return PLQCD_OK;
+}
+
+// the RHS-pair configuration that runs this xpay hop with fused sums: the
+// environment's, else the tuned one (false when it is another kernel)
+static bool mrhs_sink_config(const Geom &g, int prec, int recon, int nrhs, TuneResult *t) {
+    const char *ev = getenv("PLQCD_MRHS_VARIANT");
+    if (ev && *ev) {
+        const char *eb = getenv("PLQCD_MRHS_BLOCK");
+        t->variant = atoi(ev);
+        t->block = (eb && *eb) ? atoi(eb) : 128;
+    } else {
+        char key[256];
+        mrhs_key(key, sizeof key, g, prec, recon, nrhs, true);
+        if (!tune_lookup(key, t)) return false;
+    }
+    const int v = t->variant;
+    return v == 2002 || v == 2022 || v == 2032 || v == 2102 || v == 2122;
+}
+
+bool dslash_mrhs_sink_ok(const Geom &g, int prec, int recon, int nrhs) {
+    TuneResult t;
+    return prec != PLQCD_F64 && nrhs >= 2 && mrhs_sink_config(g, prec, recon, nrhs, &t);
+}
+
+int launch_dslash_mrhs_sink(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
+                            const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x,
+                            double b, int epi, const RhsSink &sink) {
+    TuneResult t;
+    if (!x || (epi != 1 && epi != 2) || prec == PLQCD_F64 || !mrhs_sink_config(g, prec, recon, nrhs, &t))
+        return set_error(PLQCD_ERR_ARG, "dslash_mrhs: no RHS-pair configuration for fused sums");
+    dev::MrhsArgs m;
+    PLQCD_TRY(mrhs_args(g, gauge, prec, out, in, nrhs, out_parity, flags, a, x, b, m));
+    m.sink = sink;
+    PLQCD_TRY(mrhs_dispatch(g, s, prec, recon, m, t.variant, t.block, true, epi));
+    const int nsb = (int)((g.Vh + t.block - 1) / t.block);
+    if (epi == 1)
+        dev::k_sink_finish<1><<<nrhs, 1024, 0, s>>>(sink, nsb);
+    else
+        dev::k_sink_finish<2><<<nrhs, 1024, 0, s>>>(sink, nsb);
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
+                       const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b) {
+    dev::MrhsArgs m;
+    PLQCD_TRY(mrhs_args(g, gauge, prec, out, in, nrhs, out_parity, flags, a, x, b, m));
     const bool xpay = x != nullptr;
     char key[256];
     mrhs_key(key, sizeof key, g, prec, recon, nrhs, xpay);

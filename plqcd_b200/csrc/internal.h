@@ -146,6 +146,26 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
 // true when launch_dslash_mrhs of this configuration would not tune
 bool dslash_mrhs_tuned(const Geom &g, int prec, int recon, int nrhs, bool xpay);
 
+// CG dot products fused into the epilogue of a multi-RHS xpay hop (the
+// RHS-pair kernels): per-RHS FP64 sums, per-block partials summed in a fixed
+// order by a one-block-per-RHS kernel after the hop, applied to the solver's
+// scalars of every active RHS.
+//   epi 1: out = t as usual; pAp = |t|^2, alpha = rr / pAp
+//   epi 2: out = Ap is not stored; r -= alpha Ap in place (rvec);
+//          rr_old = rr, rr = |r|^2, beta = rr / rr_old
+struct RhsSink {
+    double *partials;    // nrhs * ceil(Vh / 32) doubles
+    double *rr, *rr_old, *pAp, *alpha, *beta;
+    const int *active;
+    char *rvec;
+};
+// the tuned xpay configuration of this multi-RHS hop is an RHS-pair kernel,
+// so launch_dslash_mrhs_sink can run it
+bool dslash_mrhs_sink_ok(const Geom &g, int prec, int recon, int nrhs);
+int launch_dslash_mrhs_sink(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
+                            const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x,
+                            double b, int epi, const RhsSink &sink);
+
 // dynamic shared-memory opt-in of kernel `func` on the current device, set
 // once per (kernel, device) to at least `bytes` (utils.cpp)
 int smem_optin(const void *func, size_t bytes);

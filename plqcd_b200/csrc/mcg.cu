@@ -400,6 +400,10 @@ struct Item {
     char *rs = nullptr, *p = nullptr, *Ap = nullptr, *t = nullptr, *tmps = nullptr, *xs = nullptr;
     McgState st{};
     void *mem = nullptr;
+    // the sloppy hops that produce t and Ap carry |t|^2 and r -= alpha Ap,
+    // |r|^2 in their epilogues (RHS-pair kernels; see RhsSink)
+    bool fused = false;
+    double *hop_partials = nullptr;  // nrhs * ceil(Vh / 32)
 };
 
 struct Batch {
@@ -419,6 +423,15 @@ struct Batch {
         unsigned fi = dagger ? PLQCD_DSLASH_G5_IN : 0u, fo = dagger ? PLQCD_DSLASH_G5_OUT : 0u;
         PLQCD_TRY(hop(it, gf, tmp_o, in, PLQCD_ODD, fi));
         return hop(it, gf, out, tmp_o, PLQCD_EVEN, fo, in, -kappa * kappa, 1.0);
+    }
+    // mhat with the CG sums of epi (1: |out|^2 -> pAp, alpha; 2: r -= alpha
+    // out, |r|^2 -> rr, beta, out not stored) in the second hop's epilogue
+    int mhat_fused(Item &it, const plqcd_gauge *gf, void *out, const void *in, void *tmp_o, bool dagger, int epi) {
+        unsigned fi = dagger ? PLQCD_DSLASH_G5_IN : 0u, fo = dagger ? PLQCD_DSLASH_G5_OUT : 0u;
+        PLQCD_TRY(hop(it, gf, tmp_o, in, PLQCD_ODD, fi));
+        RhsSink k{it.hop_partials, it.st.rr, it.st.rr_old, it.st.pAp, it.st.alpha, it.st.beta, it.st.active, it.rs};
+        return launch_dslash_mrhs_sink(*it.g, s, gf->data, gf->prec, gf->recon, out, tmp_o, it.in.nrhs, PLQCD_EVEN,
+                                       fo, -kappa * kappa, in, 1.0, epi, k);
     }
     int norm2(Item &it, const void *x, int prec, MOp op, bool only_active) {
         dim3 grid(it.st.nb, it.in.nrhs);
@@ -485,6 +498,11 @@ struct Batch {
     int part_sloppy() {
         for (Item &it : items) {
             const plqcd_gauge *gs = it.in.g_sloppy ? it.in.g_sloppy : it.in.g64;
+            if (it.fused) {
+                PLQCD_TRY(mhat_fused(it, gs, it.t, it.p, it.tmps, false, 1));   // t, pAp, alpha
+                PLQCD_TRY(mhat_fused(it, gs, it.Ap, it.t, it.tmps, true, 2));   // r, rr, beta
+                continue;
+            }
             PLQCD_TRY(mhat(it, gs, it.t, it.p, it.tmps, false));
             PLQCD_TRY(norm2(it, it.t, it.ps, M_ALPHA, true));
             PLQCD_TRY(mhat(it, gs, it.Ap, it.t, it.tmps, true));
@@ -565,8 +583,10 @@ int alloc_item(Batch &B, Item &it, bool own_ws) {
     it.st.nrhs = n;
     it.st.nb = red_blocks(Vh, n);
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t nsb = (size_t)(Vh + 31) / 32;  // site blocks of a fused hop, at most
     const size_t need = 4 * al(it.fb64 * n) + 5 * al(it.fbs * n) + al(it.fbx * n) + 10 * al(sizeof(double) * n) +
-                        3 * al(sizeof(int) * n) + al(sizeof(double) * n * it.st.nb) + al(sizeof(unsigned) * n);
+                        3 * al(sizeof(int) * n) + al(sizeof(double) * n * it.st.nb) + al(sizeof(unsigned) * n) +
+                        al(sizeof(double) * n * nsb);
     void *ws = nullptr;
     if (own_ws) {
         if (cudaMalloc(&it.mem, need) != cudaSuccess) {
@@ -601,6 +621,7 @@ int alloc_item(Batch &B, Item &it, bool own_ws) {
     it.st.fresh = reinterpret_cast<int *>(take(sizeof(int) * n));
     it.st.partials = reinterpret_cast<double *>(take(sizeof(double) * n * it.st.nb));
     it.st.counters = reinterpret_cast<unsigned *>(take(sizeof(unsigned) * n));
+    it.hop_partials = reinterpret_cast<double *>(take(sizeof(double) * n * nsb));
     cudaStream_t s = B.s;
     PLQCD_CUDA_TRY(cudaMemsetAsync(it.st.counters, 0, sizeof(unsigned) * n, s));
     PLQCD_CUDA_TRY(cudaMemsetAsync(it.st.conv_iter, 0xff, sizeof(int) * n, s));
@@ -621,12 +642,27 @@ int tune_item(Batch &B, Item &it) {
                       dslash_mrhs_tuned(*it.g, gs->prec, gs->recon, n, true) &&
                       dslash_mrhs_tuned(*it.g, PLQCD_F64, in.g64->recon, n, false) &&
                       dslash_mrhs_tuned(*it.g, PLQCD_F64, in.g64->recon, n, true);
-    if (done) return PLQCD_OK;
-    cudaStream_t s = B.s;
-    PLQCD_CUDA_TRY(cudaMemsetAsync(it.p, 0, it.fbs * n, s));
-    PLQCD_CUDA_TRY(cudaMemsetAsync(it.r64, 0, it.fb64 * n, s));
-    PLQCD_TRY(B.mhat(it, gs, it.t, it.p, it.tmps, false));
-    return B.mhat(it, in.g64, it.t64, it.r64, it.tmp64, false);
+    if (!done) {
+        cudaStream_t s = B.s;
+        PLQCD_CUDA_TRY(cudaMemsetAsync(it.p, 0, it.fbs * n, s));
+        PLQCD_CUDA_TRY(cudaMemsetAsync(it.r64, 0, it.fb64 * n, s));
+        PLQCD_TRY(B.mhat(it, gs, it.t, it.p, it.tmps, false));
+        PLQCD_TRY(B.mhat(it, in.g64, it.t64, it.r64, it.tmp64, false));
+    }
+    // fused CG sums when the tuned sloppy xpay hop is an RHS-pair kernel
+    // (PLQCD_MCG_FUSED=0: separate passes)
+    const char *e = getenv("PLQCD_MCG_FUSED");
+    it.fused = B.mixed && !(e && e[0] == '0') && dslash_mrhs_sink_ok(*it.g, gs->prec, gs->recon, n);
+    if (it.fused) {
+        // load the fused kernels and set their shared memory before any
+        // capture (on zeroed fields; the solve's start overwrites every
+        // scalar they set)
+        PLQCD_CUDA_TRY(cudaMemsetAsync(it.p, 0, it.fbs * n, B.s));
+        PLQCD_CUDA_TRY(cudaMemsetAsync(it.rs, 0, it.fbs * n, B.s));
+        PLQCD_TRY(B.mhat_fused(it, gs, it.t, it.p, it.tmps, false, 1));
+        PLQCD_TRY(B.mhat_fused(it, gs, it.Ap, it.t, it.tmps, true, 2));
+    }
+    return PLQCD_OK;
 }
 
 // start of the solve: b' = b_e + kappa H_eo b_o, |b'|^2, x = 0, the start

@@ -79,3 +79,40 @@ def test_batch_rejects_mismatched_sloppy_gauge(cuda):
     it = _lattice_item((4, 4, 4, 8), 1, 9, P.F16)
     info, _ = P.invert_cg_batch([it], P.cg_param(kappa=KAPPA, sloppy_prec=P.F32), True, raise_on_error=False)
     assert "sloppy gauge does not match" in P.last_error()
+
+
+@pytest.mark.parametrize("variant", [2102, 2022])
+def test_batch_fused_sums_match_separate_passes(cuda, monkeypatch, tmp_path, variant):
+    """With an RHS-pair kernel as the sloppy xpay hop, the batched solver
+    moves |t|^2 and r -= alpha Ap, |r|^2 into the hops' epilogues. The solves
+    (5 RHS: a partial RHS pair; Vh = 96: a partial site block) agree with the
+    separate passes (PLQCD_MCG_FUSED=0) and reach the FP64 residual."""
+    import json
+    prm = P.cg_param(kappa=KAPPA, tol=1e-10, sloppy_prec=P.F16)
+    items = [_lattice_item((8, 8, 8, 16), 5, 11, P.F16), _lattice_item((4, 6, 4, 8), 2, 13, P.F16)]
+    P.invert_cg_batch(items, P.cg_param(kappa=KAPPA, tol=1e-10, sloppy_prec=P.F16, max_iter=2), True,
+                      raise_on_error=False)  # tunes every configuration
+    path = str(tmp_path / "tune.json")
+    assert P.lib().plqcd_tune_save(path.encode()) == 0
+    lines = []
+    for line in open(path):
+        e = json.loads(line)
+        if f"dslash_mrhs|p{P.F16}|r12|xpay|" in e["key"]:
+            e["variant"], e["block"] = variant, 64
+        lines.append(json.dumps(e))
+    open(path, "w").write("\n".join(lines) + "\n")
+    P.lib().plqcd_tune_clear()
+    assert P.lib().plqcd_tune_load(path.encode()) == 0
+    try:
+        sols = {}
+        for fused in ("1", "0"):
+            monkeypatch.setenv("PLQCD_MCG_FUSED", fused)
+            info, res = P.invert_cg_batch(items, prm, True)
+            assert info.converged and info.max_schur_residual <= 1e-10 and max(res) < 1e-9
+            sols[fused] = (info.iterations, [_host_field(it, it["x_even"], it["x_odd"], r)
+                                             for it in items for r in range(it["nrhs"])])
+        assert abs(sols["1"][0] - sols["0"][0]) <= 1
+        for a, b in zip(sols["1"][1], sols["0"][1]):
+            assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-8
+    finally:
+        P.lib().plqcd_tune_clear()
