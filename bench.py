@@ -712,7 +712,8 @@ def run_mrhs(torch, P, lat, g64, args, nrhs=8):
     16-bit ones the tensor-core kernel (3001), are also timed forced (keys
     variant/block), beside the tuner's choice."""
     res = {"nrhs": nrhs}
-    for name, prec, recon, sb, lb in (("f64_18", P.F64, 18, 192, 144), ("f32_12", P.F32, 12, 96, 48),
+    for name, prec, recon, sb, lb in (("f64_18", P.F64, 18, 192, 144), ("f64_12", P.F64, 12, 192, 96),
+                                      ("f32_12", P.F32, 12, 96, 48),
                                       ("f16_12", P.F16, 12, 52, 24), ("bf16_12", P.BF16, 12, 52, 24)):
         if args.mrhs_formats and name not in args.mrhs_formats.split(","):
             continue
@@ -735,7 +736,7 @@ def run_mrhs(torch, P, lat, g64, args, nrhs=8):
         res[name] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)
         cfg = tuned_config(P, f"dslash_mrhs|p{prec}|r{recon}|plain|n{nrhs}|{lat.dims[0]}x")
         res[name]["tuned_variant"] = cfg[0] if cfg else None
-        if prec == P.F64:
+        if (prec, recon) == (P.F64, 18):
             forced = {}
             for v, blk in ((4208, 256), (4204, 128), (4308, 256), (4304, 128), (100, 128), (102, 64), (2, 128),
                            (1022, 64)):

@@ -109,68 +109,6 @@ __global__ void __launch_bounds__(kBlasBlock) k_norm2(const void *x, long Vh, Re
     reduce_finish(acc, r, op);
 }
 
-// x_s (XP) += alpha p ; r_s (P) -= alpha Ap ; |r_s|^2
-template <int P, int XP>
-__global__ void __launch_bounds__(kBlasBlock) k_cg_update(void *xs, void *rs, const void *p, const void *Ap, long Vh,
-                                                          RedScratch r) {
-    using R = typename SpinorIO<P>::real;
-    using RX = typename SpinorIO<XP>::real;
-    const double alpha = r.state->alpha;
-    double acc = 0;
-    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
-        cx<R> pv[12], av[12], rv[12];
-        cx<RX> xv[12];
-        SpinorIO<P>::load(p, Vh, h, pv);
-        SpinorIO<P>::load(Ap, Vh, h, av);
-        SpinorIO<P>::load(rs, Vh, h, rv);
-        SpinorIO<XP>::load(xs, Vh, h, xv);
-        const R a = (R)alpha;
-        const RX ax = (RX)alpha;
-#pragma unroll
-        for (int k = 0; k < 12; k++) {
-            xv[k] = {fma(ax, (RX)pv[k].re, xv[k].re), fma(ax, (RX)pv[k].im, xv[k].im)};
-            rv[k] = {fma(-a, av[k].re, rv[k].re), fma(-a, av[k].im, rv[k].im)};
-        }
-        SpinorIO<XP>::store(xs, Vh, h, xv);
-        SpinorIO<P>::store(rs, Vh, h, rv);
-        acc += norm2_site(rv);
-    }
-    reduce_finish(acc, r, RED_RR);
-}
-
-// p = r + beta p
-template <int P>
-__global__ void __launch_bounds__(kBlasBlock) k_cg_p(void *p, const void *rs, long Vh, const CgState *st) {
-    using R = typename SpinorIO<P>::real;
-    const R beta = (R)st->beta;
-    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
-        cx<R> pv[12], rv[12];
-        SpinorIO<P>::load(p, Vh, h, pv);
-        SpinorIO<P>::load(rs, Vh, h, rv);
-#pragma unroll
-        for (int k = 0; k < 12; k++) pv[k] = {fma(beta, pv[k].re, rv[k].re), fma(beta, pv[k].im, rv[k].im)};
-        SpinorIO<P>::store(p, Vh, h, pv);
-    }
-}
-
-template <int XP>
-__global__ void __launch_bounds__(kBlasBlock) k_accum_zero(void *x64, void *xs, long Vh) {
-    using RX = typename SpinorIO<XP>::real;
-    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
-        cx<double> xv[12];
-        cx<RX> sv[12], z[12];
-        SpinorIO<PLQCD_F64>::load(x64, Vh, h, xv);
-        SpinorIO<XP>::load(xs, Vh, h, sv);
-#pragma unroll
-        for (int k = 0; k < 12; k++) {
-            xv[k] = {xv[k].re + (double)sv[k].re, xv[k].im + (double)sv[k].im};
-            z[k] = {RX(0), RX(0)};
-        }
-        SpinorIO<PLQCD_F64>::store(x64, Vh, h, xv);
-        SpinorIO<XP>::store(xs, Vh, h, z);
-    }
-}
-
 __global__ void __launch_bounds__(kBlasBlock) k_sub_norm2(void *out, const void *a, const void *b, long Vh,
                                                           RedScratch r, RedOp op) {
     double acc = 0;
@@ -181,6 +119,108 @@ __global__ void __launch_bounds__(kBlasBlock) k_sub_norm2(void *out, const void 
 #pragma unroll
         for (int k = 0; k < 12; k++) av[k] = csub(av[k], bv[k]);
         SpinorIO<PLQCD_F64>::store(out, Vh, h, av);
+        acc += norm2_site(av);
+    }
+    reduce_finish(acc, r, op);
+}
+
+// r_s -= alpha Ap ; |r_s|^2 (the solution update of the iteration is in k_cg_p_x)
+template <int P>
+__global__ void __launch_bounds__(kBlasBlock) k_cg_update_r(void *rs, const void *Ap, long Vh, RedScratch r) {
+    using R = typename SpinorIO<P>::real;
+    const R a = (R)r.state->alpha;
+    double acc = 0;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<R> av[12], rv[12];
+        SpinorIO<P>::load(Ap, Vh, h, av);
+        SpinorIO<P>::load(rs, Vh, h, rv);
+#pragma unroll
+        for (int k = 0; k < 12; k++) rv[k] = {fma(-a, av[k].re, rv[k].re), fma(-a, av[k].im, rv[k].im)};
+        SpinorIO<P>::store(rs, Vh, h, rv);
+        acc += norm2_site(rv);
+    }
+    reduce_finish(acc, r, RED_RR);
+}
+
+// XMODE 1: x_s = alpha p (x_s counts as zero); 2: x_s += alpha p; 0: no x
+// update (a reliable update folded alpha p into x). Then p = r + beta p.
+template <int P, int XP, int XMODE>
+__global__ void __launch_bounds__(kBlasBlock) k_cg_p_x(void *p, const void *rs, void *xs, long Vh, const CgState *st) {
+    using R = typename SpinorIO<P>::real;
+    using RX = typename SpinorIO<XP>::real;
+    const R beta = (R)st->beta;
+    const RX ax = (RX)st->alpha;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<R> pv[12], rv[12];
+        SpinorIO<P>::load(p, Vh, h, pv);
+        SpinorIO<P>::load(rs, Vh, h, rv);
+        if (XMODE) {
+            cx<RX> xv[12];
+            if (XMODE == 1) {
+#pragma unroll
+                for (int k = 0; k < 12; k++) xv[k] = {RX(0), RX(0)};
+            } else {
+                SpinorIO<XP>::load(xs, Vh, h, xv);
+            }
+#pragma unroll
+            for (int k = 0; k < 12; k++)
+                xv[k] = {fma(ax, (RX)pv[k].re, xv[k].re), fma(ax, (RX)pv[k].im, xv[k].im)};
+            SpinorIO<XP>::store(xs, Vh, h, xv);
+        }
+#pragma unroll
+        for (int k = 0; k < 12; k++) pv[k] = {fma(beta, pv[k].re, rv[k].re), fma(beta, pv[k].im, rv[k].im)};
+        SpinorIO<P>::store(p, Vh, h, pv);
+    }
+}
+
+// x64 += x_s (FRESH: x_s counts as zero) [+ alpha p when P >= 0, the
+// current iteration's update, computed as k_cg_p_x would]
+template <int P, int XP, bool FRESH>
+__global__ void __launch_bounds__(kBlasBlock) k_accum(void *x64, const void *xs, const void *p, long Vh,
+                                                      const CgState *st) {
+    using RX = typename SpinorIO<XP>::real;
+    const RX ax = (RX)st->alpha;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<double> xv[12];
+        cx<RX> sv[12];
+        SpinorIO<PLQCD_F64>::load(x64, Vh, h, xv);
+        if (FRESH) {
+#pragma unroll
+            for (int k = 0; k < 12; k++) sv[k] = {RX(0), RX(0)};
+        } else {
+            SpinorIO<XP>::load(xs, Vh, h, sv);
+        }
+        if constexpr (P >= 0) {
+            using R = typename SpinorIO<P>::real;
+            cx<R> pv[12];
+            SpinorIO<P>::load(p, Vh, h, pv);
+#pragma unroll
+            for (int k = 0; k < 12; k++)
+                sv[k] = {fma(ax, (RX)pv[k].re, sv[k].re), fma(ax, (RX)pv[k].im, sv[k].im)};
+        }
+#pragma unroll
+        for (int k = 0; k < 12; k++) xv[k] = {xv[k].re + (double)sv[k].re, xv[k].im + (double)sv[k].im};
+        SpinorIO<PLQCD_F64>::store(x64, Vh, h, xv);
+    }
+}
+
+// z = a - b (F64) ; |z|^2 -> op ; out = z in format SP (z itself is not stored)
+template <int SP>
+__global__ void __launch_bounds__(kBlasBlock) k_sub_norm2_to(void *out, const void *a, const void *b, long Vh,
+                                                             RedScratch r, RedOp op) {
+    using RS = typename SpinorIO<SP>::real;
+    double acc = 0;
+    for (long h = (long)blockIdx.x * blockDim.x + threadIdx.x; h < Vh; h += (long)gridDim.x * blockDim.x) {
+        cx<double> av[12], bv[12];
+        SpinorIO<PLQCD_F64>::load(a, Vh, h, av);
+        SpinorIO<PLQCD_F64>::load(b, Vh, h, bv);
+        cx<RS> d[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) {
+            av[k] = csub(av[k], bv[k]);
+            d[k] = {(RS)av[k].re, (RS)av[k].im};
+        }
+        SpinorIO<SP>::store(out, Vh, h, d);
         acc += norm2_site(av);
     }
     reduce_finish(acc, r, op);
@@ -217,48 +257,83 @@ int blas_norm2(const Geom &g, cudaStream_t s, const void *x, int prec, const Red
     return PLQCD_OK;
 }
 
-int blas_cg_update(const Geom &g, cudaStream_t s, void *xs, int xprec, void *rs, const void *p, const void *Ap,
-                   int prec, const RedScratch &r) {
-    const int nb = dev::blas_grid(g.Vh);
-    if (xprec == PLQCD_F64) {
-#define F(P) dev::k_cg_update<P, PLQCD_F64><<<nb, kBlasBlock, 0, s>>>(xs, rs, p, Ap, g.Vh, r)
-        BLAS_PREC_SWITCH(prec, F)
-#undef F
-    } else if (xprec == PLQCD_F32) {
-#define F(P) dev::k_cg_update<P, PLQCD_F32><<<nb, kBlasBlock, 0, s>>>(xs, rs, p, Ap, g.Vh, r)
-        BLAS_PREC_SWITCH(prec, F)
-#undef F
-    } else {
-        return set_error(PLQCD_ERR_ARG, "blas_cg_update: solution accumulator must be F64 or F32");
-    }
+int blas_sub_norm2(const Geom &g, cudaStream_t s, void *out, const void *a, const void *b, const RedScratch &r,
+                   RedOp op) {
+    dev::k_sub_norm2<<<dev::blas_grid(g.Vh), kBlasBlock, 0, s>>>(out, a, b, g.Vh, r, op);
     PLQCD_CUDA_TRY(cudaGetLastError());
     return PLQCD_OK;
 }
 
-int blas_cg_p(const Geom &g, cudaStream_t s, void *p, const void *rs, int prec, const RedScratch &r) {
+int blas_cg_update_r(const Geom &g, cudaStream_t s, void *rs, const void *Ap, int prec, const RedScratch &r) {
     const int nb = dev::blas_grid(g.Vh);
-#define F(P) dev::k_cg_p<P><<<nb, kBlasBlock, 0, s>>>(p, rs, g.Vh, r.state)
+#define F(P) dev::k_cg_update_r<P><<<nb, kBlasBlock, 0, s>>>(rs, Ap, g.Vh, r)
     BLAS_PREC_SWITCH(prec, F)
 #undef F
     PLQCD_CUDA_TRY(cudaGetLastError());
     return PLQCD_OK;
 }
 
-int blas_accum_zero(const Geom &g, cudaStream_t s, void *x64, void *xs, int xprec) {
+int blas_cg_p_x(const Geom &g, cudaStream_t s, void *p, const void *rs, int prec, void *xs, int xprec, int xmode,
+                const RedScratch &r) {
     const int nb = dev::blas_grid(g.Vh);
-    if (xprec == PLQCD_F64)
-        dev::k_accum_zero<PLQCD_F64><<<nb, kBlasBlock, 0, s>>>(x64, xs, g.Vh);
-    else if (xprec == PLQCD_F32)
-        dev::k_accum_zero<PLQCD_F32><<<nb, kBlasBlock, 0, s>>>(x64, xs, g.Vh);
-    else
-        return set_error(PLQCD_ERR_ARG, "blas_accum_zero: accumulator must be F64 or F32");
+    if (xprec != PLQCD_F64 && xprec != PLQCD_F32)
+        return set_error(PLQCD_ERR_ARG, "blas_cg_p_x: solution accumulator must be F64 or F32");
+#define G(P, XP)                                                                                        \
+    switch (xmode) {                                                                                    \
+        case 0: dev::k_cg_p_x<P, XP, 0><<<nb, kBlasBlock, 0, s>>>(p, rs, xs, g.Vh, r.state); break;     \
+        case 1: dev::k_cg_p_x<P, XP, 1><<<nb, kBlasBlock, 0, s>>>(p, rs, xs, g.Vh, r.state); break;     \
+        default: dev::k_cg_p_x<P, XP, 2><<<nb, kBlasBlock, 0, s>>>(p, rs, xs, g.Vh, r.state); break;   \
+    }
+#define F(P)                         \
+    if (xprec == PLQCD_F64) {        \
+        G(P, PLQCD_F64)              \
+    } else {                         \
+        G(P, PLQCD_F32)              \
+    }
+    BLAS_PREC_SWITCH(prec, F)
+#undef F
+#undef G
     PLQCD_CUDA_TRY(cudaGetLastError());
     return PLQCD_OK;
 }
 
-int blas_sub_norm2(const Geom &g, cudaStream_t s, void *out, const void *a, const void *b, const RedScratch &r,
-                   RedOp op) {
-    dev::k_sub_norm2<<<dev::blas_grid(g.Vh), kBlasBlock, 0, s>>>(out, a, b, g.Vh, r, op);
+int blas_accum(const Geom &g, cudaStream_t s, void *x64, const void *xs, int xprec, bool fresh, const void *p,
+               int prec, const RedScratch &r) {
+    const int nb = dev::blas_grid(g.Vh);
+    if (xprec != PLQCD_F64 && xprec != PLQCD_F32)
+        return set_error(PLQCD_ERR_ARG, "blas_accum: accumulator must be F64 or F32");
+    if (!p) {
+        if (fresh) return PLQCD_OK;  // x_s is zero
+        if (xprec == PLQCD_F64)
+            dev::k_accum<-1, PLQCD_F64, false><<<nb, kBlasBlock, 0, s>>>(x64, xs, nullptr, g.Vh, r.state);
+        else
+            dev::k_accum<-1, PLQCD_F32, false><<<nb, kBlasBlock, 0, s>>>(x64, xs, nullptr, g.Vh, r.state);
+    } else {
+#define G(P, XP)                                                                                   \
+    if (fresh)                                                                                     \
+        dev::k_accum<P, XP, true><<<nb, kBlasBlock, 0, s>>>(x64, xs, p, g.Vh, r.state);            \
+    else                                                                                           \
+        dev::k_accum<P, XP, false><<<nb, kBlasBlock, 0, s>>>(x64, xs, p, g.Vh, r.state);
+#define F(P)                   \
+    if (xprec == PLQCD_F64) {  \
+        G(P, PLQCD_F64)        \
+    } else {                   \
+        G(P, PLQCD_F32)        \
+    }
+        BLAS_PREC_SWITCH(prec, F)
+#undef F
+#undef G
+    }
+    PLQCD_CUDA_TRY(cudaGetLastError());
+    return PLQCD_OK;
+}
+
+int blas_sub_norm2_to(const Geom &g, cudaStream_t s, void *out, int prec, const void *a, const void *b,
+                      const RedScratch &r, RedOp op) {
+    const int nb = dev::blas_grid(g.Vh);
+#define F(P) dev::k_sub_norm2_to<P><<<nb, kBlasBlock, 0, s>>>(out, a, b, g.Vh, r, op)
+    BLAS_PREC_SWITCH(prec, F)
+#undef F
     PLQCD_CUDA_TRY(cudaGetLastError());
     return PLQCD_OK;
 }

@@ -45,13 +45,6 @@ enum RedOp : int {
 
 // sum |x|^2 (FP64 accumulation); finalised by `op`
 int blas_norm2(const Geom &g, cudaStream_t s, const void *x, int prec, const RedScratch &r, RedOp op);
-// x_s += alpha p; r_s -= alpha Ap; sum |r_s|^2 -> RED_RR
-int blas_cg_update(const Geom &g, cudaStream_t s, void *xs, int xprec, void *rs, const void *p, const void *Ap,
-                   int prec, const RedScratch &r);
-// p = r + beta p
-int blas_cg_p(const Geom &g, cudaStream_t s, void *p, const void *rs, int prec, const RedScratch &r);
-// x64 += xs; xs = 0
-int blas_accum_zero(const Geom &g, cudaStream_t s, void *x64, void *xs, int xprec);
 // out64 = a64 - b64; sum |out|^2 -> op
 int blas_sub_norm2(const Geom &g, cudaStream_t s, void *out, const void *a, const void *b, const RedScratch &r,
                    RedOp op);
@@ -63,5 +56,16 @@ int launch_norm2_multi(const Geom &g, cudaStream_t s, const void *fields, int pr
                        unsigned *counters, double *out);
 // y = a x + b y (F64 fields)
 int blas_axpby64(const Geom &g, cudaStream_t s, double a, const void *x, double b, void *y);
+// r_s -= alpha Ap, |r_s|^2 -> RED_RR (no solution update)
+int blas_cg_update_r(const Geom &g, cudaStream_t s, void *rs, const void *Ap, int prec, const RedScratch &r);
+// xmode 1: x_s = alpha p, 2: x_s += alpha p, 0: no x update; then p = r + beta p
+int blas_cg_p_x(const Geom &g, cudaStream_t s, void *p, const void *rs, int prec, void *xs, int xprec, int xmode,
+                const RedScratch &r);
+// x64 += x_s (fresh: x_s counts as zero) [+ alpha p when p != null, with p in prec]
+int blas_accum(const Geom &g, cudaStream_t s, void *x64, const void *xs, int xprec, bool fresh, const void *p,
+               int prec, const RedScratch &r);
+// out (prec) = a - b, |a - b|^2 -> op (a, b F64)
+int blas_sub_norm2_to(const Geom &g, cudaStream_t s, void *out, int prec, const void *a, const void *b,
+                      const RedScratch &r, RedOp op);
 
 }  // namespace plqcd

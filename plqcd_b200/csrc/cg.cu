@@ -167,9 +167,10 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
             inf.converged = 1;
             break;
         }
-        // x = 0, r = p = rhs
+        // x = 0, r = p = rhs. The sloppy solution x_s is not cleared: while
+        // `fresh` it counts as zero, and its next update writes it unread
         cudaMemsetAsync(x_even, 0, b64, s);
-        cudaMemsetAsync(xs, 0, bx, s);
+        bool fresh = true;
         if (mixed) {
             // the sloppy recursion starts from rhs in sloppy precision, so
             // the sloppy operator computes it; convergence is decided on the
@@ -203,7 +204,10 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
             if ((rc = op.mhat(gs, t, p, tmps, false))) break;
             if ((rc = blas_norm2(g, s, t, ps, red, RED_ALPHA))) break;
             if ((rc = op.mhat(gs, Ap, t, tmps, true))) break;
-            if ((rc = blas_cg_update(g, s, xs, xprec, rs, p, Ap, ps, red))) break;
+            // r -= alpha Ap ; |r|^2. The solution update x_s += alpha p of
+            // this iteration runs in the p update below (which reads p
+            // anyway), or in the fold of a reliable update
+            if ((rc = blas_cg_update_r(g, s, rs, Ap, ps, red))) break;
             inf.sloppy_hops += 4;
             inf.iterations = it;
             if ((rc = read_state())) break;
@@ -214,10 +218,17 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
             }
             const bool reliable = (mixed && rr < delta2 * maxrr) || rr <= target || it - last_reliable >= max_sloppy_run;
             if (reliable) {
-                // defect correction: solution and Schur residual in FP64
-                if ((rc = blas_accum_zero(g, s, x_even, xs, xprec))) break;
+                // defect correction: x += x_s + alpha p, then the Schur
+                // residual b' - Mhat x in FP64 (for the mixed solve written
+                // only in the sloppy format: the restart needs nothing more)
+                if ((rc = blas_accum(g, s, x_even, xs, xprec, fresh, p, ps, red))) break;
+                fresh = true;
                 if ((rc = op.mhat(g64, t64, x_even, tmp64, false))) break;
-                if ((rc = blas_sub_norm2(g, s, r64, bprime, t64, red, RED_SR2))) break;
+                if (mixed)
+                    rc = blas_sub_norm2_to(g, s, t, ps, bprime, t64, red, RED_SR2);
+                else
+                    rc = blas_sub_norm2(g, s, r64, bprime, t64, red, RED_SR2);
+                if (rc) break;
                 inf.f64_hops += 2;
                 inf.reliable_updates++;
                 last_reliable = it;
@@ -233,7 +244,6 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
                 // FP64 residual above decides convergence; the restart
                 // direction only needs the sloppy operator's accuracy
                 if (mixed) {
-                    if ((rc = launch_spinor_convert(g, s, t, ps, r64, PLQCD_F64))) break;
                     if ((rc = op.mhat(gs, rs, t, tmps, true))) break;
                     if ((rc = blas_norm2(g, s, rs, ps, red, RED_RR_TRUE))) break;
                     inf.sloppy_hops += 2;
@@ -249,12 +259,13 @@ extern "C" int plqcd_invert_cg(plqcd_lattice *lat, const plqcd_gauge *g64, const
             } else {
                 maxrr = std::max(maxrr, rr);
             }
-            if ((rc = blas_cg_p(g, s, p, rs, ps, red))) break;
+            if ((rc = blas_cg_p_x(g, s, p, rs, ps, xs, xprec, reliable ? 0 : (fresh ? 1 : 2), red))) break;
+            if (!reliable) fresh = false;
         }
         if (rc) break;
         if (!inf.converged) {
             // fold in what the sloppy recursion has so far
-            blas_accum_zero(g, s, x_even, xs, xprec);
+            if ((rc = blas_accum(g, s, x_even, xs, xprec, fresh, nullptr, ps, red))) break;
         }
         // x_o = b_o + kappa H_oe x_e
         if ((rc = op.hop(g64, x_odd, x_even, PLQCD_ODD, 0, b_odd, prm->kappa, 1.0))) break;
