@@ -736,7 +736,7 @@ def run_mrhs(torch, P, lat, g64, args, nrhs=8):
         res[name] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)
         cfg = tuned_config(P, f"dslash_mrhs|p{prec}|r{recon}|plain|n{nrhs}|{lat.dims[0]}x")
         res[name]["tuned_variant"] = cfg[0] if cfg else None
-        if (prec, recon) == (P.F64, 18):
+        if prec == P.F64:
             forced = {}
             for v, blk in ((4208, 256), (4204, 128), (4308, 256), (4304, 128), (100, 128), (102, 64), (2, 128),
                            (1022, 64)):
