@@ -753,9 +753,12 @@ static bool mrhs_sink_config(const Geom &g, int prec, int recon, int nrhs, TuneR
     return v == 2002 || v == 2022 || v == 2032 || v == 2102 || v == 2122;
 }
 
-bool dslash_mrhs_sink_ok(const Geom &g, int prec, int recon, int nrhs) {
+bool dslash_mrhs_sink_ok(const Geom &g, int prec, int recon, int nrhs, int *variant, int *block) {
     TuneResult t;
-    return prec != PLQCD_F64 && nrhs >= 2 && mrhs_sink_config(g, prec, recon, nrhs, &t);
+    if (prec == PLQCD_F64 || nrhs < 2 || !mrhs_sink_config(g, prec, recon, nrhs, &t)) return false;
+    if (variant) *variant = t.variant;
+    if (block) *block = t.block;
+    return true;
 }
 
 int launch_dslash_mrhs_sink(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,

@@ -161,7 +161,7 @@ struct RhsSink {
 };
 // the tuned xpay configuration of this multi-RHS hop is an RHS-pair kernel,
 // so launch_dslash_mrhs_sink can run it
-bool dslash_mrhs_sink_ok(const Geom &g, int prec, int recon, int nrhs);
+bool dslash_mrhs_sink_ok(const Geom &g, int prec, int recon, int nrhs, int *variant = nullptr, int *block = nullptr);
 int launch_dslash_mrhs_sink(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
                             const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x,
                             double b, int epi, const RhsSink &sink);
@@ -169,6 +169,11 @@ int launch_dslash_mrhs_sink(const Geom &g, cudaStream_t s, const void *gauge, in
 // dynamic shared-memory opt-in of kernel `func` on the current device, set
 // once per (kernel, device) to at least `bytes` (utils.cpp)
 int smem_optin(const void *func, size_t bytes);
+
+// ID of the current CUDA context (unique within the process, never reused;
+// a cudaDeviceReset gives the device a new one), 0 when the driver does not
+// provide it (utils.cpp)
+unsigned long long current_context_id();
 
 // device workspace of at least `bytes`, owned by the lattice (cg.cu)
 int lattice_workspace(plqcd_lattice *lat, size_t bytes, void **out);

@@ -24,6 +24,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <string>
 #include <vector>
 
 #include "blas.cuh"
@@ -631,6 +634,20 @@ int alloc_item(Batch &B, Item &it, bool own_ws) {
     return PLQCD_OK;
 }
 
+// true the first time a (CUDA context, lattice, format, RHS count, kernel
+// configuration) runs the fused hops in this process
+bool first_fused_use(const Geom &g, int prec, int recon, int nrhs, int variant, int block) {
+    static std::mutex mu;
+    static std::set<std::string> seen;
+    const unsigned long long ctx = current_context_id();
+    if (!ctx) return true;  // no context ID: warm every time
+    char key[160];
+    snprintf(key, sizeof key, "%llu|%d|%d|%d|%dx%dx%dx%d|%d|%d", ctx, prec, recon, nrhs, g.L[0], g.L[1], g.L[2],
+             g.L[3], variant, block);
+    std::lock_guard<std::mutex> lk(mu);
+    return seen.insert(key).second;
+}
+
 // tune the plain and xpay hops of the sloppy and the FP64 operator on this
 // item's block (zeroed fields) when the tuner has no entry for them yet: a
 // captured launch cannot tune and would take the first candidate
@@ -652,11 +669,13 @@ int tune_item(Batch &B, Item &it) {
     // fused CG sums when the tuned sloppy xpay hop is an RHS-pair kernel
     // (PLQCD_MCG_FUSED=0: separate passes)
     const char *e = getenv("PLQCD_MCG_FUSED");
-    it.fused = B.mixed && !(e && e[0] == '0') && dslash_mrhs_sink_ok(*it.g, gs->prec, gs->recon, n);
-    if (it.fused) {
+    int variant = 0, block = 0;
+    it.fused = B.mixed && !(e && e[0] == '0') &&
+               dslash_mrhs_sink_ok(*it.g, gs->prec, gs->recon, n, &variant, &block);
+    if (it.fused && first_fused_use(*it.g, gs->prec, gs->recon, n, variant, block)) {
         // load the fused kernels and set their shared memory before any
-        // capture (on zeroed fields; the solve's start overwrites every
-        // scalar they set)
+        // capture, once per device and configuration (on zeroed fields; the
+        // solve's start overwrites every scalar they set)
         PLQCD_CUDA_TRY(cudaMemsetAsync(it.p, 0, it.fbs * n, B.s));
         PLQCD_CUDA_TRY(cudaMemsetAsync(it.rs, 0, it.fbs * n, B.s));
         PLQCD_TRY(B.mhat_fused(it, gs, it.t, it.p, it.tmps, false, 1));

@@ -35,32 +35,6 @@ std::mutex g_mu;
 void *g_scratch_ptr[kMaxDevices] = {};
 unsigned long long g_scratch_ctx[kMaxDevices] = {};  // context ID the address belongs to
 
-// ID of the current CUDA context (unique within the process, never reused),
-// 0 when the driver does not provide it
-unsigned long long current_context_id() {
-    using GetCurrent = CUresult (*)(CUcontext *);
-    using GetId = CUresult (*)(CUcontext, unsigned long long *);
-    static GetCurrent get_current = nullptr;
-    static GetId get_id = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr, *q = nullptr;
-        cudaDriverEntryPointQueryResult r1 = cudaDriverEntryPointSymbolNotFound, r2 = r1;
-        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r1) == cudaSuccess &&
-            cudaGetDriverEntryPoint("cuCtxGetId", &q, cudaEnableDefault, &r2) == cudaSuccess &&
-            r1 == cudaDriverEntryPointSuccess && r2 == cudaDriverEntryPointSuccess) {
-            get_current = reinterpret_cast<GetCurrent>(p);
-            get_id = reinterpret_cast<GetId>(q);
-        } else {
-            cudaGetLastError();
-        }
-    });
-    CUcontext c = nullptr;
-    unsigned long long id = 0;
-    if (!get_current || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
-    return id;
-}
-
 // Device address of the scratch on the current device. The set-up (the
 // first call on a device, with that device current) looks it up with
 // cudaGetSymbolAddress and loads the reduction kernel of every precision.
@@ -70,7 +44,7 @@ int scratch_address(int device, void **out) {
     if (device < 0 || device >= kMaxDevices)
         return plqcd::set_error(PLQCD_ERR_ARG, "plqcd_spinor_norm2_noalloc: device %d out of range", device);
     std::lock_guard<std::mutex> lk(g_mu);
-    const unsigned long long ctx = current_context_id();
+    const unsigned long long ctx = plqcd::current_context_id();
     if (!g_scratch_ptr[device] || g_scratch_ctx[device] != ctx) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_norm2_scratch);

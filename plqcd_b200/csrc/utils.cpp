@@ -7,6 +7,7 @@
 // ordinary aligned heap memory. A registry maps each aligned address back to
 // its allocation so afree can release it (and ignores unknown addresses, as
 // lib/utils.c:68-90 does).
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <sys/time.h>
 
@@ -179,5 +180,32 @@ int smem_optin(const void *func, size_t bytes) {
     have = bytes;
     return PLQCD_OK;
 }
+
+// ID of the current CUDA context (unique within the process, never reused),
+// 0 when the driver does not provide it
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr, *q = nullptr;
+        cudaDriverEntryPointQueryResult r1 = cudaDriverEntryPointSymbolNotFound, r2 = r1;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r1) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &q, cudaEnableDefault, &r2) == cudaSuccess &&
+            r1 == cudaDriverEntryPointSuccess && r2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrent>(p);
+            get_id = reinterpret_cast<GetId>(q);
+        } else {
+            cudaGetLastError();
+        }
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
 
 }  // namespace plqcd
