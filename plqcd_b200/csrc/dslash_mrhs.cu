@@ -253,8 +253,11 @@ __global__ void __launch_bounds__(1024) k_sink_finish(const RhsSink k, int nsb) 
     if (EPI == 1) {
         k.pAp[f] = tot;
         k.alpha[f] = tot > 0 ? k.rr[f] / tot : 0.0;
-    } else {
+    } else if (EPI == 2) {
         k.rr_old[f] = k.rr[f];
+        k.rr[f] = tot;
+        k.beta[f] = k.rr_old[f] > 0 ? tot / k.rr_old[f] : 0.0;
+    } else {  // 3: the restart residual of a reliable update
         k.rr[f] = tot;
         k.beta[f] = k.rr_old[f] > 0 ? tot / k.rr_old[f] : 0.0;
     }
@@ -304,10 +307,10 @@ __device__ __forceinline__ void pair_epilogue(const MrhsArgs &a, int r0, bool tw
             }
         } else {
             SIO::store(a.out + (size_t)(r0 + j) * a.fbytes, a.Vh, h, o);
-            if (EPI == 1) v[j] = sq_sum(o);
+            if (EPI == 1 || EPI == 3) v[j] = sq_sum(o);
         }
     }
-    if (EPI > 0) sink_block(a, r0, two, v[0], v[1]);
+    if (EPI > 0 && EPI < 4) sink_block(a, r0, two, v[0], v[1]);
 }
 
 // RHS-pair kernel: one thread, one output site, two right-hand sides on the
@@ -324,9 +327,11 @@ __global__ void __launch_bounds__(256, MINB) k_dslash_mrhs_pair(const MrhsArgs a
     const int tile = blockIdx.x % a.ntiles;
     const int hh = (blockIdx.x / a.ntiles) * blockDim.x + threadIdx.x;
     const bool valid = hh < a.Vh;
-    if (EPI == 0 && !valid) return;  // (EPI > 0: every thread takes part in the sums)
+    if ((EPI == 0 || EPI == 4) && !valid) return;  // (EPI 1-3: every thread takes part in the sums)
     const int h = valid ? hh : (int)a.Vh - 1;
     const int r0 = 2 * tile;
+    // restart hops (EPI 3, 4): a pair of retired RHS has nothing to compute (whole block)
+    if (EPI >= 3 && !a.sink.active[r0] && !(r0 + 1 < a.nrhs && a.sink.active[r0 + 1])) return;
     const bool two = r0 + 1 < a.nrhs;
     const char *in0 = a.in + (size_t)r0 * a.fbytes;
     const char *in1 = two ? in0 + a.fbytes : in0;
@@ -381,10 +386,12 @@ __global__ void __launch_bounds__(256, MINB) k_dslash_mrhs_pair_pipe(const MrhsA
     const int tile = blockIdx.x % a.ntiles;
     const int hh = (blockIdx.x / a.ntiles) * B + threadIdx.x;
     const bool valid = hh < a.Vh;
-    // no block-level barrier below except the sums of EPI > 0, in which
+    // no block-level barrier below except the sums of EPI 1-3, in which
     // every thread (a past-the-end one on the last site) takes part
-    if (EPI == 0 && !valid) return;
+    if ((EPI == 0 || EPI == 4) && !valid) return;
     const int h = valid ? hh : (int)a.Vh - 1;
+    // restart hops (EPI 3, 4): a pair of retired RHS has nothing to compute (whole block)
+    if (EPI >= 3 && !a.sink.active[2 * tile] && !(2 * tile + 1 < a.nrhs && a.sink.active[2 * tile + 1])) return;
     const int r0 = 2 * tile;
     const bool two = r0 + 1 < a.nrhs;
     const char *in0 = a.in + (size_t)r0 * a.fbytes;
@@ -462,12 +469,15 @@ static int launch_pair(const Geom &g, cudaStream_t s, MrhsArgs a, int block, boo
         return set_error(PLQCD_ERR_ARG, "dslash_mrhs: the RHS-pair kernel computes in FP32 only");
     } else {
         if (g.Vh >= (1L << 31)) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: lattice too large for 32-bit sites");
-        if (epi && (!xpay || block > 256 || block % 32)) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: fused sums need an xpay hop");
+        if (epi && ((epi == 4) == xpay || block > 256 || block % 32))
+            return set_error(PLQCD_ERR_ARG, "dslash_mrhs: fused epilogue %d does not fit this hop", epi);
         a.ntiles = (a.nrhs + 1) / 2;
         const long nblk = (g.Vh + block - 1) / block * a.ntiles;
         if (nblk > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: grid too large");
         if constexpr (ST == 0) {
-            auto k = epi == 2 ? k_dslash_mrhs_pair<SIO, LIO, true, MINB, 2>
+            auto k = epi == 4 ? k_dslash_mrhs_pair<SIO, LIO, false, MINB, 4>
+                   : epi == 3 ? k_dslash_mrhs_pair<SIO, LIO, true, MINB, 3>
+                   : epi == 2 ? k_dslash_mrhs_pair<SIO, LIO, true, MINB, 2>
                    : epi == 1 ? k_dslash_mrhs_pair<SIO, LIO, true, MINB, 1>
                    : xpay     ? k_dslash_mrhs_pair<SIO, LIO, true, MINB, 0>
                               : k_dslash_mrhs_pair<SIO, LIO, false, MINB, 0>;
@@ -476,7 +486,9 @@ static int launch_pair(const Geom &g, cudaStream_t s, MrhsArgs a, int block, boo
             constexpr int NS = LIO::NSLOT + 2 * SIO::NSLOT;
             const size_t smem = (size_t)(ST * NS + (xpay ? 2 * SIO::NSLOT : 0)) * 16 * block;
             if (smem > 227 * 1024) return set_error(PLQCD_ERR_ARG, "dslash_mrhs: %zu bytes of shared memory", smem);
-            auto k = epi == 2 ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB, 2>
+            auto k = epi == 4 ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, false, MINB, 4>
+                   : epi == 3 ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB, 3>
+                   : epi == 2 ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB, 2>
                    : epi == 1 ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB, 1>
                    : xpay     ? k_dslash_mrhs_pair_pipe<SIO, LIO, ST, true, MINB, 0>
                               : k_dslash_mrhs_pair_pipe<SIO, LIO, ST, false, MINB, 0>;
@@ -738,7 +750,7 @@ static int mrhs_args(const Geom &g, const void *gauge, int prec, void *out, cons
 
 // the RHS-pair configuration that runs this xpay hop with fused sums: the
 // environment's, else the tuned one (false when it is another kernel)
-static bool mrhs_sink_config(const Geom &g, int prec, int recon, int nrhs, TuneResult *t) {
+static bool mrhs_sink_config(const Geom &g, int prec, int recon, int nrhs, TuneResult *t, bool xpay = true) {
     const char *ev = getenv("PLQCD_MRHS_VARIANT");
     if (ev && *ev) {
         const char *eb = getenv("PLQCD_MRHS_BLOCK");
@@ -746,7 +758,7 @@ static bool mrhs_sink_config(const Geom &g, int prec, int recon, int nrhs, TuneR
         t->block = (eb && *eb) ? atoi(eb) : 128;
     } else {
         char key[256];
-        mrhs_key(key, sizeof key, g, prec, recon, nrhs, true);
+        mrhs_key(key, sizeof key, g, prec, recon, nrhs, xpay);
         if (!tune_lookup(key, t)) return false;
     }
     const int v = t->variant;
@@ -754,8 +766,10 @@ static bool mrhs_sink_config(const Geom &g, int prec, int recon, int nrhs, TuneR
 }
 
 bool dslash_mrhs_sink_ok(const Geom &g, int prec, int recon, int nrhs, int *variant, int *block) {
-    TuneResult t;
-    if (prec == PLQCD_F64 || nrhs < 2 || !mrhs_sink_config(g, prec, recon, nrhs, &t)) return false;
+    TuneResult t, tp;
+    if (prec == PLQCD_F64 || nrhs < 2 || !mrhs_sink_config(g, prec, recon, nrhs, &t) ||
+        !mrhs_sink_config(g, prec, recon, nrhs, &tp, false))
+        return false;
     if (variant) *variant = t.variant;
     if (block) *block = t.block;
     return true;
@@ -765,17 +779,21 @@ int launch_dslash_mrhs_sink(const Geom &g, cudaStream_t s, const void *gauge, in
                             const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x,
                             double b, int epi, const RhsSink &sink) {
     TuneResult t;
-    if (!x || (epi != 1 && epi != 2) || prec == PLQCD_F64 || !mrhs_sink_config(g, prec, recon, nrhs, &t))
-        return set_error(PLQCD_ERR_ARG, "dslash_mrhs: no RHS-pair configuration for fused sums");
+    const bool xpay = epi != 4;
+    if (epi < 1 || epi > 4 || (xpay != (x != nullptr)) || prec == PLQCD_F64 ||
+        !mrhs_sink_config(g, prec, recon, nrhs, &t, xpay))
+        return set_error(PLQCD_ERR_ARG, "dslash_mrhs: no RHS-pair configuration for fused epilogue %d", epi);
     dev::MrhsArgs m;
     PLQCD_TRY(mrhs_args(g, gauge, prec, out, in, nrhs, out_parity, flags, a, x, b, m));
     m.sink = sink;
-    PLQCD_TRY(mrhs_dispatch(g, s, prec, recon, m, t.variant, t.block, true, epi));
+    PLQCD_TRY(mrhs_dispatch(g, s, prec, recon, m, t.variant, t.block, xpay, epi));
     const int nsb = (int)((g.Vh + t.block - 1) / t.block);
     if (epi == 1)
         dev::k_sink_finish<1><<<nrhs, 1024, 0, s>>>(sink, nsb);
-    else
+    else if (epi == 2)
         dev::k_sink_finish<2><<<nrhs, 1024, 0, s>>>(sink, nsb);
+    else if (epi == 3)
+        dev::k_sink_finish<3><<<nrhs, 1024, 0, s>>>(sink, nsb);
     PLQCD_CUDA_TRY(cudaGetLastError());
     return PLQCD_OK;
 }

@@ -153,6 +153,9 @@ bool dslash_mrhs_tuned(const Geom &g, int prec, int recon, int nrhs, bool xpay);
 //   epi 1: out = t as usual; pAp = |t|^2, alpha = rr / pAp
 //   epi 2: out = Ap is not stored; r -= alpha Ap in place (rvec);
 //          rr_old = rr, rr = |r|^2, beta = rr / rr_old
+//   epi 3: out as usual; rr = |out|^2, beta = rr / rr_old (the restart of
+//          a reliable update); RHS pairs that are both retired are skipped
+//   epi 4: a plain hop (x null), no sums; retired RHS pairs are skipped
 struct RhsSink {
     double *partials;    // nrhs * ceil(Vh / 32) doubles
     double *rr, *rr_old, *pAp, *alpha, *beta;

@@ -330,20 +330,25 @@ __global__ void k_ctl_iter(McgControl *c, const McgState *st, int nst, int mixed
     }
 }
 
-// after a reliable update: every x_s was folded into x (fresh), retire
-// converged RHS, tighten convergence triggers
+// within a reliable update, once item s's FP64 Schur residuals are in:
+// retire its converged RHS (before its restart, which then skips them)
+__global__ void k_ctl_converged(McgControl *c, const McgState *st, int s) {
+    for (int f = threadIdx.x; f < st[s].nrhs; f += blockDim.x)
+        if (st[s].active[f] && st[s].sr2[f] <= c->tol2 * st[s].bp2[f]) {
+            st[s].active[f] = 0;
+            st[s].conv_iter[f] = c->iter;
+        }
+}
+
+// after a reliable update: every x_s was folded into x (fresh); tighten
+// the convergence triggers of the RHS still active
 __global__ void k_ctl_reliable(McgControl *c, const McgState *st, int nst) {
     for (int s = 0; s < nst; s++)
         for (int f = threadIdx.x; f < st[s].nrhs; f += blockDim.x) {
             st[s].fresh[f] = 1;
             if (!st[s].active[f]) continue;
             st[s].maxrr[f] = st[s].rr[f];
-            if (st[s].sr2[f] <= c->tol2 * st[s].bp2[f]) {
-                st[s].active[f] = 0;
-                st[s].conv_iter[f] = c->iter;
-            } else if (st[s].rr[f] <= st[s].target[f]) {
-                st[s].target[f] *= 0.25;
-            }
+            if (st[s].rr[f] <= st[s].target[f]) st[s].target[f] *= 0.25;
         }
     if (threadIdx.x == 0) {
         c->reliable_count++;
@@ -426,6 +431,16 @@ struct Batch {
         unsigned fi = dagger ? PLQCD_DSLASH_G5_IN : 0u, fo = dagger ? PLQCD_DSLASH_G5_OUT : 0u;
         PLQCD_TRY(hop(it, gf, tmp_o, in, PLQCD_ODD, fi));
         return hop(it, gf, out, tmp_o, PLQCD_EVEN, fo, in, -kappa * kappa, 1.0);
+    }
+    // rs = Mhat^dag t (the restart of a reliable update) with |rs|^2 -> rr,
+    // beta in the second hop's epilogue; RHS pairs that are both retired
+    // skip both hops
+    int restart_fused(Item &it, const plqcd_gauge *gs) {
+        RhsSink k{it.hop_partials, it.st.rr, it.st.rr_old, it.st.pAp, it.st.alpha, it.st.beta, it.st.active, it.rs};
+        PLQCD_TRY(launch_dslash_mrhs_sink(*it.g, s, gs->data, gs->prec, gs->recon, it.tmps, it.t, it.in.nrhs,
+                                          PLQCD_ODD, PLQCD_DSLASH_G5_IN, 1.0, nullptr, 0.0, 4, k));
+        return launch_dslash_mrhs_sink(*it.g, s, gs->data, gs->prec, gs->recon, it.rs, it.tmps, it.in.nrhs,
+                                       PLQCD_EVEN, PLQCD_DSLASH_G5_OUT, -kappa * kappa, it.t, 1.0, 3, k);
     }
     // mhat with the CG sums of epi (1: |out|^2 -> pAp, alpha; 2: r -= alpha
     // out, |r|^2 -> rr, beta, out not stored) in the second hop's epilogue
@@ -528,10 +543,17 @@ struct Batch {
             if (mixed) {
                 const plqcd_gauge *gs = it.in.g_sloppy ? it.in.g_sloppy : it.in.g64;
                 PLQCD_TRY(sub_norm2_to(it, it.t, it.ps, it.bprime, it.t64, M_SR2));
-                PLQCD_TRY(mhat(it, gs, it.rs, it.t, it.tmps, true));
-                PLQCD_TRY(norm2(it, it.rs, it.ps, M_RR_TRUE, false));
+                PLQCD_TRY(ctl_converged(it));
+                if (it.fused) {
+                    // |r|^2 in the second hop; pairs of retired RHS skipped
+                    PLQCD_TRY(restart_fused(it, gs));
+                } else {
+                    PLQCD_TRY(mhat(it, gs, it.rs, it.t, it.tmps, true));
+                    PLQCD_TRY(norm2(it, it.rs, it.ps, M_RR_TRUE, false));
+                }
             } else {
                 PLQCD_TRY(sub_norm2(it, it.r64, it.bprime, it.t64, M_SR2));
+                PLQCD_TRY(ctl_converged(it));
                 PLQCD_TRY(mhat(it, it.in.g64, it.t64, it.r64, it.tmp64, true));
                 PLQCD_TRY(norm2(it, it.t64, PLQCD_F64, M_RR_TRUE, false));
                 PLQCD_TRY(convert(it, it.rs, it.ps, it.t64, PLQCD_F64));
@@ -556,6 +578,11 @@ struct Batch {
     // h: condition to set from the device (graph mode), or none (eager)
     int ctl_iter(const cudaGraphConditionalHandle *h) {
         dev::k_ctl_iter<<<1, 256, 0, s>>>(ctl, st_dev, (int)items.size(), mixed, h != nullptr, h ? *h : 0);
+        PLQCD_CUDA_TRY(cudaGetLastError());
+        return PLQCD_OK;
+    }
+    int ctl_converged(const Item &it) {
+        dev::k_ctl_converged<<<1, 256, 0, s>>>(ctl, st_dev, (int)(&it - items.data()));
         PLQCD_CUDA_TRY(cudaGetLastError());
         return PLQCD_OK;
     }
@@ -680,6 +707,7 @@ int tune_item(Batch &B, Item &it) {
         PLQCD_CUDA_TRY(cudaMemsetAsync(it.rs, 0, it.fbs * n, B.s));
         PLQCD_TRY(B.mhat_fused(it, gs, it.t, it.p, it.tmps, false, 1));
         PLQCD_TRY(B.mhat_fused(it, gs, it.Ap, it.t, it.tmps, true, 2));
+        PLQCD_TRY(B.restart_fused(it, gs));
     }
     return PLQCD_OK;
 }
