@@ -788,9 +788,10 @@ def run_batch(torch, P, d: Dist, args, f64_single_seconds: float | None):
         items.append(dict(lat=lat, g64=g64, g_sloppy=gs, nrhs=n, b_even=blk[0], b_odd=blk[1], x_even=blk[2],
                           x_odd=blk[3]))
     prm = P.cg_param(kappa=kappa, tol=tol, sloppy_prec=P.F16, delta=args.delta)
-    P.invert_cg_batch(items, P.cg_param(kappa=kappa, tol=tol, sloppy_prec=P.F16, max_iter=3), True,
+    graph = not args.eager
+    P.invert_cg_batch(items, P.cg_param(kappa=kappa, tol=tol, sloppy_prec=P.F16, max_iter=3), graph,
                       raise_on_error=False)  # warm-up: tunes every launch configuration
-    info, res = P.invert_cg_batch(items, prm, True)
+    info, res = P.invert_cg_batch(items, prm, graph)
     site_rhs = sum(it["lat"].V * it["nrhs"] for it in items)
     out = {"lattices": [[list(L), n] for L, n in spec], "kappa": kappa, "tol": tol, "sloppy": "f16_12",
            "delta": args.delta,
@@ -817,7 +818,7 @@ def run_batch(torch, P, d: Dist, args, f64_single_seconds: float | None):
     # multi-RHS mixed CG at 32^3x64 (8 RHS) alone, per RHS, against one plain
     # FP64 CG: the median of three solves (single solves vary by a few percent)
     it = items[2]
-    runs = [P.invert_cg_batch([it], prm, True)[0] for _ in range(3)]
+    runs = [P.invert_cg_batch([it], prm, graph)[0] for _ in range(3)]
     info8 = sorted(runs, key=lambda r: r.seconds)[1]
     out["mrhs_32x32x32x64"] = {"nrhs": it["nrhs"], "seconds": round(info8.seconds, 4),
                                "seconds_runs": [round(r.seconds, 4) for r in runs],
@@ -897,6 +898,9 @@ def main():
                     help="dslash / cg: only that section (profiling runs); sharded: the t-slab "
                          "decomposition with --shards slabs held on one GPU")
     ap.add_argument("--shards", type=int, default=4, help="slabs of --only sharded")
+    ap.add_argument("--eager", action="store_true",
+                    help="batched solves as eager loops instead of one graph launch (ncu does not profile "
+                         "the kernels of graphs with conditional nodes)")
     ap.add_argument("--mrhs-formats", default="", help="comma list of the multi-RHS formats to time (default all)")
     args = ap.parse_args()
     args.lattice = tuple(int(x) for x in args.lattice.split(","))
