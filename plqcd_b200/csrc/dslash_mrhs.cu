@@ -1,13 +1,22 @@
 // dslash_mrhs.cu -- hopping matrix on a block of right-hand sides.
 //
-// One thread handles one output site for a tile of NR right-hand sides: per
-// direction it loads the link once and applies it to the NR neighbour
-// spinors, so a link's HBM bytes are shared by the tile. Consecutive blocks
-// cover the RHS tiles of the same sites (tile index fastest), so the other
-// tiles find the links in L2 and the link traffic per launch is paid once
-// for all nrhs right-hand sides: bytes per site and RHS =
+// Kernel families (the tuner times them per format, lattice and RHS count):
+// - RHS tiles: one thread handles one output site for a tile of NR RHS; per
+//   direction it loads the link once and applies it to the NR neighbour
+//   spinors (direct loads, or a cp.async ring);
+// - RHS pairs (FP32, F16, BF16): two RHS on the two lanes of packed FP32
+//   instructions, the link loaded, rebuilt and broadcast once per pair;
+//   their xpay form can carry the CG's dot products in its epilogue
+//   (RhsSink, for the batched solver);
+// - FP64 link sharing: a block of RHS warps over 32 sites reads each link
+//   from shared memory;
+// - the single-RHS kernels with the RHS index folded into the grid
+//   (dslash.cu), and the tensor-core kernel (dslash_mrhs_tc.cu).
+// Consecutive blocks cover the RHS tiles of the same sites (tile index
+// fastest), so the other tiles find the links in L2 and the link traffic per
+// launch is paid once for all nrhs right-hand sides: bytes per site and RHS =
 // 2 * spinor + 8 * link / nrhs. The per-direction arithmetic is that of the
-// single-RHS kernel (dslash_core.cuh).
+// single-RHS kernel (dslash_core.cuh), and every family gives the same bits.
 //
 // A block of fields is nrhs one-parity fields back to back (field r at
 // base + r * field_bytes).

@@ -6,6 +6,9 @@
 // its own CG recursion (own alpha, beta, residuals) on Mhat^dag Mhat,
 // Mhat = 1 - kappa^2 H_eo H_oe (the operator of cg.cu), but the hopping
 // kernels process the whole block (dslash_mrhs.cu), sharing link traffic.
+// Per iteration the vector work is |t|^2, r -= alpha Ap with |r|^2, and
+// p = r + beta p with the solution update x_s += alpha p; when the sloppy
+// hops are RHS-pair kernels, the first two ride in the hops' epilogues.
 // All scalars live in device memory and are finalised by the reductions;
 // three small control kernels decide, on the device, whether the iteration
 // needs a reliable update (any active RHS whose sloppy residual dropped by
