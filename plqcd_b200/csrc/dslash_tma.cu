@@ -78,6 +78,7 @@ struct TmaGeom {
     // failure-detection test hook) each consumer warp first waits, with that
     // limit, on a barrier that nothing completes, so the wait runs out
     uint64_t cwait_ns;
+    uint32_t wait_hint_ns;  // suspend hint of the mbarrier retries (0: plain polls)
     int stall;
     void *out0, *out1;  // output of parity 0 / 1 (full); out0 otherwise
     const void *x;      // xpay operand (single parity)
@@ -293,8 +294,8 @@ constexpr uint64_t kDrainLimitNs = 200000000ull;  // 0.2 s
 // no lane leaves while the others go on to __syncwarp. Lane 0 records the
 // abort for the CTA's producer and the timeout for the host.
 __device__ __forceinline__ bool consumer_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns,
-                                              volatile int *abort) {
-    const bool ok = __all_sync(0xffffffffu, mbar_wait(bar, parity, limit_ns, abort));
+                                              volatile int *abort, uint32_t hint_ns = 0) {
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(bar, parity, limit_ns, abort, hint_ns));
     if (!ok && (threadIdx.x & 31) == 0) {
         *abort = 1;
         atomicExch(&g_tma_status, 1);
@@ -520,7 +521,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
 #pragma unroll 1
             for (int kd = 0; kd < 8; kd++) {
                 // the consumers released this buffer's previous use
-                if (!mbar_wait(empty_bar + 8u * b, (k + 1) & 1, kWaitLimitNs, abort)) {
+                if (!mbar_wait(empty_bar + 8u * b, (k + 1) & 1, kWaitLimitNs, abort, g.wait_hint_ns)) {
                     ok = false;
                     break;
                 }
@@ -567,7 +568,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
 #pragma unroll
         for (int kd = 0; kd < 8; kd++) {
             const int d = dir_at(kd);
-            if (!consumer_wait(full_bar + 8u * b, k & 1, g.cwait_ns, abort)) return;
+            if (!consumer_wait(full_bar + 8u * b, k & 1, g.cwait_ns, abort, g.wait_hint_ns)) return;
             const uint8_t *st = sbase + (size_t)b * g.stage_bytes;
             // element index and plane stride of the neighbour spinor and the
             // link, in the NY-row box or in the one-row box of a y stage
@@ -663,7 +664,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
         bool ok = true;
         for (int it = 0; it < nmine && ok; it++) {
             const TileCoord c = tile_coord(g, bid + it * (int)gridDim.x);
-            if (!mbar_wait(emptyA + 8u * a, (ka + 1) & 1, kWaitLimitNs, abort)) {
+            if (!mbar_wait(emptyA + 8u * a, (ka + 1) & 1, kWaitLimitNs, abort, g.wait_hint_ns)) {
                 ok = false;
                 break;
             }
@@ -675,7 +676,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
             }
 #pragma unroll 1
             for (int s = 0; s < kStages; s++) {
-                if (!mbar_wait(emptyB + 8u * b, (kb + 1) & 1, kWaitLimitNs, abort)) {
+                if (!mbar_wait(emptyB + 8u * b, (kb + 1) & 1, kWaitLimitNs, abort, g.wait_hint_ns)) {
                     ok = false;
                     break;
                 }
@@ -720,13 +721,13 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
         cx<R> acc[12];
 #pragma unroll
         for (int e = 0; e < 12; e++) acc[e] = {R(0), R(0)};
-        if (!consumer_wait(fullA + 8u * a, ka & 1, g.cwait_ns, abort)) return;
+        if (!consumer_wait(fullA + 8u * a, ka & 1, g.cwait_ns, abort, g.wait_hint_ns)) return;
         const uint8_t *sa = sbase + (size_t)a * g.a_bytes;
         const uint8_t *sps = nullptr;  // split: the spinor stage waiting for its link stage
         int bsp = 0;
 #pragma unroll
         for (int s = 0; s < kStages; s++) {
-            if (!consumer_wait(fullB + 8u * b, kb & 1, g.cwait_ns, abort)) return;
+            if (!consumer_wait(fullB + 8u * b, kb & 1, g.cwait_ns, abort, g.wait_hint_ns)) return;
             const uint8_t *st = sbase + (size_t)nA * g.a_bytes + (size_t)b * g.stage_bytes;
             // directions of this stage: one, or the forward and backward
             // terms of x or y for a two-link stage
@@ -1096,6 +1097,12 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     tg.b = a.b;
     tg.g5_in = a.g5_in;
     tg.cwait_ns = dev::kWaitLimitNs;
+    // PLQCD_TMA_WAIT_HINT: suspend hint (ns) of the mbarrier retries
+    {
+        const char *e = getenv("PLQCD_TMA_WAIT_HINT");
+        const long v = (e && *e) ? atol(e) : 0;
+        tg.wait_hint_ns = v > 0 && v < 1000000 ? (uint32_t)v : 0u;
+    }
     tg.stall = 0;
     if (const unsigned long long ns = g_stall_test_ns.load(std::memory_order_relaxed)) {
         tg.stall = 1;

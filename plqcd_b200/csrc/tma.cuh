@@ -50,17 +50,33 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
+// try_wait that may suspend the thread for up to hint_ns until the phase
+// completes (instead of returning at once)
+__device__ __forceinline__ bool mbar_try_wait_hint(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait. Returns false when `limit_ns` passed first, or when another
-// thread of the CTA raised `*abort` meanwhile.
+// thread of the CTA raised `*abort` meanwhile. hint_ns > 0: each retry may
+// suspend the thread up to hint_ns until the phase completes (fewer polls
+// issued while waiting).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns,
-                                          const volatile int *abort) {
+                                          const volatile int *abort, uint32_t hint_ns = 0) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (;;) {
 #pragma unroll 1
         for (int i = 0; i < 32; i++)
-            if (mbar_try_wait(bar, parity)) return true;
-        if (*abort) return false;
+            if (hint_ns ? mbar_try_wait_hint(bar, parity, hint_ns) : mbar_try_wait(bar, parity)) return true;
+        if (abort && *abort) return false;
         if (global_ns() - t0 > limit_ns) return false;
     }
 }
