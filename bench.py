@@ -738,8 +738,11 @@ def run_mrhs(torch, P, lat, g64, args, nrhs=8):
         res[name]["tuned_variant"] = cfg[0] if cfg else None
         if prec == P.F64:
             forced = {}
+            # 4xxx: links shared in shared memory; 1xxxxx-8xxxxx: TMA-staged
+            # rows with RHS tiles (100000 * RHS per tile + TMA variant)
             for v, blk in ((4208, 256), (4204, 128), (4308, 256), (4304, 128), (100, 128), (102, 64), (2, 128),
-                           (1022, 64)):
+                           (1022, 64), (402202, 0), (402102, 0), (404202, 0), (402201, 0), (202202, 0),
+                           (802101, 0)):
                 os.environ["PLQCD_MRHS_VARIANT"], os.environ["PLQCD_MRHS_BLOCK"] = str(v), str(blk)
                 try:
                     forced[f"{v}/{blk}"] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)["us"]

@@ -22,6 +22,7 @@
 // base + r * field_bytes).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <type_traits>
@@ -713,6 +714,15 @@ int launch_dslash_mrhs_tc(const Geom &g, cudaStream_t s, const void *gauge, int 
                           const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x, double b,
                           int tiles);
 
+// TMA-staged RHS tiles: variant 100000 * nr + 1000 * kind + 100 * nstage + ny
+static int launch_mrhs_tma(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
+                           const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x,
+                           double b, int variant) {
+    const int nr = variant / 100000, rest = variant % 100000;
+    return launch_dslash_tma_mrhs(g, s, gauge, prec, recon, out, in, nrhs, out_parity, flags, a, x, b, rest / 1000,
+                                  (rest / 100) % 10, rest % 100, nr);
+}
+
 // tuner key of a multi-RHS hop
 static void mrhs_key(char *key, size_t n, const Geom &g, int prec, int recon, int nrhs, bool xpay) {
     snprintf(key, n, "%sdslash_mrhs|p%d|r%d|%s|n%d|%dx%dx%dx%d", device_tag().c_str(), prec, recon,
@@ -828,6 +838,26 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
             cands.push_back(t);
         }
 
+    // FP64: TMA-staged rows with RHS tiles (dslash_tma.cu; variant 100000 *
+    // RHS per tile + 1000 * kind + 100 * ring depth + rows per tile): the
+    // tile's links are staged once for its RHS, and the spinor rows move
+    // without LSU wavefronts
+    if (prec == PLQCD_F64 && !(flags & PLQCD_DSLASH_COMPAT) && getenv("PLQCD_NO_TMA") == nullptr)
+        for (int nr : {4, 2, 8})
+            for (int kind : {2, 4})
+                for (int ny : {2, 1, 4})
+                    for (int ns : {1, 2, 3}) {
+                        if (nrhs % nr || (kind == 2 ? ns == 3 : ns == 1)) continue;
+                        int blk = 0;
+                        if (dslash_tma_plan(g, prec, recon, kind, ns, ny, &blk, nullptr, nr) != PLQCD_OK) {
+                            clear_error();
+                            continue;
+                        }
+                        TuneResult t;
+                        t.variant = 100000 * nr + 1000 * kind + 100 * ns + ny;
+                        t.block = blk;
+                        cands.push_back(t);
+                    }
     // FP64: the link-sharing block kernel (4000 + 100 * depth + RHS per block)
     if (prec == PLQCD_F64 && nrhs >= 4)
         for (int v : {4208, 4204, 4308, 4304}) {
@@ -887,9 +917,14 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
         if (t.variant >= 3000 && t.variant < 4000)
             return launch_dslash_mrhs_tc(g, s, gauge, prec, recon, out, in, nrhs, out_parity, flags, a, x, b,
                                          t.variant - 3000);
+        if (t.variant >= 100000)
+            return launch_mrhs_tma(g, s, gauge, prec, recon, out, in, nrhs, out_parity, flags, a, x, b, t.variant);
         return mrhs_dispatch(g, s, prec, recon, m, t.variant, t.block, xpay);
     }
+    std::vector<int> tma_checked;
     auto launch = [&](const TuneResult &t, char *dst) -> int {
+        if (t.variant >= 100000)
+            return launch_mrhs_tma(g, s, gauge, prec, recon, dst, in, nrhs, out_parity, flags, a, x, b, t.variant);
         if (t.variant >= 3000 && t.variant < 4000)
             return launch_dslash_mrhs_tc(g, s, gauge, prec, recon, dst, in, nrhs, out_parity, flags, a, x, b,
                                          t.variant - 3000);
@@ -907,6 +942,14 @@ int launch_dslash_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int pre
         if (!scratch && cudaMalloc(&scratch, m.fbytes * nrhs) != cudaSuccess) {
             cudaGetLastError();
             return set_error(PLQCD_ERR_NOMEM, "tune: scratch allocation failed");
+        }
+        if (t.variant >= 100000 && std::find(tma_checked.begin(), tma_checked.end(), t.variant) == tma_checked.end()) {
+            // first trial of a TMA configuration: run it alone and check that
+            // no stage wait ran out before it is timed
+            tma_checked.push_back(t.variant);
+            PLQCD_TRY(launch(t, static_cast<char *>(scratch)));
+            PLQCD_CUDA_TRY(cudaStreamSynchronize(s));
+            if (dslash_tma_status(true)) return set_error(PLQCD_ERR_CUDA, "dslash_mrhs: TMA stage wait timed out");
         }
         return launch(t, static_cast<char *>(scratch));
     };

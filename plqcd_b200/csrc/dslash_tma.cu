@@ -82,6 +82,12 @@ struct TmaGeom {
     int stall;
     void *out0, *out1;  // output of parity 0 / 1 (full); out0 otherwise
     const void *x;      // xpay operand (single parity)
+    // RHS tiles (k_dslash_tma_xy with MR): nr RHS of a block of fields per
+    // tile, ngr = nrhs / nr groups, fields fbytes apart; sp_main_rb /
+    // sp_row_rb are the bytes one RHS takes in an NY-row / one-row box
+    int nr, ngr;
+    size_t fbytes;
+    uint32_t sp_main_rb[2], sp_row_rb[2];
 };
 
 // tensor maps: input spinor field f (full mode: field 0 = even input, read
@@ -222,12 +228,23 @@ __device__ int g_tma_status;  // set to 1 when a stage wait ran out
 
 struct TileCoord {
     int p, y0, zt, z, t;
+    int r0;  // first RHS of the tile (RHS tiles; 0 otherwise)
 };
 
+// MR (RHS tiles): the RHS group runs fastest, so the groups of the same
+// rows are in flight together and the links one of them brings from HBM
+// serve the others from L2
+template <bool MR = false>
 __device__ __forceinline__ TileCoord tile_coord(const TmaGeom &g, int item) {
     TileCoord c;
     int tile;
-    if (g.full) {
+    c.r0 = 0;
+    if constexpr (MR) {
+        c.p = g.out_parity;
+        const int grp = item % g.ngr;
+        c.r0 = grp * g.nr;
+        tile = item / g.ngr;
+    } else if (g.full) {
         c.p = item & 1;
         tile = item >> 1;
     } else {
@@ -333,7 +350,18 @@ __device__ __forceinline__ bool stall_test_wait(const TmaGeom &g, uint32_t never
 // results are the same bits. Per tile it stages NY+2 own-line rows instead
 // of 4 NY + 2.
 
+// a spinor box: NY rows (or one) of the (z, t) line zt; MR: of the RHS
+// c.r0 .. c.r0 + nr - 1 of the block (5-D map, RHS outermost)
+template <bool MR>
+__device__ __forceinline__ void tma_load_sp(uint32_t dst, const void *map, uint32_t bar, int y, int zt, int r0) {
+    if constexpr (MR)
+        tma_load_5d(dst, map, bar, 0, y, zt, 0, r0);
+    else
+        tma_load_4d(dst, map, bar, 0, y, zt, 0);
+}
+
 // own-line rows of the input (y0-1 and y0+NY wrapped) into an A buffer
+template <bool MR = false>
 __device__ __forceinline__ void tma_issue_xy_a(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, uint32_t dst,
                                                uint32_t bar) {
     const int f = g.full ? (c.p == 0 ? 1 : 0) : 0;
@@ -345,9 +373,9 @@ __device__ __forceinline__ void tma_issue_xy_a(const TmaMaps &m, const TmaGeom &
     for (int gr = 0; gr < g.sp_ng; gr++) {
         const void *spm = f ? (const void *)&m.sp_main[1][gr] : (const void *)&m.sp_main[0][gr];
         const void *spr = f ? (const void *)&m.sp_row[1][gr] : (const void *)&m.sp_row[0][gr];
-        tma_load_4d(dst + g.off_a_main[gr], spm, bar, 0, c.y0, c.zt, 0);
-        tma_load_4d(dst + g.off_a_lo[gr], spr, bar, 0, ylo, c.zt, 0);
-        tma_load_4d(dst + g.off_a_hi[gr], spr, bar, 0, yhi, c.zt, 0);
+        tma_load_sp<MR>(dst + g.off_a_main[gr], spm, bar, c.y0, c.zt, c.r0);
+        tma_load_sp<MR>(dst + g.off_a_lo[gr], spr, bar, ylo, c.zt, c.r0);
+        tma_load_sp<MR>(dst + g.off_a_hi[gr], spr, bar, yhi, c.zt, c.r0);
     }
 }
 
@@ -367,6 +395,7 @@ __device__ __forceinline__ int neighbour_line(const TmaGeom &g, const TileCoord 
 }
 
 // the NY spinor rows of the neighbour line of direction d (2, 3, 6, 7)
+template <bool MR = false>
 __device__ __forceinline__ uint32_t tma_issue_line_spinor(const TmaMaps &m, const TmaGeom &g, const TileCoord &c,
                                                           int d, uint32_t dst, uint32_t bar) {
     const int f = g.full ? (c.p == 0 ? 1 : 0) : 0;
@@ -374,7 +403,7 @@ __device__ __forceinline__ uint32_t tma_issue_line_spinor(const TmaMaps &m, cons
     uint32_t bytes = 0;
     for (int gr = 0; gr < g.sp_ng; gr++) {
         const void *spm = f ? (const void *)&m.sp_main[1][gr] : (const void *)&m.sp_main[0][gr];
-        tma_load_4d(dst + g.off_sp_main[gr], spm, bar, 0, c.y0, szt, 0);
+        tma_load_sp<MR>(dst + g.off_sp_main[gr], spm, bar, c.y0, szt, c.r0);
         bytes += g.sp_main_bytes[gr];
     }
     return bytes;
@@ -399,6 +428,7 @@ __device__ __forceinline__ void tma_issue_link_row(const TmaMaps &m, const TmaGe
 
 // link-ring stage s (0..5 of the six-stage table) into a B buffer. The
 // expected byte count is set before the loads are issued.
+template <bool MR = false>
 __device__ __forceinline__ void tma_issue_xy_b(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, int s,
                                                uint32_t dst, uint32_t bar) {
     if (s < 2) {  // forward and backward links of mu = s
@@ -412,7 +442,7 @@ __device__ __forceinline__ void tma_issue_xy_b(const TmaMaps &m, const TmaGeom &
     uint32_t bytes = g.lk_main_bytes;
     for (int gr = 0; gr < g.sp_ng; gr++) bytes += g.sp_main_bytes[gr];
     mbar_arrive_expect_tx(bar, bytes);
-    tma_issue_line_spinor(m, g, c, d, dst, bar);
+    tma_issue_line_spinor<MR>(m, g, c, d, dst, bar);
     tma_issue_link(m, g, c, d, dst + g.off_lk_main, bar);
 }
 
@@ -428,6 +458,7 @@ static_assert(dir_at(0) == 0 && dir_at(1) == 4 && dir_at(2) == 1 && dir_at(3) ==
               "accumulation order x+, x-, y+, y-, z+, z-, t+, t-");
 
 // split stage s (0..11) into a B buffer
+template <bool MR = false>
 __device__ __forceinline__ void tma_issue_xy_split(const TmaMaps &m, const TmaGeom &g, const TileCoord &c, int s,
                                                    uint32_t dst, uint32_t bar) {
     const int d = split_dir(s);
@@ -435,7 +466,7 @@ __device__ __forceinline__ void tma_issue_xy_split(const TmaMaps &m, const TmaGe
         uint32_t bytes = 0;
         for (int gr = 0; gr < g.sp_ng; gr++) bytes += g.sp_main_bytes[gr];
         mbar_arrive_expect_tx(bar, bytes);
-        tma_issue_line_spinor(m, g, c, d, dst, bar);
+        tma_issue_line_spinor<MR>(m, g, c, d, dst, bar);
         return;
     }
     mbar_arrive_expect_tx(bar, g.lk_main_bytes + (d == 5 ? g.lk_row_bytes : 0u));
@@ -453,15 +484,23 @@ __device__ __forceinline__ void tma_drain(uint32_t full_bar, long issued, int n)
     }
 }
 
-// the xpay / scale epilogue and the store of one output site
-template <class SIO, bool XPAY, class R>
-__device__ __forceinline__ void tma_epilogue(const TmaGeom &g, const TileCoord &c, int xh, int y, cx<R> acc[12]) {
+// the xpay / scale epilogue and the store of one output site (MR: of RHS
+// c.r0 + r of the block)
+template <class SIO, bool XPAY, class R, bool MR = false>
+__device__ __forceinline__ void tma_epilogue(const TmaGeom &g, const TileCoord &c, int xh, int y, cx<R> acc[12],
+                                             int r = 0) {
     const R aup = (R)g.a_up, alow = (R)g.a_low;
     const long h = xh + (long)g.L0h * (y + (long)g.L1 * c.zt);
     void *out = (g.full && c.p == 1) ? g.out1 : g.out0;
+    const void *xin = g.x;
+    if constexpr (MR) {
+        const size_t off = (size_t)(c.r0 + r) * g.fbytes;
+        out = static_cast<char *>(g.out0) + off;
+        if (XPAY) xin = static_cast<const char *>(g.x) + off;
+    }
     if (XPAY) {
         cx<R> xv[12];
-        SIO::load(g.x, g.Vh, h, xv);
+        SIO::load(xin, g.Vh, h, xv);
         const R bb = (R)g.b;
 #pragma unroll
         for (int e = 0; e < 12; e++) {
@@ -512,6 +551,8 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
         // producer warp: lane 0 issues every stage of every tile of this CTA
         if (tid != nthr_c) return;
         tma_prefetch_map(&m.lk_main);
+        // each refill of a buffer: wait until every consumer warp released
+        // it, fence the async proxy behind their reads, then load
         int b = 0;
         uint32_t k = 0;  // completed passes over the ring
         long issued = 0;
@@ -525,6 +566,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
                     ok = false;
                     break;
                 }
+                fence_async_proxy_shared();  // their reads before the refill
                 tma_issue_dir(m, g, c, dir_at(kd), base + (uint32_t)b * g.stage_bytes, full_bar + 8u * b);
                 issued++;
                 if (++b == g.nstage) {
@@ -614,7 +656,12 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma(const __grid_constant__ T
 // A empty | B full | B empty barriers]. Bounded waits and the drain as in
 // k_dslash_tma. A consumer warp releases the A buffer after its last read
 // of the own-line rows (direction 5), a B buffer after its last read of it.
-template <class SIO, class LIO, bool XPAY, bool SPLIT>
+// MR (RHS tiles, one parity of a block of fields): a tile is NY rows of nr
+// RHS; the spinor boxes carry the nr RHS (RHS outermost in shared memory),
+// the link boxes are staged once and serve all of them. Consumer thread
+// (RHS r, row j, half-x xh); each computes what the single-field kernel
+// computes for its RHS, in the same order (the same bits).
+template <class SIO, class LIO, bool XPAY, bool SPLIT, bool MR = false>
 __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant__ TmaMaps m,
                                                            const __grid_constant__ TmaGeom g) {
     using R = typename SIO::real;
@@ -663,12 +710,13 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
         long na = 0, nb = 0;
         bool ok = true;
         for (int it = 0; it < nmine && ok; it++) {
-            const TileCoord c = tile_coord(g, bid + it * (int)gridDim.x);
+            const TileCoord c = tile_coord<MR>(g, bid + it * (int)gridDim.x);
             if (!mbar_wait(emptyA + 8u * a, (ka + 1) & 1, kWaitLimitNs, abort, g.wait_hint_ns)) {
                 ok = false;
                 break;
             }
-            tma_issue_xy_a(m, g, c, base + (uint32_t)a * g.a_bytes, fullA + 8u * a);
+            fence_async_proxy_shared();  // the consumers' reads before the refill
+            tma_issue_xy_a<MR>(m, g, c, base + (uint32_t)a * g.a_bytes, fullA + 8u * a);
             na++;
             if (++a == nA) {
                 a = 0;
@@ -680,11 +728,12 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
                     ok = false;
                     break;
                 }
+                fence_async_proxy_shared();
                 const uint32_t dst = b_base + (uint32_t)b * g.stage_bytes;
                 if (SPLIT)
-                    tma_issue_xy_split(m, g, c, s, dst, fullB + 8u * b);
+                    tma_issue_xy_split<MR>(m, g, c, s, dst, fullB + 8u * b);
                 else
-                    tma_issue_xy_b(m, g, c, s, dst, fullB + 8u * b);
+                    tma_issue_xy_b<MR>(m, g, c, s, dst, fullB + 8u * b);
                 nb++;
                 if (++b == nB) {
                     b = 0;
@@ -702,18 +751,24 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
         return;
     }
 
-    // consumers: thread (row j, half-x xh) of the tile
+    // consumers: thread (row j, half-x xh) of the tile; MR: of RHS r
     const int L0h = g.L0h;
-    const int j = tid / L0h, xh = tid - j * L0h;
-    const int own = j * L0h + xh;
     const int SM = g.NY * L0h;  // plane stride of an NY-row box, in elements
+    const int r = MR ? tid / SM : 0;
+    const int ts = tid - r * SM;
+    const int j = ts / L0h, xh = ts - j * L0h;
+    const int own = j * L0h + xh;
+    // byte offset of this thread's RHS in an NY-row / one-row spinor box
+    // (plane groups 0 and 1)
+    const uint32_t rm0 = MR ? (uint32_t)r * g.sp_main_rb[0] : 0u, rm1 = MR ? (uint32_t)r * g.sp_main_rb[1] : 0u;
+    const uint32_t rr0 = MR ? (uint32_t)r * g.sp_row_rb[0] : 0u, rr1 = MR ? (uint32_t)r * g.sp_row_rb[1] : 0u;
     const R sg = (R)g.g5_in;
     const bool top = j + 1 == g.NY, bottom = j == 0;
     if (!stall_test_wait(g, never, abort)) return;
     int a = 0, b = 0;
     uint32_t ka = 0, kb = 0;
     for (int it = 0; it < nmine; it++) {
-        const TileCoord c = tile_coord(g, bid + it * (int)gridDim.x);
+        const TileCoord c = tile_coord<MR>(g, bid + it * (int)gridDim.x);
         const int y = c.y0 + j;
         const int x = 2 * xh + ((y + c.z + c.t + c.p) & 1);
         const int xph = ((x + 1 == g.L0) ? 0 : x + 1) >> 1;
@@ -747,15 +802,15 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
                     if (d == 0 || d == 4) {
                         // x: neighbour in the same row; the backward link sits there too
                         const int si = own - xh + (d == 0 ? xph : xmh);
-                        TmaSpinor<SIO>::load(sa + g.off_a_main[0], sa + g.off_a_main[1], si, SM, sv, n);
+                        TmaSpinor<SIO>::load(sa + g.off_a_main[0] + rm0, sa + g.off_a_main[1] + rm1, si, SM, sv, n);
                         TmaLink<LIO>::load(lk, d == 0 ? own : si, SM, U);
                     } else if (d == 1 || d == 5) {
                         // y: the row above / below, across the tile edge from the
                         // extra rows; the backward link of row 0 is the link row
                         const bool fwd = d == 1;
                         const bool edge = fwd ? top : bottom;
-                        const uint32_t so0 = edge ? (fwd ? g.off_a_hi[0] : g.off_a_lo[0]) : g.off_a_main[0];
-                        const uint32_t so1 = edge ? (fwd ? g.off_a_hi[1] : g.off_a_lo[1]) : g.off_a_main[1];
+                        const uint32_t so0 = edge ? (fwd ? g.off_a_hi[0] : g.off_a_lo[0]) + rr0 : g.off_a_main[0] + rm0;
+                        const uint32_t so1 = edge ? (fwd ? g.off_a_hi[1] : g.off_a_lo[1]) + rr1 : g.off_a_main[1] + rm1;
                         const int syi = edge ? xh : (fwd ? own + L0h : own - L0h);
                         TmaSpinor<SIO>::load(sa + so0, sa + so1, syi, edge ? L0h : SM, sv, n);
                         if (fwd)
@@ -767,7 +822,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
                     } else {
                         // z / t: the neighbour line's rows
                         const uint8_t *sp = SPLIT ? sps : st;
-                        TmaSpinor<SIO>::load(sp + g.off_sp_main[0], sp + g.off_sp_main[1], own, SM, sv, n);
+                        TmaSpinor<SIO>::load(sp + g.off_sp_main[0] + rm0, sp + g.off_sp_main[1] + rm1, own, SM, sv, n);
                         TmaLink<LIO>::load(lk, own, SM, U);
                         if (SPLIT) rel2 = bsp;
                     }
@@ -792,7 +847,7 @@ __global__ void __launch_bounds__(288, 1) k_dslash_tma_xy(const __grid_constant_
             a = 0;
             ka++;
         }
-        tma_epilogue<SIO, XPAY, R>(g, c, xh, y, acc);
+        tma_epilogue<SIO, XPAY, R, MR>(g, c, xh, y, acc, r);
     }
 }
 
@@ -849,18 +904,25 @@ bool tma_format(int prec, int recon, TmaFormat *f) {
 
 // `planes` planes of `eb`-byte elements over the half lattice, viewed as
 // (row elements, L1, L2*L3, planes[, 8 parity-mu blocks]); rows of 16- and
-// 8-byte elements are moved as 8-byte words, rows of 4-byte elements as such
-int encode_map(CUtensorMap *m, const void *base, const Geom &g, int eb, int planes, bool links, int rows) {
+// 8-byte elements are moved as 8-byte words, rows of 4-byte elements as such.
+// nfields > 0: a spinor plane group of a block of nfields fields, fstride
+// bytes apart, as a fifth dimension whose box takes nbox fields
+int encode_map(CUtensorMap *m, const void *base, const Geom &g, int eb, int planes, bool links, int rows,
+               int nfields = 0, size_t fstride = 0, int nbox = 1) {
     auto fn = encode_fn();
     if (!fn) return set_error(PLQCD_ERR_CUDA, "dslash: cuTensorMapEncodeTiled is not available");
     const cuuint64_t row_b = (cuuint64_t)g.L0h * eb;
     const int word = eb >= 8 ? 8 : 4;
     const cuuint64_t inner = row_b / word;
-    cuuint64_t dims[5] = {inner, (cuuint64_t)g.L[1], (cuuint64_t)g.L[2] * g.L[3], (cuuint64_t)planes, 8};
-    cuuint64_t strides[4] = {row_b, row_b * g.L[1], (cuuint64_t)g.Vh * eb, (cuuint64_t)g.Vh * eb * planes};
-    cuuint32_t box[5] = {(cuuint32_t)inner, (cuuint32_t)rows, 1, (cuuint32_t)planes, 1};
+    const bool blockf = !links && nfields > 0;
+    cuuint64_t dims[5] = {inner, (cuuint64_t)g.L[1], (cuuint64_t)g.L[2] * g.L[3], (cuuint64_t)planes,
+                          blockf ? (cuuint64_t)nfields : 8};
+    cuuint64_t strides[4] = {row_b, row_b * g.L[1], (cuuint64_t)g.Vh * eb,
+                             blockf ? (cuuint64_t)fstride : (cuuint64_t)g.Vh * eb * planes};
+    cuuint32_t box[5] = {(cuuint32_t)inner, (cuuint32_t)rows, 1, (cuuint32_t)planes, blockf ? (cuuint32_t)nbox : 1};
     cuuint32_t es[5] = {1, 1, 1, 1, 1};
-    CUresult r = fn(m, word == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32, links ? 5 : 4,
+    CUresult r = fn(m, word == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32,
+                    (links || blockf) ? 5 : 4,
                     const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(PLQCD_ERR_CUDA, "dslash: tensor map encoding failed (%d)", (int)r);
@@ -887,11 +949,13 @@ int sm_count() {
 
 inline uint32_t round128(uint32_t v) { return (v + 127u) & ~127u; }
 
-template <class SIO, class LIO, bool XPAY>
+template <class SIO, class LIO, bool XPAY, bool MR = false>
 int launch_tma_t(cudaStream_t s, const dev::TmaMaps &m, const dev::TmaGeom &tg, int block, size_t smem) {
-    auto k = !tg.nstage_a ? dev::k_dslash_tma<SIO, LIO, XPAY>
-             : tg.split   ? dev::k_dslash_tma_xy<SIO, LIO, XPAY, true>
-                          : dev::k_dslash_tma_xy<SIO, LIO, XPAY, false>;
+    auto k = MR ? (tg.split ? dev::k_dslash_tma_xy<SIO, LIO, XPAY, true, MR>
+                            : dev::k_dslash_tma_xy<SIO, LIO, XPAY, false, MR>)
+             : !tg.nstage_a ? dev::k_dslash_tma<SIO, LIO, XPAY>
+             : tg.split     ? dev::k_dslash_tma_xy<SIO, LIO, XPAY, true>
+                            : dev::k_dslash_tma_xy<SIO, LIO, XPAY, false>;
     PLQCD_TRY(smem_optin((const void *)k, smem));
     int occ = 0;
     PLQCD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, block, smem));
@@ -915,7 +979,8 @@ struct StageLayout {
     uint32_t sp_main_bytes[2] = {0, 0}, sp_row_bytes[2] = {0, 0}, lk_main_bytes = 0, lk_row_bytes = 0;
 };
 
-StageLayout stage_layout(const TmaFormat &f, int L0h, int ny) {
+// nr > 1: spinor boxes of nr RHS (RHS tiles); the link boxes are per tile
+StageLayout stage_layout(const TmaFormat &f, int L0h, int ny, int nr = 1) {
     StageLayout l;
     uint32_t off = 0;
     auto take = [&](uint32_t n) {
@@ -924,9 +989,9 @@ StageLayout stage_layout(const TmaFormat &f, int L0h, int ny) {
         return o;
     };
     for (int gr = 0; gr < f.sp_ng; gr++) {
-        l.sp_main_bytes[gr] = (uint32_t)(f.sp_np[gr] * f.sp_eb[gr] * L0h * ny);
+        l.sp_main_bytes[gr] = (uint32_t)(f.sp_np[gr] * f.sp_eb[gr] * L0h * ny * nr);
         l.off_sp_main[gr] = take(l.sp_main_bytes[gr]);
-        l.sp_row_bytes[gr] = (uint32_t)(f.sp_np[gr] * f.sp_eb[gr] * L0h);
+        l.sp_row_bytes[gr] = (uint32_t)(f.sp_np[gr] * f.sp_eb[gr] * L0h * nr);
         l.off_sp_row[gr] = take(l.sp_row_bytes[gr]);
     }
     l.lk_main_bytes = (uint32_t)(f.lk_np * f.lk_eb * L0h * ny);
@@ -989,22 +1054,26 @@ bool row_ok(int L0h, int eb) {
 
 }  // namespace
 
-int dslash_tma_plan(const Geom &g, int prec, int recon, int kind, int nstage, int ny, int *block, size_t *smem) {
+int dslash_tma_plan(const Geom &g, int prec, int recon, int kind, int nstage, int ny, int *block, size_t *smem,
+                    int nr) {
     TmaFormat f;
     if (!tma_format(prec, recon, &f))
         return set_error(PLQCD_ERR_ARG, "dslash: no TMA kernel for precision/reconstruction %d/%d", prec, recon);
+    // RHS tiles: FP64 fields, own-line kinds with one own-line buffer
+    if (nr < 1 || (nr > 1 && (prec != PLQCD_F64 || (kind != 2 && kind != 4))))
+        return set_error(PLQCD_ERR_ARG, "dslash: no TMA RHS tile of %d for kind %d, precision %d", nr, kind, prec);
     bool rows = row_ok(g.L0h, f.lk_eb);
     for (int gr = 0; gr < f.sp_ng; gr++) rows = rows && row_ok(g.L0h, f.sp_eb[gr]);
     // kind 1: one stage per direction (a ring of at least 2); 2, 3: own-line
     // rows in 1 or 2 buffers of their own; 4, 5: the same with one box per
     // stage (a spinor stage waits for the link stage after it: 2 at least)
     const int min_stage = kind == 2 || kind == 3 ? 1 : 2;
-    const int nsites = ny * g.L0h;  // consumer threads
+    const int nsites = nr * ny * g.L0h;  // consumer threads
     if (kind < 1 || kind > 5 || nstage < min_stage || nstage > 8 || ny < 1 || !rows || g.L[1] % ny ||
-        (ny * g.L0h) % 32 || nsites > 256)
+        nsites % 32 || nsites > 256)
         return set_error(PLQCD_ERR_ARG, "dslash: TMA tile %d rows x %d stages (kind %d) does not fit %dx%dx%dx%d", ny,
                          nstage, kind, g.L[0], g.L[1], g.L[2], g.L[3]);
-    const StageLayout l = stage_layout(f, g.L0h, ny);
+    const StageLayout l = stage_layout(f, g.L0h, ny, nr);
     size_t bytes = (size_t)nstage * l.bytes + 16u * nstage + 128;
     if (kind > 1) {
         const XyLayout x = xy_layout(f, l, kind_split(kind));
@@ -1017,21 +1086,14 @@ int dslash_tma_plan(const Geom &g, int prec, int recon, int kind, int nstage, in
     return PLQCD_OK;
 }
 
-int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, int prec, int recon, bool full,
-                      bool xpay, int kind, int nstage, int ny) {
-    int block = 0;
-    size_t smem = 0;
-    PLQCD_TRY(dslash_tma_plan(g, prec, recon, kind, nstage, ny, &block, &smem));
-    // whole t-slices of one field (all of them for the full lattice)
-    const long S = (long)g.L0h * g.L[1] * g.L[2];
-    if (a.nrhs != 1 || (full && xpay) || a.h_begin % S || (a.h_end - a.h_begin) % S ||
-        (full && (a.h_begin != 0 || a.h_end != g.Vh)))
-        return set_error(PLQCD_ERR_ARG, "dslash: the TMA kernel takes whole t-slices of single fields");
-    TmaFormat fmt;
-    tma_format(prec, recon, &fmt);
-    const StageLayout lay = stage_layout(fmt, g.L0h, ny);
+namespace {
 
-    dev::TmaGeom tg;
+// tile geometry, stage layout and wait limits shared by the single-field and
+// the RHS-tile launches: tiles of ny rows over the t-slices [h_begin, h_end)
+// (half-site range of whole t-slices)
+void fill_tile_geom(dev::TmaGeom &tg, const Geom &g, const TmaFormat &fmt, const StageLayout &lay, int kind,
+                    int nstage, int ny, long h_begin, long h_end) {
+    const long S = (long)g.L0h * g.L[1] * g.L[2];
     memset(&tg, 0, sizeof tg);
     tg.Vh = g.Vh;
     tg.L0 = g.L[0];
@@ -1048,8 +1110,8 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     // t neighbours of a slice are at most a few waves of tiles old
     {
         auto div4 = [](int L) { return L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : 1); };
-        const int tc = (int)((a.h_end - a.h_begin) / S);
-        tg.t0 = (int)(a.h_begin / S);
+        const int tc = (int)((h_end - h_begin) / S);
+        tg.t0 = (int)(h_begin / S);
         tg.tc = tc;
         int bz = g.L[2], bt = div4(tc);
         if (const char *e = getenv("PLQCD_TMA_ORDER"))
@@ -1057,13 +1119,8 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
         tg.bz = (bz > 0 && g.L[2] % bz == 0) ? bz : 1;
         tg.bt = (bt > 0 && tc % bt == 0) ? bt : 1;
     }
-    const long ntiles = (long)tg.nty * g.L[2] * tg.tc;
-    if (ntiles * (full ? 2 : 1) > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash: lattice too large");
-    tg.nitems = (int)(ntiles * (full ? 2 : 1));
     tg.nstage = nstage;
     tg.ncw = ny * g.L0h / 32;
-    tg.full = full ? 1 : 0;
-    tg.out_parity = a.out_parity;
     tg.sp_ng = fmt.sp_ng;
     for (int gr = 0; gr < 2; gr++) {
         tg.sp_main_bytes[gr] = lay.sp_main_bytes[gr];
@@ -1092,10 +1149,6 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
         tg.off_lk_row = xl.off_lk_row;
         tg.stage_bytes = xl.b_bytes;
     }
-    tg.a_up = a.a_up;
-    tg.a_low = a.a_low;
-    tg.b = a.b;
-    tg.g5_in = a.g5_in;
     tg.cwait_ns = dev::kWaitLimitNs;
     // PLQCD_TMA_WAIT_HINT: suspend hint (ns) of the mbarrier retries
     {
@@ -1108,6 +1161,35 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
         tg.stall = 1;
         tg.cwait_ns = ns;
     }
+}
+
+}  // namespace
+
+int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, int prec, int recon, bool full,
+                      bool xpay, int kind, int nstage, int ny) {
+    int block = 0;
+    size_t smem = 0;
+    PLQCD_TRY(dslash_tma_plan(g, prec, recon, kind, nstage, ny, &block, &smem));
+    // whole t-slices of one field (all of them for the full lattice)
+    const long S = (long)g.L0h * g.L[1] * g.L[2];
+    if (a.nrhs != 1 || (full && xpay) || a.h_begin % S || (a.h_end - a.h_begin) % S ||
+        (full && (a.h_begin != 0 || a.h_end != g.Vh)))
+        return set_error(PLQCD_ERR_ARG, "dslash: the TMA kernel takes whole t-slices of single fields");
+    TmaFormat fmt;
+    tma_format(prec, recon, &fmt);
+    const StageLayout lay = stage_layout(fmt, g.L0h, ny);
+
+    dev::TmaGeom tg;
+    fill_tile_geom(tg, g, fmt, lay, kind, nstage, ny, a.h_begin, a.h_end);
+    const long ntiles = (long)tg.nty * g.L[2] * tg.tc;
+    if (ntiles * (full ? 2 : 1) > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash: lattice too large");
+    tg.nitems = (int)(ntiles * (full ? 2 : 1));
+    tg.full = full ? 1 : 0;
+    tg.out_parity = a.out_parity;
+    tg.a_up = a.a_up;
+    tg.a_low = a.a_low;
+    tg.b = a.b;
+    tg.g5_in = a.g5_in;
     tg.out0 = a.out[0];
     tg.out1 = full ? a.out[1] : a.out[0];
     tg.x = a.x;
@@ -1145,6 +1227,72 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     PLQCD_TMA_CASE(PLQCD_BF16, 12)
 #undef PLQCD_TMA_CASE
     return set_error(PLQCD_ERR_ARG, "dslash: no TMA kernel for precision/reconstruction %d/%d", prec, recon);
+}
+
+// RHS tiles: nr RHS of the block per tile, the links staged once per tile.
+// Per output site and RHS the staged bytes fall from 6 spinor rows + 8.5
+// link rows per row (one field at a time) to 6 spinor rows + 8.5 / nr link
+// rows (2 rows per tile).
+int launch_dslash_tma_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
+                           const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x,
+                           double b, int kind, int nstage, int ny, int nr) {
+    int block = 0;
+    size_t smem = 0;
+    PLQCD_TRY(dslash_tma_plan(g, prec, recon, kind, nstage, ny, &block, &smem, nr));
+    if (nr < 2 || nrhs < nr || nrhs % nr || (flags & PLQCD_DSLASH_COMPAT) || (out_parity != 0 && out_parity != 1))
+        return set_error(PLQCD_ERR_ARG, "dslash: TMA RHS tile of %d does not divide %d RHS", nr, nrhs);
+    TmaFormat fmt;
+    tma_format(prec, recon, &fmt);
+    const StageLayout lay = stage_layout(fmt, g.L0h, ny, nr);
+    const size_t fbytes = spinor_parity_bytes(g.Vh, prec);
+    if (fbytes % 16) return set_error(PLQCD_ERR_ARG, "dslash: field stride %zu is not a multiple of 16", fbytes);
+
+    dev::TmaGeom tg;
+    fill_tile_geom(tg, g, fmt, lay, kind, nstage, ny, 0, g.Vh);
+    const long ntiles = (long)tg.nty * g.L[2] * tg.tc;
+    if (ntiles * (nrhs / nr) > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash: lattice too large");
+    tg.nr = nr;
+    tg.ngr = nrhs / nr;
+    tg.nitems = (int)(ntiles * tg.ngr);
+    tg.ncw = nr * ny * g.L0h / 32;
+    tg.fbytes = fbytes;
+    for (int gr = 0; gr < fmt.sp_ng; gr++) {
+        tg.sp_main_rb[gr] = lay.sp_main_bytes[gr] / (uint32_t)nr;
+        tg.sp_row_rb[gr] = lay.sp_row_bytes[gr] / (uint32_t)nr;
+    }
+    tg.full = 0;
+    tg.out_parity = out_parity;
+    tg.a_up = a;
+    tg.a_low = (flags & PLQCD_DSLASH_G5_OUT) ? -a : a;
+    tg.b = b;
+    tg.g5_in = (flags & PLQCD_DSLASH_G5_IN) ? -1.0 : 1.0;
+    tg.out0 = tg.out1 = out;
+    tg.x = x;
+
+    dev::TmaMaps m;
+    memset(&m, 0, sizeof m);
+    size_t goff = 0;
+    for (int gr = 0; gr < fmt.sp_ng; gr++) {
+        const void *base = static_cast<const char *>(in) + goff;
+        PLQCD_TRY(encode_map(&m.sp_main[0][gr], base, g, fmt.sp_eb[gr], fmt.sp_np[gr], false, ny, nrhs, fbytes, nr));
+        PLQCD_TRY(encode_map(&m.sp_row[0][gr], base, g, fmt.sp_eb[gr], fmt.sp_np[gr], false, 1, nrhs, fbytes, nr));
+        m.sp_main[1][gr] = m.sp_main[0][gr];
+        m.sp_row[1][gr] = m.sp_row[0][gr];
+        goff += (size_t)fmt.sp_np[gr] * fmt.sp_eb[gr] * g.Vh;
+    }
+    PLQCD_TRY(encode_map(&m.lk_main, gauge, g, fmt.lk_eb, fmt.lk_np, true, ny));
+    PLQCD_TRY(encode_map(&m.lk_row, gauge, g, fmt.lk_eb, fmt.lk_np, true, 1));
+
+    using namespace dev;
+    const bool xpay = x != nullptr;
+#define PLQCD_TMA_CASE(P, RC)                                                                              \
+    if (prec == P && recon == RC)                                                                          \
+        return xpay ? launch_tma_t<SpinorIO<P>, LinkIO<P, RC>, true, true>(s, m, tg, block, smem)          \
+                    : launch_tma_t<SpinorIO<P>, LinkIO<P, RC>, false, true>(s, m, tg, block, smem);
+    PLQCD_TMA_CASE(PLQCD_F64, 18)
+    PLQCD_TMA_CASE(PLQCD_F64, 12)
+#undef PLQCD_TMA_CASE
+    return set_error(PLQCD_ERR_ARG, "dslash: no TMA RHS-tile kernel for precision/reconstruction %d/%d", prec, recon);
 }
 
 // Reads (and with `reset`, clears) the timeout flag of the TMA kernel on the

@@ -135,7 +135,15 @@ int launch_dslash(const Geom &g, cudaStream_t s, const DslashCall &c);
 // one tile-load box per ring stage), nstage ring buffers and ny rows per
 // tile. `plan` checks that the configuration exists for this lattice and
 // format and gives block / bytes.
-int dslash_tma_plan(const Geom &g, int prec, int recon, int kind, int nstage, int ny, int *block, size_t *smem);
+int dslash_tma_plan(const Geom &g, int prec, int recon, int kind, int nstage, int ny, int *block, size_t *smem,
+                    int nr = 1);
+// TMA-staged hop on a block of nrhs one-parity FP64 fields with RHS tiles
+// (own-line kinds 2 and 4 with nr RHS per tile; nrhs % nr == 0): the
+// variant 100000 * nr + 1000 * kind + 100 * nstage + ny of the multi-RHS
+// tuner. out = a * H in (+ b * x if x != null), flags as launch_dslash_mrhs
+int launch_dslash_tma_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int prec, int recon, void *out,
+                           const void *in, int nrhs, int out_parity, unsigned flags, double a, const void *x,
+                           double b, int kind, int nstage, int ny, int nr);
 // the device flag a TMA stage wait sets when it runs out (reset: clear it)
 int dslash_tma_status(bool reset);
 // variant 0: direct loads, 2/3: cp.async pipeline depth; no tuning

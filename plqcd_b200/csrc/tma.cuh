@@ -33,6 +33,19 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t byt
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
+// Proxy fence for shared memory. A buffer's consumers read it with plain
+// (generic-proxy) loads and release it on an mbarrier; the producer then
+// refills it with tile loads, which write through the async proxy. The
+// producer issues this fence after it has acquired the released buffer and
+// before the refill: the fence then lies on the causality path from the
+// consumers' reads to the refill's writes, so no write can land before a
+// read of the old contents. Without it, on B200, a refill now and then
+// overwrote a stage that was still being read (whole tiles of wrong results,
+// mostly with longer epilogues).
+__device__ __forceinline__ void fence_async_proxy_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }

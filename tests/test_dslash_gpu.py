@@ -788,18 +788,20 @@ def test_tma_kernel_bit_identical_at_benchmark_size(cuda, monkeypatch):
     lat.spinor_gaussian(fe, P.F64, 0, 11)
     lat.spinor_gaussian(fo, P.F64, 1, 12)
     outs = {}
-    variants = ("1204", "2204", "4304")
+    variants = ("1204", "2204", "4304", "2216")
     for v in ("2",) + variants:
         monkeypatch.setenv("PLQCD_DSLASH_STAGES", v)
         monkeypatch.setenv("PLQCD_DSLASH_BLOCK", "64")
-        oe, oo, o1 = dev_bytes(bs), dev_bytes(bs), dev_bytes(bs)
-        lat.dslash_full(g64, oe, oo, fe, fo, P.F64)
-        lat.dslash(g64, o1, fe, P.ODD, P.F64)
-        lat.synchronize()
-        outs[v] = (oe, oo, o1)
+        for rep in range(2 if v != "2" else 1):  # repeats: the same bits every launch
+            oe, oo, o1 = dev_bytes(bs), dev_bytes(bs), dev_bytes(bs)
+            lat.dslash_full(g64, oe, oo, fe, fo, P.F64)
+            lat.dslash(g64, o1, fe, P.ODD, P.F64)
+            lat.synchronize()
+            outs[(v, rep)] = (oe, oo, o1)
     for v in variants:
-        for a, b in zip(outs["2"], outs[v]):
-            assert bool((a == b).all()), v
+        for rep in range(2):
+            for a, b in zip(outs[("2", 0)], outs[(v, rep)]):
+                assert bool((a == b).all()), (v, rep)
 
 
 @pytest.mark.parametrize("variant", ["intrin_256", "intrin_512", "single_mic", "single_mic_short"])
@@ -913,6 +915,116 @@ def test_tma_wait_that_runs_out_reports_timeout(cuda, monkeypatch, variant):
     lat.dslash_full(g64, oe, oo, fe, fo, P.F64)
     lat.synchronize()
     assert bool((oe == re_).all()) and bool((oo == ro_).all())
+
+
+def _mrhs_tma_case(L, nrhs, seed, par):
+    lat, g64, u = _device_setup(L, seed)
+    bs = lat.spinor_bytes(P.F64)
+    blk_in, blk_out, blk_x = dev_bytes(nrhs * bs), dev_bytes(nrhs * bs), dev_bytes(nrhs * bs)
+    for r in range(nrhs):
+        lat.spinor_gaussian(blk_in[r * bs:(r + 1) * bs], P.F64, par ^ 1, 900 + r)
+        lat.spinor_gaussian(blk_x[r * bs:(r + 1) * bs], P.F64, par, 950 + r)
+    return lat, g64, bs, blk_in, blk_out, blk_x
+
+
+# variant = 100000 * RHS per tile + 1000 * kind + 100 * ring depth + rows per tile
+@pytest.mark.parametrize("L,nrhs,variant", [
+    ((8, 4, 6, 8), 8, 402102), ((8, 4, 6, 8), 8, 402202), ((8, 4, 6, 8), 8, 404202), ((8, 4, 6, 8), 8, 404302),
+    ((8, 4, 6, 8), 8, 802101), ((8, 4, 6, 8), 8, 804201), ((8, 4, 6, 8), 8, 202104), ((8, 4, 6, 8), 12, 402202),
+    ((16, 4, 4, 6), 8, 202202), ((16, 4, 4, 6), 6, 204202), ((12, 8, 4, 4), 16, 802204)])
+@pytest.mark.parametrize("recon", [18, 12])
+@pytest.mark.parametrize("xpay", [False, True])
+def test_multi_rhs_tma_rhs_tile_kernel_is_bit_identical(cuda, monkeypatch, L, nrhs, variant, recon, xpay):
+    """The TMA-staged FP64 multi-RHS hop with RHS tiles (several RHS of the
+    block per tile, each tile's links staged once for all of them; own-line
+    kinds 2 and 4), forced past the tuner, stores the same bytes as the
+    single-RHS kernel for every field of the block: several RHS groups,
+    tiles of 1, 2 and 4 rows, a tile that covers all of y (the rows on either
+    side wrap onto it), both link formats."""
+    par = 1 if xpay else 0
+    lat, g64, bs, blk_in, blk_out, blk_x = _mrhs_tma_case(L, nrhs, 61 + recon, par)
+    g = g64 if recon == 18 else P.Gauge(lat, P.F64, 12)
+    if g is not g64:
+        g.copy_from(g64)
+    monkeypatch.setenv("PLQCD_MRHS_VARIANT", str(variant))
+    flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
+    if xpay:
+        lat.dslash_mrhs_xpay(g, blk_out, blk_in, nrhs, par, P.F64, -0.0144, blk_x, 1.0, flags)
+    else:
+        lat.dslash_mrhs(g, blk_out, blk_in, nrhs, par, P.F64)
+    lat.synchronize()
+    monkeypatch.delenv("PLQCD_MRHS_VARIANT")
+    for r in range(nrhs):
+        sl = slice(r * bs, (r + 1) * bs)
+        one = dev_bytes(bs)
+        if xpay:
+            lat.dslash_xpay(g, one, blk_in[sl], par, P.F64, -0.0144, blk_x[sl], 1.0, flags)
+        else:
+            lat.dslash(g, one, blk_in[sl], par, P.F64)
+        lat.synchronize()
+        assert bool((blk_out[sl] == one).all()), (variant, r)
+
+
+def test_multi_rhs_tma_xpay_repeats_bit_identical_at_scale(cuda, monkeypatch):
+    """Persistent CTAs with many tiles each (16^3x32, 32 RHS, tiles of 4 RHS x
+    2 rows, 4 CTAs per SM): every repeat of the xpay hop gives the bytes of
+    the cp.async multi-RHS kernel. The producer must fence the async proxy
+    after a buffer's release and before its refill (the consumers read it
+    through the generic proxy); without that fence every repeat of this case
+    had tiles refilled under their readers."""
+    L, nrhs = (16, 16, 16, 32), 32
+    lat, g64, bs, blk_in, blk_out, blk_x = _mrhs_tma_case(L, nrhs, 81, 0)
+    flags = P.DSLASH_G5_IN | P.DSLASH_G5_OUT
+    ref = dev_bytes(nrhs * bs)
+    monkeypatch.setenv("PLQCD_MRHS_VARIANT", "102")
+    monkeypatch.setenv("PLQCD_MRHS_BLOCK", "64")
+    lat.dslash_mrhs_xpay(g64, ref, blk_in, nrhs, 0, P.F64, -0.0144, blk_x, 1.0, flags)
+    monkeypatch.setenv("PLQCD_MRHS_VARIANT", "402202")
+    for rep in range(3):
+        blk_out.zero_()
+        lat.dslash_mrhs_xpay(g64, blk_out, blk_in, nrhs, 0, P.F64, -0.0144, blk_x, 1.0, flags)
+        lat.synchronize()
+        assert bool((blk_out == ref).all()), rep
+
+
+def test_multi_rhs_tma_rhs_tile_rejects_tiles_that_do_not_fit(cuda, monkeypatch):
+    """RHS tiles that do not divide the block, or whose tile exceeds 256
+    consumer threads, are refused with a message; nothing is launched."""
+    lat, g64, bs, blk_in, blk_out, blk_x = _mrhs_tma_case((8, 4, 6, 8), 6, 3, 0)
+    for variant, msg in ((402202, "does not divide"), (202203, "does not fit")):
+        monkeypatch.setenv("PLQCD_MRHS_VARIANT", str(variant))
+        rc = P.lib().plqcd_dslash_mrhs(lat.handle, g64.handle, blk_out.data_ptr(), blk_in.data_ptr(), 6, 0, P.F64, 0)
+        assert rc == -1 and msg in P.last_error(), (variant, P.last_error())
+    monkeypatch.delenv("PLQCD_MRHS_VARIANT")
+
+
+def test_multi_rhs_tma_wait_that_runs_out_reports_timeout(cuda, monkeypatch):
+    """The bounded stage waits of the RHS-tile kernel: with the test hook on,
+    the consumer waits run out, synchronize reports PLQCD_ERR_TIMEOUT, and
+    the next launch gives the single-RHS kernel's bytes again."""
+    nrhs = 8
+    lat, g64, bs, blk_in, blk_out, blk_x = _mrhs_tma_case((16, 8, 6, 4), nrhs, 71, 0)
+    ref = dev_bytes(nrhs * bs)
+    for r in range(nrhs):
+        sl = slice(r * bs, (r + 1) * bs)
+        lat.dslash(g64, ref[sl], blk_in[sl], 0, P.F64)
+    lat.synchronize()
+    monkeypatch.setenv("PLQCD_MRHS_VARIANT", "402202")
+    lib = P.lib()
+    P.check(lib.plqcd_tma_timeout_test(1, 200_000))
+    try:
+        P.check(lib.plqcd_dslash_mrhs(lat.handle, g64.handle, blk_out.data_ptr(), blk_in.data_ptr(), nrhs, 0,
+                                      P.F64, 0))
+        rc = lib.plqcd_lattice_synchronize(lat.handle)
+        msg = P.last_error()
+    finally:
+        P.check(lib.plqcd_tma_timeout_test(0, 0))
+    assert rc == P.ERR_TIMEOUT, (rc, msg)
+    assert lib.plqcd_lattice_synchronize(lat.handle) == 0
+    lat.dslash_mrhs(g64, blk_out, blk_in, nrhs, 0, P.F64)
+    lat.synchronize()
+    monkeypatch.delenv("PLQCD_MRHS_VARIANT")
+    assert bool((blk_out == ref).all())
 
 
 def test_tma_timeout_test_hook_rejects_bad_limits(cuda):
