@@ -353,7 +353,7 @@ def run_ours(args, d: Dist):
             print(json.dumps({"only": "sharded", "sharded": res}))
         return 0
     if args.only == "mrhs":  # the multi-RHS kernels alone (profiling runs)
-        res = run_mrhs(torch, P, lat, g64, args)
+        res = run_mrhs(torch, P, lat, g64, args, args.mrhs_nrhs)
         if d.rank == 0:
             print(json.dumps({"only": "mrhs", "lattice": list(L), "mrhs_dslash": res}))
         return 0
@@ -736,7 +736,17 @@ def run_mrhs(torch, P, lat, g64, args, nrhs=8):
         res[name] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)
         cfg = tuned_config(P, f"dslash_mrhs|p{prec}|r{recon}|plain|n{nrhs}|{lat.dims[0]}x")
         res[name]["tuned_variant"] = cfg[0] if cfg else None
-        if prec == P.F64:
+        if args.mrhs_forced:  # profiling runs: only these forced configurations
+            forced = {}
+            for vb in args.mrhs_forced.split(","):
+                v, blk = (int(x) for x in vb.split("/"))
+                os.environ["PLQCD_MRHS_VARIANT"], os.environ["PLQCD_MRHS_BLOCK"] = str(v), str(blk)
+                try:
+                    forced[f"{v}/{blk}"] = rate(time_kernel(torch, hop, 20, 3) / 20 / 1e3)["us"]
+                finally:
+                    del os.environ["PLQCD_MRHS_VARIANT"], os.environ["PLQCD_MRHS_BLOCK"]
+            res[name]["forced_us"] = forced
+        elif prec == P.F64:
             forced = {}
             # 4xxx: links shared in shared memory; 1xxxxx-8xxxxx: TMA-staged
             # rows with RHS tiles (100000 * RHS per tile + TMA variant)
@@ -905,6 +915,10 @@ def main():
                     help="batched solves as eager loops instead of one graph launch (ncu does not profile "
                          "the kernels of graphs with conditional nodes)")
     ap.add_argument("--mrhs-formats", default="", help="comma list of the multi-RHS formats to time (default all)")
+    ap.add_argument("--mrhs-nrhs", type=int, default=8, help="RHS of --only mrhs")
+    ap.add_argument("--mrhs-forced", default="",
+                    help="--only mrhs: comma list of variant/block configurations to time forced (default: a "
+                         "built-in list)")
     args = ap.parse_args()
     args.lattice = tuple(int(x) for x in args.lattice.split(","))
     d = Dist()
