@@ -29,6 +29,16 @@
 // Every coordinate passed to a tile load is a wrapped, in-range coordinate
 // and the innermost one is always 0, so no load reads out of bounds.
 //
+// Consumers read a stage with plain loads, then lane 0 of each warp
+// arrives on the stage's empty barrier. The producer refills a buffer only
+// after that barrier completes, and fences the async proxy first: the
+// refill's tile loads must not land before the consumers' reads of the old
+// contents.
+//
+// The own-line kernel also runs RHS tiles (MR): one parity of a block of
+// FP64 fields, a tile of NY rows of nr RHS, the spinor boxes with an RHS
+// dimension and the tile's link boxes shared by its nr RHS.
+//
 // Every mbarrier wait is bounded (2 s by %globaltimer). A wait that runs
 // out sets a device status flag (read by dslash_tma_status()), the CTA's
 // threads stop, and the producer waits (bounded again) for the copies it
