@@ -50,12 +50,13 @@ BYTES_HALF_12 = 52 + 8 * 24 + 52
 # (profiles/dslash_full_f64_dram_32x32x32x64.txt): variant -> bytes/site.
 # Variant 2 is the cp.async kernel, 1000*kind + 100*stages + rows a TMA kernel
 # (kind 1: a stage per direction; 2-5: own-line rows staged once per tile).
-# 2216 is captured with the default tile order (whole z, 4 t-slices), the
-# others with the earlier 8 x 8 (z, t) blocks.
+# 2216 is captured with the full-lattice default tile order (blocks of half
+# the z extent x all t-slices), the others with the earlier 8 x 8 (z, t)
+# blocks.
 DRAM_BYTES_PER_SITE_F64_FULL = {
     2: 2127234136 / 2097152, 1204: 2191090112 / 2097152, 2204: 2253279192 / 2097152,
     4304: 2204120856 / 2097152, 1304: 2527646688 / 2097152, 1408: 2198568976 / 2097152,
-    2216: (1738938624 + 388427008) / 2097152,
+    2216: (1778083584 + 387864064) / 2097152,
 }
 
 
