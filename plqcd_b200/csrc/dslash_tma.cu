@@ -55,6 +55,7 @@
 
 #include "dslash_core.cuh"
 #include "internal.h"
+#include "tile_order.cuh"
 #include "tma.cuh"
 
 namespace plqcd {
@@ -235,47 +236,6 @@ template <>
 struct TmaLink<LinkIO<PLQCD_BF16, 12>> : TmaLink16<PLQCD_BF16> {};
 
 __device__ int g_tma_status;  // set to 1 when a stage wait ran out
-
-struct TileCoord {
-    int p, y0, zt, z, t;
-    int r0;  // first RHS of the tile (RHS tiles; 0 otherwise)
-};
-
-// MR (RHS tiles): the RHS group runs fastest, so the groups of the same
-// rows are in flight together and the links one of them brings from HBM
-// serve the others from L2
-template <bool MR = false>
-__device__ __forceinline__ TileCoord tile_coord(const TmaGeom &g, int item) {
-    TileCoord c;
-    int tile;
-    c.r0 = 0;
-    if constexpr (MR) {
-        c.p = g.out_parity;
-        const int grp = item % g.ngr;
-        c.r0 = grp * g.nr;
-        tile = item / g.ngr;
-    } else if (g.full) {
-        c.p = item & 1;
-        tile = item >> 1;
-    } else {
-        c.p = g.out_parity;
-        tile = item;
-    }
-    // y-tiles fastest, then z and t inside a (bz x bt) block, then the
-    // blocks (z-blocks inner): a block's z and t neighbours are read while
-    // they are still in L2
-    int k = tile / g.nty;
-    c.y0 = (tile - k * g.nty) * g.NY;
-    const int zin = k % g.bz;
-    k /= g.bz;
-    const int tin = k % g.bt;
-    k /= g.bt;
-    const int nbz = g.L2 / g.bz;
-    c.z = (k % nbz) * g.bz + zin;
-    c.t = g.t0 + (k / nbz) * g.bt + tin;
-    c.zt = c.z + g.L2 * c.t;
-    return c;
-}
 
 // loads of direction d (0..3 forward mu, 4..7 backward mu) into the stage
 // buffer at shared address dst, completing on `bar`
@@ -1100,9 +1060,10 @@ namespace {
 
 // tile geometry, stage layout and wait limits shared by the single-field and
 // the RHS-tile launches: tiles of ny rows over the t-slices [h_begin, h_end)
-// (half-site range of whole t-slices)
+// (half-site range of whole t-slices); `launch` (dev::TileLaunch) picks the
+// default tile order
 void fill_tile_geom(dev::TmaGeom &tg, const Geom &g, const TmaFormat &fmt, const StageLayout &lay, int kind,
-                    int nstage, int ny, long h_begin, long h_end) {
+                    int nstage, int ny, long h_begin, long h_end, int launch) {
     const long S = (long)g.L0h * g.L[1] * g.L[2];
     memset(&tg, 0, sizeof tg);
     tg.Vh = g.Vh;
@@ -1113,18 +1074,15 @@ void fill_tile_geom(dev::TmaGeom &tg, const Geom &g, const TmaFormat &fmt, const
     tg.L3 = g.L[3];
     tg.NY = ny;
     tg.nty = g.L[1] / ny;
-    // tile-order block: PLQCD_TMA_ORDER="bz,bt" (each must divide its extent;
-    // 1,1 = plain z-fastest order). Default here: all of z, then 4 (or 2, 1)
-    // t-slices (the full-lattice and RHS-tile launches set their own). At
-    // 32^3x64 (FP64 full lattice, 16-row tiles) this reads 829 DRAM bytes per
-    // site against 866 for 8x8 blocks (768 algorithmic): the t neighbours of a
-    // slice are at most a few waves of tiles old
+    // tile-order block: the launch's default (tile_order.cuh), or
+    // PLQCD_TMA_ORDER="bz,bt" (each must divide its extent, else 1; 1,1 = the
+    // plain z-fastest order)
     {
-        auto div4 = [](int L) { return L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : 1); };
         const int tc = (int)((h_end - h_begin) / S);
         tg.t0 = (int)(h_begin / S);
         tg.tc = tc;
-        int bz = g.L[2], bt = div4(tc);
+        int bz = 1, bt = 1;
+        dev::tile_order_default(launch, g.L[2], tc, &bz, &bt);
         if (const char *e = getenv("PLQCD_TMA_ORDER"))
             if (sscanf(e, "%d,%d", &bz, &bt) != 2) bz = bt = 1;
         tg.bz = (bz > 0 && g.L[2] % bz == 0) ? bz : 1;
@@ -1191,14 +1149,8 @@ int launch_dslash_tma(const Geom &g, cudaStream_t s, const dev::DslashArgs &a, i
     const StageLayout lay = stage_layout(fmt, g.L0h, ny);
 
     dev::TmaGeom tg;
-    fill_tile_geom(tg, g, fmt, lay, kind, nstage, ny, a.h_begin, a.h_end);
-    // full lattice: blocks of half the z extent x all t-slices unless
-    // PLQCD_TMA_ORDER sets the order. FP64 at 32^3x64, 2216, ten interleaved
-    // rounds: median 448.5 us against 459.2 for whole z lines (4304: even)
-    if (full && !getenv("PLQCD_TMA_ORDER")) {
-        tg.bz = g.L[2] % 2 == 0 ? g.L[2] / 2 : g.L[2];
-        tg.bt = tg.tc;
-    }
+    fill_tile_geom(tg, g, fmt, lay, kind, nstage, ny, a.h_begin, a.h_end,
+                   full ? dev::kTileFull : dev::kTileParity);
     const long ntiles = (long)tg.nty * g.L[2] * tg.tc;
     if (ntiles * (full ? 2 : 1) > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash: lattice too large");
     tg.nitems = (int)(ntiles * (full ? 2 : 1));
@@ -1266,20 +1218,9 @@ int launch_dslash_tma_mrhs(const Geom &g, cudaStream_t s, const void *gauge, int
     if (fbytes % 16) return set_error(PLQCD_ERR_ARG, "dslash: field stride %zu is not a multiple of 16", fbytes);
 
     dev::TmaGeom tg;
-    fill_tile_geom(tg, g, fmt, lay, kind, nstage, ny, 0, g.Vh);
+    fill_tile_geom(tg, g, fmt, lay, kind, nstage, ny, 0, g.Vh, dev::kTileRhs);
     const long ntiles = (long)tg.nty * g.L[2] * tg.tc;
     if (ntiles * (nrhs / nr) > 0x7fffffffL) return set_error(PLQCD_ERR_ARG, "dslash: lattice too large");
-    // tile order: blocks of a quarter of the z extent (if it divides) x all
-    // t-slices, unless PLQCD_TMA_ORDER sets it. With several RHS per tile a
-    // t-slice of whole z lines is tens of MB, and a row's t neighbours leave
-    // L2 before their second use (L2 hit rate 51% at 24^3x48, 16 RHS).
-    // 402202, this order against whole z lines: 32^3x64 / 8 RHS 1630 against
-    // 1731 us, 16^3x32 / 32 RHS 363 against 385 us; 24^3x48 / 16 RHS within
-    // the spread of two boxes (1189-1285 against 1243-1338 us)
-    if (!getenv("PLQCD_TMA_ORDER")) {
-        tg.bz = g.L[2] % 4 == 0 ? g.L[2] / 4 : g.L[2];
-        tg.bt = tg.tc;
-    }
     tg.nr = nr;
     tg.ngr = nrhs / nr;
     tg.nitems = (int)(ntiles * tg.ngr);
